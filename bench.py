@@ -1,0 +1,309 @@
+"""Benchmark: Kerr rays/s on one B200 (or N independent replicas).
+
+Workload (default ``disk16``): the adaptive Dormand-Prince disk scene, 16
+frames of 1024x1024 pixels, spin a in {0, 0.5, 0.9, 0.998} crossed with
+inclination in {17, 45, 75, 85} deg, observer at r = 1000 M, image plane
+alpha, beta in [-12, 12] M, rtol 1e-8, atol 1e-10, up to 3 crossings of a
+transparent thin disk r_isco..30 M. One step = one render of all 16 frames.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun as N independent replicas (every pixel is
+independent: no exchange step); value = all ranks' rays / max-over-ranks time.
+``--impl reference`` times the reference's own CPU path on the host cores
+(oracle/_ref: the reference's compiled src/physics/kerr.cpp potentials
+driving the same tracer) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Kerr rays/sec on 1 B200: FP64 plain vs mixed/surrogate at stated g-error"
+UNIT = "rays/s"
+
+# Algorithmic FLOPs (add, mul, div, sqrt each 1) per accepted integration
+# step, frozen from the oracle's counting scalar over seeded pixels of each
+# workload (tests/test_flop_constants.py re-derives them).
+FLOPS_PER_STEP = {"dp45": 566.0, "rk4": 211.0}
+
+WORKLOADS = {
+    # name: (frames, width, integrator, max_crossings)
+    "disk16": dict(width=1024, height=1024, integrator=1, max_crossings=3,
+                   frames=[(a, i) for a in (0.0, 0.5, 0.9, 0.998) for i in (17.0, 45.0, 75.0, 85.0)]),
+    "c0_256": dict(width=256, height=256, integrator=0, max_crossings=1, frames=[(0.9, 60.0)]),
+    "disk_2048": dict(width=2048, height=2048, integrator=0, max_crossings=1, frames=[(0.9, 60.0)]),
+}
+OUT_FIELDS_USED = ("cls", "steps", "n_cross", "r_hit", "phi_hit", "g", "intensity", "theta_inf", "phi_inf")
+
+
+def scenes_for(workload: str, precision: int):
+    from blackhole_b200._abi import default_scene
+
+    w = WORKLOADS[workload]
+    out = []
+    for spin, inc in w["frames"]:
+        out.append(default_scene(width=w["width"], height=w["height"], spin=spin, theta_obs=math.radians(inc),
+                                 integrator=w["integrator"], max_crossings=w["max_crossings"],
+                                 precision=precision))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args, rank: int, world: int, dist):
+    import torch
+
+    from blackhole_b200 import _abi, kerr
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    lib = _abi.load_library()
+    precision = 1 if args.precision == "mixed" else 0
+    scenes = scenes_for(args.workload, precision)
+    wl = WORKLOADS[args.workload]
+    integ = "dp45" if wl["integrator"] == 1 else "rk4"
+    n_frame = wl["width"] * wl["height"]
+    rays_per_step = n_frame * len(scenes)
+    stream = torch.cuda.Stream(device=dev)
+    outs = [kerr.alloc_image_outputs(s, device=dev, fields=list(OUT_FIELDS_USED)) for s in scenes]
+
+    def render(ev=None):
+        for i, s in enumerate(scenes):
+            if ev is not None:
+                ev[i][0].record(stream)
+            kerr.trace_image(s, outs[i], stream=stream)
+            if ev is not None:
+                ev[i][1].record(stream)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        render()
+    torch.cuda.synchronize(dev)
+    barrier()
+    torch.cuda.synchronize(dev)
+
+    sampler = ClockSampler(dev.index if "CUDA_VISIBLE_DEVICES" not in os.environ else 0)
+    sampler.start()
+    time.sleep(0.3)
+    per_launch = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                   for _ in scenes] for _ in range(args.steps)]
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for k in range(args.steps):
+        render(per_launch[k])
+    t1.record(stream)
+    torch.cuda.synchronize(dev)
+    clocks = sampler.stop()
+    barrier()
+    elapsed_ms = t0.elapsed_time(t1)
+    launch_ms = [a.elapsed_time(b) for step in per_launch for (a, b) in step]
+    total_steps = sum(int(o["steps"].sum().item()) for o in outs)  # accepted steps of one render
+
+    if dist is not None:
+        t = torch.tensor([elapsed_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+
+    value = rays_per_step * args.steps * world / (elapsed_ms * 1e-3)
+    ms_per_step = elapsed_ms / args.steps
+
+    # ---- end to end through the host-buffer C entry point (pinned host memory) ----
+    e2e = None
+    if rank == 0:
+        pinned = []
+        for s in scenes:
+            d = {}
+            for f in OUT_FIELDS_USED:
+                shape = (s.max_crossings * n_frame,) if f in _abi.PLANE_FIELDS else (n_frame,)
+                dt = torch.int32 if f in _abi.INT_FIELDS else torch.float64
+                d[f] = torch.empty(shape, dtype=dt).pin_memory()
+            pinned.append(d)
+        structs = []
+        for d in pinned:
+            o = _abi.KerrImageOut()
+            for f, t in d.items():
+                setattr(o, f, t.data_ptr())
+            structs.append(o)
+        d2h = sum(t.numel() * t.element_size() for d in pinned for t in d.values())
+        h2d = C.sizeof(_abi.KerrScene) * len(scenes)
+        for s, o in zip(scenes, structs):  # warm the host path's cached buffers
+            _abi.check(lib.bh_kerr_trace_image_host(C.byref(s), C.byref(o)))
+        e2e_steps = max(1, min(args.steps, 3))
+        w0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            for s, o in zip(scenes, structs):
+                _abi.check(lib.bh_kerr_trace_image_host(C.byref(s), C.byref(o)))
+        w1 = time.perf_counter()
+        e2e = {"value": rays_per_step * e2e_steps / (w1 - w0), "unit": UNIT, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "api": "bh_kerr_trace_image_host"}
+
+    # ---- roofline of the tracing kernel ----
+    peak = C.c_double(0.0)
+    _abi.check(lib.bh_measure_fma_peak(1 if precision == 0 else 0, 5, C.byref(peak)))
+    mean_launch_s = statistics.mean(launch_ms) * 1e-3
+    flops_per_launch = FLOPS_PER_STEP[integ] * total_steps / len(scenes)
+    achieved = flops_per_launch / mean_launch_s / 1e12
+    roofline = {"bound": "fp64" if precision == 0 else "fp32", "achieved": achieved, "peak": peak.value,
+                "unit": "TFLOP/s", "frac": achieved / peak.value if peak.value else None, "traffic": None,
+                "peak_source": "measured FMA-pipe probe (bh_measure_fma_peak), FMA = 2 FLOPs",
+                "flops_per_step": FLOPS_PER_STEP[integ], "steps_per_launch": total_steps / len(scenes),
+                "kernel": f"k_trace_image_fp64<{1 if integ == 'dp45' else 0}>",
+                "launch_ms_mean": statistics.mean(launch_ms)}
+    return dict(value=value, ms_per_step=ms_per_step, e2e=e2e, roofline=roofline, clocks=clocks,
+                total_steps=total_steps, rays_per_step=rays_per_step, launches=len(scenes) * args.steps)
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the reference's compiled CPU code on the host cores
+# ---------------------------------------------------------------------------
+def cpu_reference(workload: str, budget_s: float, seed: int = 7):
+    """Time oracle/_ref (reference-compiled potentials) on a bounded random
+    sample of the workload's pixels until ~budget_s of wall time is spent."""
+    from oracle.pyoracle import RefLib, default_threads
+
+    lib = RefLib()
+    threads = default_threads()
+    scenes = scenes_for(workload, 0)
+    n_frame = scenes[0].width * scenes[0].height
+    rng = np.random.default_rng(seed)
+    done = 0
+    chunk = max(64, 4 * threads)
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < budget_s:
+        for s in scenes:
+            pix = rng.integers(0, n_frame, chunk)
+            lib.trace_pixels(s, pix, threads=threads)
+            done += chunk
+    el = time.perf_counter() - t0
+    return {"value": done / el, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"{done} random pixels spread over the {len(scenes)} frames of {workload}, "
+                      f"{el:.1f} s wall on {threads} threads (oracle/_ref: reference kerrPotentials)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--workload", choices=tuple(WORKLOADS), default="disk16")
+    ap.add_argument("--precision", choices=("fp64", "mixed"), default="fp64")
+    ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU baseline sampling")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    rank = int(os.environ.get("RANK", 0))
+    wl = WORKLOADS[args.workload]
+    config = {"workload": args.workload, "frames": len(wl["frames"]), "width": wl["width"], "height": wl["height"],
+              "integrator": "dp45" if wl["integrator"] == 1 else "rk4", "rtol": 1e-8, "atol": 1e-10,
+              "max_crossings": wl["max_crossings"], "r_obs": 1000.0, "image_plane_M": [-12, 12],
+              "parallelism": f"replicas{world}", "l2": "outputs written once per step (1.7 GB > L2); no inputs"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        cb = cpu_reference(args.workload, args.cpu_budget)
+        line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config, "impl": "reference",
+                "cpu_baseline": cb,
+                "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+
+        dist_mod.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+        dist = dist_mod
+    res = run_ours(args, rank, world, dist)
+    if rank == 0:
+        cb = cpu_reference(args.workload, args.cpu_budget) if (world == 1 and args.cpu_budget > 0) else None
+        line = {"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+                "data": "synthetic", "config": config, "precision": args.precision,
+                "steps_per_s": res["total_steps"] * args.steps * world / (res["ms_per_step"] * args.steps * 1e-3),
+                "e2e": res["e2e"], "roofline": res["roofline"], "cpu_baseline": cb, "clocks": res["clocks"],
+                "gpu_launches": res["launches"]}
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

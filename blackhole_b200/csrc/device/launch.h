@@ -1,0 +1,73 @@
+// launch.h - internal C ABI between the C++23 host layer (csrc/host) and the
+// CUDA translation units (csrc/device). POD structs and plain functions only,
+// so that g++ -std=c++23 and nvcc see the same layout.
+#pragma once
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+// Everything the image kernels need about one scene, precomputed on the host
+// (including every libm-derived constant, so that the device never calls a
+// transcendental function that could differ from the CPU oracle by an ulp).
+typedef struct BhkImageParams {
+  double a, a2;            // spin and spin^2
+  double r_obs;
+  double r_hor;            // horizon_factor * r_+
+  double r_esc;            // escape_factor * r_obs
+  double r_in, r_out;      // disk edges
+  double sin_o, cos_o;     // observer inclination
+  double alpha_min, dalpha, beta_min, dbeta;  // pixel-centre grid
+  double step_coeff, step_rcap;
+  double rtol, atol;
+  double nt_isco;          // ISCO of NovikovThorneDisk (pow form)
+  double nt_flux_peak;     // its flux at 1.5 r_isco
+  int64_t n_pix;
+  int32_t width;
+  int32_t max_steps;
+  int32_t max_cross;       // 1..3
+  int32_t form;            // 0 reference, 1 Carter
+  int32_t integrator;      // 0 RK4, 1 DP45
+  int32_t pad;
+} BhkImageParams;
+
+typedef struct BhkImageOut {
+  int32_t *cls, *steps, *n_cross;
+  double *r_hit, *phi_hit, *g;  // [max_cross][n]
+  double *flux, *intensity, *theta_inf, *phi_inf;
+} BhkImageOut;
+
+typedef struct BhkLaunch {
+  int32_t grid;      // CTAs
+  int32_t block;     // threads per CTA
+} BhkLaunch;
+
+// FP64 image tracer. work_counter: one zeroed-on-stream 64-bit device word.
+int bhk_trace_image_fp64(const BhkImageParams *p, const BhkImageOut *o, unsigned long long *work_counter,
+                         BhkLaunch launch, void *stream);
+// Occupancy query: max resident CTAs per SM for the given block size.
+int bhk_trace_image_fp64_occupancy(int integrator, int block, int *blocks_per_sm);
+
+// Reference stepper kernels (src/physics/kerr.cpp semantics), FP64.
+typedef struct BhkStateSoA { double *r, *theta, *phi, *t, *sr, *sth; } BhkStateSoA;
+typedef struct BhkConstsSoA { const double *e, *lz, *q; } BhkConstsSoA;
+
+int bhk_kerr_potentials(int64_t n, const double *r, const double *theta, double mass, double a,
+                        BhkConstsSoA c, double *rp, double *drp, double *tp, double *dtp, void *stream);
+int bhk_kerr_step_mino(int64_t n, BhkStateSoA s, double mass, double a, BhkConstsSoA c, const double *dlam,
+                       double dlam_scalar, void *stream);
+int bhk_kerr_trace_rays(int64_t n, BhkStateSoA init, BhkConstsSoA c, double mass, double a, double r_horizon,
+                        double r_escape, double step, int32_t max_steps, int32_t *status, int32_t *steps,
+                        double *dist, double *rf, double *thf, double *phf, double *redshift, void *stream);
+
+// FMA-throughput probe (probe.cu).
+int bhk_fma_probe(int fp64, int iters, int repeats, double *tflops);
+
+// Last CUDA error string of the device layer (thread-local).
+const char *bhk_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif

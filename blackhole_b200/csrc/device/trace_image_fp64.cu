@@ -1,0 +1,253 @@
+// trace_image_fp64.cu - FP64 image-plane Kerr tracer (sm_100a).
+//
+// One ray per lane in a persistent grid: each warp keeps 32 rays in
+// registers and, whenever rays terminate (horizon, disk, escape, step
+// budget), refills exactly those lanes from a global work counter with one
+// warp-aggregated atomicAdd (ballot + popc), so finished rays never idle a
+// lane while work remains. The integration follows the reference trace loop
+// order (src/physics/raytracer.h:338-365): step budget, horizon test, escape
+// test, step; then the equatorial-crossing test with bisection
+// (src/physics/event_detection.h:127-180 pattern).
+//
+// Built with -fmad=false: bit-identical to the FP64 CPU oracle.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+
+#include "image_fp64.cuh"
+#include "launch.h"
+
+namespace bhk {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+struct RayFp64 {
+  RayC c;
+  Yd y;
+  Yd k1;        // DP45: FSAL stage of y
+  double h;     // DP45: next trial step
+  double inten;
+  long long pix;
+  int steps;
+  int attempts;
+  int ncross;
+};
+
+__device__ __forceinline__ void init_ray(const BhkImageParams &p, long long pix, RayFp64 &R) {
+  const long long i = pix % p.width, j = pix / p.width;
+  const double alpha = p.alpha_min + ((double)i + 0.5) * p.dalpha;
+  const double beta = p.beta_min + ((double)j + 0.5) * p.dbeta;
+  R.c.a = p.a;
+  R.c.a2 = p.a2;
+  R.c.lam = -alpha * p.sin_o;
+  const double eta = (beta * beta) + (((alpha * alpha) - (p.a * p.a)) * p.cos_o) * p.cos_o;
+  R.c.qTh = eta + (R.c.lam * R.c.lam);
+  const double qR = (p.form == 1) ? eta : R.c.qTh;
+  R.c.K = qR + ((R.c.lam - R.c.a) * (R.c.lam - R.c.a));
+  R.y.r = p.r_obs;
+  R.y.u = p.cos_o;
+  R.y.phi = 0.0;
+  const double Rv = pot_R(R.y.r, R.c);
+  R.y.pr = -sqrt((Rv < 0.0) ? 0.0 : Rv);
+  R.y.pu = beta * p.sin_o;
+  R.steps = 0;
+  R.attempts = 0;
+  R.ncross = 0;
+  R.inten = 0.0;
+  R.pix = pix;
+  if (p.integrator == 1) {
+    const double hh = p.step_coeff * dmin_(R.y.r, p.step_rcap);
+    const double sigma = (R.y.r * R.y.r) + ((p.a2 * R.y.u) * R.y.u);
+    R.h = hh / sigma;
+    R.k1 = rhs(R.y, R.c);
+  }
+}
+
+template <int INTEG>
+__device__ __forceinline__ Yd sub_step(const BhkImageParams &p, const RayC &c, const Yd &y, double h) {
+  if (INTEG == 0) return rk4(y, h, c, rhs(y, c));
+  return dp45(y, h, c, rhs(y, c), p.rtol, p.atol, false).y5;
+}
+
+// Bisection on the sub-step for u = 0 inside [0, h] from y0.
+template <int INTEG>
+__device__ __noinline__ Yd bisect_equator(const BhkImageParams &p, const RayC &c, const Yd &y0, double h) {
+  double la = 0.0, lb = h;
+  Yd sa = y0;
+  for (int i = 0; i < 60; ++i) {
+    const double lm = 0.5 * (la + lb);
+    const Yd sm = sub_step<INTEG>(p, c, sa, lm - la);
+    if (fabs(sm.u) < 1e-13) return sm;
+    if ((sa.u * sm.u) < 0.0) {
+      lb = lm;
+    } else {
+      la = lm;
+      sa = sm;
+    }
+  }
+  const double lm = 0.5 * (la + lb);
+  return sub_step<INTEG>(p, c, sa, lm - la);
+}
+
+// Records a crossing at yc when it lies on the disk; returns true when the
+// ray stops there (last allowed crossing).
+__device__ __forceinline__ bool on_crossing(const BhkImageParams &p, const BhkImageOut &o, RayFp64 &R,
+                                            const Yd &yc) {
+  if (!(yc.r >= p.r_in && yc.r <= p.r_out)) return false;
+  const int k = R.ncross;
+  const long long off = (long long)k * p.n_pix + R.pix;
+  const double g = disk_g(yc.r, p.a, R.c.lam);
+  if (o.r_hit) o.r_hit[off] = yc.r;
+  if (o.phi_hit) o.phi_hit[off] = yc.phi;
+  if (o.g) o.g[off] = g;
+  const double q = p.r_in / yc.r;
+  const double g2 = g * g;
+  R.inten = R.inten + ((((g2 * g2) * q) * q) * q);
+  if (k == 0 && o.flux) o.flux[R.pix] = nt_flux(yc.r, p.nt_isco, p.nt_flux_peak);
+  R.ncross = k + 1;
+  return R.ncross >= p.max_cross;
+}
+
+__device__ __forceinline__ void finish(const BhkImageParams &p, const BhkImageOut &o, const RayFp64 &R,
+                                       int cls) {
+  const long long pix = R.pix;
+  if (o.cls) o.cls[pix] = cls;
+  if (o.steps) o.steps[pix] = R.steps;
+  if (o.n_cross) o.n_cross[pix] = R.ncross;
+  if (o.intensity) o.intensity[pix] = R.inten;
+  if (R.ncross == 0 && o.flux) o.flux[pix] = 0.0;
+  for (int k = R.ncross; k < p.max_cross; ++k) {
+    const long long off = (long long)k * p.n_pix + pix;
+    if (o.r_hit) o.r_hit[off] = 0.0;
+    if (o.phi_hit) o.phi_hit[off] = 0.0;
+    if (o.g) o.g[off] = 0.0;
+  }
+  double th = 0.0, ph = 0.0;
+  if (cls == 2) {
+    const double u = R.y.u;
+    th = acos((u < -1.0) ? -1.0 : ((1.0 < u) ? 1.0 : u));
+    ph = R.y.phi;
+  }
+  if (o.theta_inf) o.theta_inf[pix] = th;
+  if (o.phi_inf) o.phi_inf[pix] = ph;
+}
+
+// One iteration of the trace loop for an active ray; returns the class when
+// the ray terminates, -1 otherwise.
+template <int INTEG>
+__device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOut &o, RayFp64 &R) {
+  if (INTEG == 0) {
+    if (R.steps >= p.max_steps) return 3;
+    if (R.y.r <= p.r_hor) return 0;
+    if (R.y.r >= p.r_esc) return 2;
+    const double hh = p.step_coeff * dmin_(R.y.r, p.step_rcap);
+    const double sigma = (R.y.r * R.y.r) + ((p.a2 * R.y.u) * R.y.u);
+    const double h = hh / sigma;
+    Yd yn = rk4(R.y, h, R.c, rhs(R.y, R.c));
+    ++R.steps;
+    if ((R.y.u * yn.u) < 0.0) {
+      const Yd yc = bisect_equator<0>(p, R.c, R.y, h);
+      if (on_crossing(p, o, R, yc)) return 1;
+    }
+    project(yn, R.c);
+    R.y = yn;
+    return -1;
+  } else {
+    const long long max_attempts = 4LL * p.max_steps + 64;
+    if (R.steps >= p.max_steps || R.attempts >= max_attempts) return 3;
+    if (R.y.r <= p.r_hor) return 0;
+    if (R.y.r >= p.r_esc) return 2;
+    ++R.attempts;
+    const DPRes d = dp45(R.y, R.h, R.c, R.k1, p.rtol, p.atol, true);
+    if (d.err <= 1.0) {
+      ++R.steps;
+      bool stop = false;
+      if ((R.y.u * d.y5.u) < 0.0) {
+        const Yd yc = bisect_equator<1>(p, R.c, R.y, R.h);
+        stop = on_crossing(p, o, R, yc);
+      }
+      R.y = d.y5;
+      R.k1 = d.k7;
+      project(R.y, R.c);
+      R.k1.r = R.y.pr;  // projection moves only the momenta
+      R.k1.u = R.y.pu;
+      R.h = R.h * step_factor(d.err, true);
+      if (stop) return 1;
+    } else {
+      R.h = R.h * step_factor(d.err, false);
+    }
+    return -1;
+  }
+}
+
+template <int INTEG>
+__global__ void __launch_bounds__(128) k_trace_image_fp64(const BhkImageParams p, const BhkImageOut o,
+                                                          unsigned long long *__restrict__ counter) {
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned lanemask_lt = (1u << lane) - 1u;
+  RayFp64 R;
+  bool active = false;
+  bool exhausted = false;
+  for (;;) {
+    const unsigned need = __ballot_sync(kFull, !active && !exhausted);
+    if (need) {
+      const int leader = __ffs(need) - 1;
+      unsigned long long base = 0;
+      if ((int)lane == leader) base = atomicAdd(counter, (unsigned long long)__popc(need));
+      base = __shfl_sync(kFull, base, leader);
+      if (!active && !exhausted) {
+        const unsigned long long mine = base + (unsigned long long)__popc(need & lanemask_lt);
+        if (mine < (unsigned long long)p.n_pix) {
+          init_ray(p, (long long)mine, R);
+          active = true;
+        } else {
+          exhausted = true;
+        }
+      }
+    }
+    if (!__any_sync(kFull, active)) break;
+    if (active) {
+      const int cls = iterate<INTEG>(p, o, R);
+      if (cls >= 0) {
+        finish(p, o, R, cls);
+        active = false;
+      }
+    }
+  }
+}
+
+}  // namespace bhk
+
+namespace {
+thread_local char g_err[256] = {0};
+int set_err(cudaError_t e, const char *what) {
+  snprintf(g_err, sizeof(g_err), "%s: %s", what, cudaGetErrorString(e));
+  return -1;
+}
+}  // namespace
+
+extern "C" const char *bhk_last_error(void) { return g_err; }
+
+extern "C" int bhk_trace_image_fp64(const BhkImageParams *p, const BhkImageOut *o, unsigned long long *counter,
+                                    BhkLaunch launch, void *stream) {
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return set_err(e, "work-counter reset");
+  if (p->integrator == 0)
+    bhk::k_trace_image_fp64<0><<<launch.grid, launch.block, 0, s>>>(*p, *o, counter);
+  else
+    bhk::k_trace_image_fp64<1><<<launch.grid, launch.block, 0, s>>>(*p, *o, counter);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(e, "k_trace_image_fp64 launch");
+  return 0;
+}
+
+extern "C" int bhk_trace_image_fp64_occupancy(int integrator, int block, int *blocks_per_sm) {
+  cudaError_t e = (integrator == 0)
+                      ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhk::k_trace_image_fp64<0>,
+                                                                      block, 0)
+                      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhk::k_trace_image_fp64<1>,
+                                                                      block, 0);
+  if (e != cudaSuccess) return set_err(e, "occupancy query");
+  return 0;
+}

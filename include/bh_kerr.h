@@ -1,0 +1,254 @@
+/*
+ * bh_kerr.h - C ABI of the B200 Kerr null-geodesic tracer.
+ *
+ * Plain C (C99) header: no C++ types, no CUDA types, no torch types. Every
+ * pointer is either a device pointer (functions without a _host suffix) or a
+ * host pointer (functions with a _host suffix). All functions return 0 on
+ * success and -1 on error; the message of the last error on the calling
+ * thread is available from bh_last_error().
+ *
+ * Two families of entry points live here:
+ *
+ *  1. Batched drop-ins for the reference's src/physics Kerr API (CGS units,
+ *     mass in grams, spin parameter a in cm, exactly as the reference):
+ *       bh_kerr_potentials      <- physics::kerrPotentials   (src/physics/kerr.cpp:69-97)
+ *       bh_kerr_step_mino       <- physics::kerrStepMino     (src/physics/kerr.cpp:99-134)
+ *       bh_kerr_trace_rays      <- physics::KerrRaytracer::trace (src/physics/raytracer.h:324-378)
+ *     These reproduce the reference's first-order, sign-flip Mino-time scheme
+ *     operation for operation (FP64, no FMA contraction).
+ *
+ *  2. The image-plane tracer (geometric units, M = 1):
+ *       bh_kerr_trace_image / bh_kerr_trace_image_host
+ *     Per-pixel backward null geodesics from a distant observer, classified as
+ *     captured / disk / escaped, with disk-hit radius, azimuth, redshift g,
+ *     Novikov-Thorne flux and intensity. Integrates the reference's Mino-time
+ *     potentials (kerr.cpp:69-97) in second-order form.
+ */
+#ifndef BH_KERR_H
+#define BH_KERR_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BH_KERR_ABI_VERSION 1
+
+/* ---------------------------------------------------------------------------
+ * Common
+ * ------------------------------------------------------------------------- */
+
+/** Message of the last failed call on this thread ("" if none). Never NULL. */
+const char *bh_last_error(void);
+
+/** ABI version of the loaded library (BH_KERR_ABI_VERSION it was built with). */
+int bh_abi_version(void);
+
+/* ---------------------------------------------------------------------------
+ * 1. Reference src/physics API, batched on the GPU (CGS units)
+ * ------------------------------------------------------------------------- */
+
+/** Status codes of physics::RayStatus (src/physics/raytracer.h:46-52). */
+enum BH_RayStatus {
+    BH_STATUS_PROPAGATING = 0,
+    BH_STATUS_ESCAPED = 1,
+    BH_STATUS_CAPTURED = 2,
+    BH_STATUS_HIT_DISK = 3,
+    BH_STATUS_MAX_STEPS = 4
+};
+
+/**
+ * Structure-of-arrays view of n Kerr geodesic states
+ * (physics::KerrGeodesicState, src/physics/kerr.h:381-388). Device pointers,
+ * each of length n. sign_r / sign_theta hold +1.0 or -1.0.
+ */
+typedef struct BH_KerrStateSoA {
+    double *r;
+    double *theta;
+    double *phi;
+    double *t;
+    double *sign_r;
+    double *sign_theta;
+} BH_KerrStateSoA;
+
+/**
+ * Structure-of-arrays view of n constants of motion
+ * (physics::KerrGeodesicConsts, src/physics/kerr.h:362-366). Device pointers.
+ */
+typedef struct BH_KerrConstsSoA {
+    const double *e;
+    const double *lz;
+    const double *q;
+} BH_KerrConstsSoA;
+
+/**
+ * Batched physics::kerrPotentials (src/physics/kerr.cpp:69-97).
+ * out_* are device arrays of length n; any of them may be NULL.
+ */
+int bh_kerr_potentials(int64_t n, const double *r, const double *theta,
+                       double mass, double a, BH_KerrConstsSoA consts,
+                       double *out_r_pot, double *out_dr_pot,
+                       double *out_theta_pot, double *out_dtheta_pot,
+                       void *stream);
+
+/**
+ * Batched physics::kerrStepMino (src/physics/kerr.cpp:99-134): one Mino-time
+ * RK4 step of each state, in place. dlam is a device array of length n, or
+ * NULL to use dlam_scalar for every state.
+ */
+int bh_kerr_step_mino(int64_t n, BH_KerrStateSoA state, double mass, double a,
+                      BH_KerrConstsSoA consts, const double *dlam,
+                      double dlam_scalar, void *stream);
+
+/**
+ * Parameters of physics::KerrRaytracer (src/physics/raytracer.h:309-399).
+ * bh_kerr_raytracer_defaults() fills them exactly as the reference's
+ * constructor does: horizon = outer horizon (or r_s if not finite/positive),
+ * escape radius = 1000 r_s, step = 0.02 r_s, 10000 steps.
+ */
+typedef struct BH_KerrRaytracerParams {
+    double mass;          /**< black-hole mass [g] */
+    double a;             /**< spin parameter [cm], already clamped like physics::Kerr */
+    double r_horizon;     /**< capture when r <= 1.001 * r_horizon */
+    double r_escape;      /**< escape when r >= r_escape */
+    double step_size;     /**< Mino-time step dlam */
+    int32_t max_steps;
+    int32_t reserved;
+} BH_KerrRaytracerParams;
+
+/** Fill params as physics::KerrRaytracer(mass, spinParam) does. */
+int bh_kerr_raytracer_defaults(double mass, double spin_param,
+                               BH_KerrRaytracerParams *out_params);
+
+/**
+ * Batched physics::KerrRaytracer::trace (src/physics/raytracer.h:324-378).
+ * initial: n start states (not modified). Outputs (device, length n, any may
+ * be NULL): status (BH_RayStatus), steps taken, total distance, final
+ * (r, theta, phi) and the redshift 1 + kerrRedshift(r_final, theta_final).
+ */
+int bh_kerr_trace_rays(int64_t n, BH_KerrStateSoA initial, BH_KerrConstsSoA consts,
+                       const BH_KerrRaytracerParams *params,
+                       int32_t *out_status, int32_t *out_steps,
+                       double *out_total_distance, double *out_r,
+                       double *out_theta, double *out_phi, double *out_redshift,
+                       void *stream);
+
+/* ---------------------------------------------------------------------------
+ * 2. Image-plane tracer (geometric units G = c = M = 1)
+ * ------------------------------------------------------------------------- */
+
+/** Per-pixel termination class. */
+enum BH_PixelClass {
+    BH_CLASS_CAPTURED = 0,  /**< r <= horizon_factor * r_+ */
+    BH_CLASS_DISK = 1,      /**< stopped by the thin disk (opaque, or last allowed crossing) */
+    BH_CLASS_ESCAPED = 2,   /**< r >= escape_factor * r_obs */
+    BH_CLASS_MAX_STEPS = 3  /**< step budget exhausted */
+};
+
+enum BH_Integrator {
+    BH_INTEGRATOR_RK4 = 0,  /**< fixed affine step h = step_coeff * min(r, step_rcap), dsigma = h / Sigma */
+    BH_INTEGRATOR_DP45 = 1  /**< Dormand-Prince 5(4), rtol/atol on (r, cos theta, phi, p_r, p_u) */
+};
+
+enum BH_Precision {
+    BH_PRECISION_FP64 = 0,  /**< every operation in FP64 */
+    BH_PRECISION_MIXED = 1  /**< FP32 right-hand sides with compensated FP32 state; FP64 set-up,
+                                 horizon-approach and disk-crossing steps */
+};
+
+/**
+ * Meaning of the Carter constant inside the potentials.
+ * REFERENCE: R(r) and Theta(theta) both take the reference's single q
+ *   (kerr.cpp:81-89, Theta = q + a^2 cos^2 - Lz^2 / sin^2); the image-plane
+ *   set-up uses q = eta + lambda^2 so that Theta matches the camera ray, the
+ *   convention of the reference's GPU set-up (src/cuda/device_physics.cuh:381-390).
+ * CARTER: the textbook Carter potentials (R with eta, Theta with eta + lambda^2).
+ */
+enum BH_PotentialForm {
+    BH_POTENTIAL_REFERENCE = 0,
+    BH_POTENTIAL_CARTER = 1
+};
+
+#define BH_MAX_CROSSINGS 3
+
+/** One image-plane scene. Pixel (i, j) looks at the centre of its cell:
+ *  alpha = alpha_min + (i + 0.5) (alpha_max - alpha_min) / width, same for beta/height. */
+typedef struct BH_KerrScene {
+    double spin;            /**< a/M, |spin| < 1 */
+    double r_obs;           /**< observer radius [M] */
+    double theta_obs;       /**< observer inclination [rad], in (0, pi) */
+    double alpha_min, alpha_max;
+    double beta_min, beta_max;
+    int32_t width, height;
+    int32_t integrator;     /**< BH_Integrator */
+    int32_t precision;      /**< BH_Precision */
+    int32_t potential_form; /**< BH_PotentialForm */
+    int32_t max_crossings;  /**< 1 = opaque disk; 2..3 = transparent disk, stop at that crossing */
+    int32_t max_steps;      /**< accepted-step budget per ray */
+    int32_t reserved0;
+    double step_coeff;      /**< RK4: affine h = step_coeff * min(r, step_rcap); DP45: first trial step */
+    double step_rcap;
+    double rtol, atol;      /**< DP45 tolerances */
+    double horizon_factor;  /**< capture radius = horizon_factor * r_+ (1.001) */
+    double escape_factor;   /**< escape radius = escape_factor * r_obs (1.01) */
+    double disk_r_in;       /**< <= 0 selects the prograde ISCO (physics::kerrIscoRadius) */
+    double disk_r_out;      /**< outer disk edge [M] (30) */
+} BH_KerrScene;
+
+/** Fill a scene with the defaults of the 256x256 a=0.9 disk scene
+ *  (r_obs = 1000, theta_obs = 60 deg, alpha, beta in [-12, 12], RK4,
+ *  h = 0.02 min(r, 20), 20000 steps, opaque disk r_isco..30). */
+void bh_kerr_scene_defaults(BH_KerrScene *scene);
+
+/**
+ * Per-pixel outputs, structure of arrays, n = width * height, row-major
+ * (pixel = j * width + i). Crossing-indexed arrays hold max_crossings planes
+ * of n values (plane k at offset k * n). Any pointer may be NULL.
+ * Values of crossings that did not happen are 0.
+ */
+typedef struct BH_KerrImageOut {
+    int32_t *cls;        /**< [n] BH_PixelClass */
+    int32_t *steps;      /**< [n] accepted integration steps */
+    int32_t *n_cross;    /**< [n] disk crossings recorded */
+    double *r_hit;       /**< [max_crossings * n] crossing radius [M] */
+    double *phi_hit;     /**< [max_crossings * n] crossing azimuth [rad], observer at phi = 0 */
+    double *g;           /**< [max_crossings * n] redshift g = E_obs / E_emit (Keplerian emitter) */
+    double *flux;        /**< [n] Novikov-Thorne normalised flux at the first crossing */
+    double *intensity;   /**< [n] sum_k g_k^4 (r_in / r_k)^3 */
+    double *theta_inf;   /**< [n] polar angle at escape [rad] */
+    double *phi_inf;     /**< [n] azimuth at escape [rad] */
+} BH_KerrImageOut;
+
+/** Check a scene; returns 0 if valid, else -1 with bh_last_error() set. */
+int bh_kerr_scene_validate(const BH_KerrScene *scene);
+
+/**
+ * Trace every pixel of the scene on the current CUDA device.
+ * out holds DEVICE pointers. stream is a cudaStream_t (NULL = legacy default).
+ * Asynchronous with respect to the host.
+ */
+int bh_kerr_trace_image(const BH_KerrScene *scene, const BH_KerrImageOut *out, void *stream);
+
+/**
+ * Same as bh_kerr_trace_image with HOST output pointers: device buffers are
+ * allocated, the trace runs, the results are copied back, and the call
+ * returns after the copies have completed.
+ */
+int bh_kerr_trace_image_host(const BH_KerrScene *scene, const BH_KerrImageOut *out_host);
+
+/** Launch configuration of the image tracer (0 = automatic). */
+int bh_kerr_set_launch(int32_t block_threads, int32_t ctas_per_sm);
+
+/**
+ * Measured FMA-pipe peak of the current device in TFLOP/s (fp64 != 0: FP64,
+ * else FP32): best of `repeats` launches of independent FMA chains covering
+ * every SM. The roofline figures of the tracer divide by this number.
+ */
+int bh_measure_fma_peak(int fp64, int repeats, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BH_KERR_H */

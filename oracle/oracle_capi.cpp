@@ -1,0 +1,264 @@
+// oracle_capi.cpp - extern "C" surface of the CPU oracle (test infrastructure
+// only: loaded by tests/, __graft_entry__.smoke() and bench.py's CPU legs).
+//
+// Wraps kerr_oracle.hpp for ctypes: batched reference stepper (Part A),
+// image tracer over any pixel subset with std::thread workers (Part B),
+// the FLOP count per step with the counting scalar, and a __float128 run of
+// the stepper.
+#include <atomic>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#include "../include/bh_kerr.h"
+#include "kerr_oracle.hpp"
+
+namespace {
+
+bho::Scene to_scene(const BH_KerrScene *s) {
+  bho::Scene o{};
+  o.spin = s->spin;
+  o.r_obs = s->r_obs;
+  o.theta_obs = s->theta_obs;
+  o.alpha_min = s->alpha_min;
+  o.alpha_max = s->alpha_max;
+  o.beta_min = s->beta_min;
+  o.beta_max = s->beta_max;
+  o.width = s->width;
+  o.height = s->height;
+  o.integrator = s->integrator;
+  o.potential_form = s->potential_form;
+  o.max_crossings = s->max_crossings;
+  o.max_steps = s->max_steps;
+  o.step_coeff = s->step_coeff;
+  o.step_rcap = s->step_rcap;
+  o.rtol = s->rtol;
+  o.atol = s->atol;
+  o.horizon_factor = s->horizon_factor;
+  o.escape_factor = s->escape_factor;
+  o.disk_r_in = s->disk_r_in;
+  o.disk_r_out = s->disk_r_out;
+  return o;
+}
+
+template <class T>
+void store(const BH_KerrImageOut *out, int64_t idx, int64_t n, int maxc, const bho::PixelResult<T> &p) {
+  if (out->cls) out->cls[idx] = p.cls;
+  if (out->steps) out->steps[idx] = p.steps;
+  if (out->n_cross) out->n_cross[idx] = p.n_cross;
+  for (int k = 0; k < maxc; ++k) {
+    if (out->r_hit) out->r_hit[k * n + idx] = double(p.r_hit[k]);
+    if (out->phi_hit) out->phi_hit[k * n + idx] = double(p.phi_hit[k]);
+    if (out->g) out->g[k * n + idx] = double(p.g[k]);
+  }
+  if (out->flux) out->flux[idx] = double(p.flux);
+  if (out->intensity) out->intensity[idx] = double(p.intensity);
+  if (out->theta_inf) out->theta_inf[idx] = double(p.theta_inf);
+  if (out->phi_inf) out->phi_inf[idx] = double(p.phi_inf);
+}
+
+template <class F> void parallel_for(int64_t n, int threads, F &&f) {
+  if (threads <= 1 || n < 2) {
+    for (int64_t i = 0; i < n; ++i) f(i);
+    return;
+  }
+  std::atomic<int64_t> next{0};
+  const int64_t chunk = 16;
+  std::vector<std::thread> pool;
+  pool.reserve(threads);
+  for (int t = 0; t < threads; ++t) {
+    pool.emplace_back([&]() {
+      for (;;) {
+        const int64_t b = next.fetch_add(chunk);
+        if (b >= n) break;
+        const int64_t e = std::min(n, b + chunk);
+        for (int64_t i = b; i < e; ++i) f(i);
+      }
+    });
+  }
+  for (auto &th : pool) th.join();
+}
+
+}  // namespace
+
+extern "C" {
+
+// Trace pixels [pix_index[0..n)] of the scene (or pixels 0..n-1 when pix_index
+// is NULL). Output arrays are indexed 0..n-1 (crossing planes have stride n).
+int bho_trace_pixels(const BH_KerrScene *scene, int64_t n, const int64_t *pix_index,
+                     const BH_KerrImageOut *out, int threads) {
+  const bho::Scene s = to_scene(scene);
+  const auto d = bho::derive<double>(s);
+  const int maxc = std::max(1, std::min(3, int(s.max_crossings)));
+  parallel_for(n, threads, [&](int64_t i) {
+    const int64_t pix = pix_index ? pix_index[i] : i;
+    double alpha, beta;
+    bho::pixel_alpha_beta(s, pix, alpha, beta);
+    const auto p = bho::trace_pixel<double>(s, d, alpha, beta);
+    store(out, i, n, maxc, p);
+  });
+  return 0;
+}
+
+// Same at explicit image-plane coordinates.
+int bho_trace_alpha_beta(const BH_KerrScene *scene, int64_t n, const double *alpha, const double *beta,
+                         const BH_KerrImageOut *out, int threads) {
+  const bho::Scene s = to_scene(scene);
+  const auto d = bho::derive<double>(s);
+  const int maxc = std::max(1, std::min(3, int(s.max_crossings)));
+  parallel_for(n, threads, [&](int64_t i) {
+    const auto p = bho::trace_pixel<double>(s, d, alpha[i], beta[i]);
+    store(out, i, n, maxc, p);
+  });
+  return 0;
+}
+
+// Same in long double (x87 80-bit) for rounding checks.
+int bho_trace_alpha_beta_ld(const BH_KerrScene *scene, int64_t n, const double *alpha, const double *beta,
+                            const BH_KerrImageOut *out, int threads) {
+  const bho::Scene s = to_scene(scene);
+  const auto d = bho::derive<long double>(s);
+  const int maxc = std::max(1, std::min(3, int(s.max_crossings)));
+  parallel_for(n, threads, [&](int64_t i) {
+    const auto p = bho::trace_pixel<long double>(s, d, (long double)alpha[i], (long double)beta[i]);
+    store(out, i, n, maxc, p);
+  });
+  return 0;
+}
+
+// FLOPs of one traced pixel with the counting scalar. counts[0..6] receive
+// add, mul, div, sqrt, trig, pow, cmp; steps[0] the accepted steps.
+int bho_count_ops(const BH_KerrScene *scene, double alpha, double beta, int64_t *counts, int32_t *steps) {
+  const bho::Scene s = to_scene(scene);
+  const auto d = bho::derive<bho::Counted>(s);
+  bho::g_counts = bho::OpCounts{};
+  const auto p = bho::trace_pixel<bho::Counted>(s, d, bho::Counted(alpha), bho::Counted(beta));
+  const bho::OpCounts c = bho::g_counts;
+  counts[0] = c.add;
+  counts[1] = c.mul;
+  counts[2] = c.div;
+  counts[3] = c.sqrt;
+  counts[4] = c.trig;
+  counts[5] = c.pow;
+  counts[6] = c.cmp;
+  steps[0] = p.steps;
+  return p.cls;
+}
+
+// FLOPs of one right-hand-side evaluation and one RK4 step (no bisection):
+// out[0..6] for the RHS, out[7..13] for the step.
+int bho_count_step_ops(double spin, double alpha, double beta, int64_t *out) {
+  bho::RayConsts<bho::Counted> c{};
+  c.a = spin;
+  c.lam = alpha;
+  c.qTh = beta * beta + alpha * alpha;
+  c.qR = c.qTh;
+  c.K = c.qR + (c.lam - c.a) * (c.lam - c.a);
+  bho::Y<bho::Counted> y{bho::Counted(10.0), bho::Counted(0.3), bho::Counted(0.0), bho::Counted(-50.0),
+                         bho::Counted(1.0)};
+  auto dump = [&](int64_t *o) {
+    o[0] = bho::g_counts.add; o[1] = bho::g_counts.mul; o[2] = bho::g_counts.div; o[3] = bho::g_counts.sqrt;
+    o[4] = bho::g_counts.trig; o[5] = bho::g_counts.pow; o[6] = bho::g_counts.cmp;
+  };
+  bho::g_counts = bho::OpCounts{};
+  (void)bho::img_rhs(y, c);
+  dump(out);
+  bho::Scene s{};
+  s.step_coeff = 0.02;
+  s.step_rcap = 20.0;
+  bho::g_counts = bho::OpCounts{};
+  const bho::Counted h = bho::mino_step(s, y, c.a);
+  const bho::PolyRhs<bho::Counted> f{c};
+  (void)bho::img_rk4(y, h, f, f(y));
+  (void)(y.r <= bho::Counted(1.0));  // horizon, escape and crossing tests
+  (void)(y.r >= bho::Counted(1.0));
+  (void)(y.u * y.u < bho::Counted(0.0));
+  dump(out + 7);
+  return 0;
+}
+
+// ----- Part A: batched reference stepper -----------------------------------
+
+int bho_kerr_potentials(int64_t n, const double *r, const double *theta, double mass, double a,
+                        const double *e, const double *lz, const double *q, double *rpot, double *drpot,
+                        double *thpot, double *dthpot) {
+  for (int64_t i = 0; i < n; ++i) {
+    const bho::Consts<double> c{e[i], lz[i], q[i]};
+    const auto p = bho::kerr_potentials<double>(r[i], theta[i], mass, a, c);
+    if (rpot) rpot[i] = p.rPot;
+    if (drpot) drpot[i] = p.dRdr;
+    if (thpot) thpot[i] = p.thetaPot;
+    if (dthpot) dthpot[i] = p.dThetadtheta;
+  }
+  return 0;
+}
+
+// state arrays are updated in place: r, theta, phi, t, sign_r, sign_theta.
+int bho_kerr_step_mino(int64_t n, double *r, double *theta, double *phi, double *t, double *sr, double *sth,
+                       double mass, double a, const double *e, const double *lz, const double *q,
+                       const double *dlam, double dlam_scalar, int32_t nsteps) {
+  for (int64_t i = 0; i < n; ++i) {
+    bho::State<double> s{r[i], theta[i], phi[i], t[i], sr[i], sth[i]};
+    const bho::Consts<double> c{e[i], lz[i], q[i]};
+    const double h = dlam ? dlam[i] : dlam_scalar;
+    for (int32_t k = 0; k < nsteps; ++k) s = bho::kerr_step_mino<double>(s, mass, a, c, h);
+    r[i] = s.r; theta[i] = s.theta; phi[i] = s.phi; t[i] = s.t; sr[i] = s.signR; sth[i] = s.signTheta;
+  }
+  return 0;
+}
+
+// Same stepper in __float128; inputs/outputs in double.
+int bho_kerr_step_mino_f128(int64_t n, double *r, double *theta, double *phi, double *t, const double *sr,
+                            const double *sth, double mass, double a, const double *e, const double *lz,
+                            const double *q, double dlam, int32_t nsteps) {
+  using F = bho::f128;
+  for (int64_t i = 0; i < n; ++i) {
+    bho::State<F> s{F(r[i]), F(theta[i]), F(phi[i]), F(t[i]), F(sr[i]), F(sth[i])};
+    const bho::Consts<F> c{F(e[i]), F(lz[i]), F(q[i])};
+    for (int32_t k = 0; k < nsteps; ++k) s = bho::kerr_step_mino<F>(s, F(mass), F(a), c, F(dlam));
+    r[i] = double(s.r); theta[i] = double(s.theta); phi[i] = double(s.phi); t[i] = double(s.t);
+  }
+  return 0;
+}
+
+int bho_kerr_trace_rays(int64_t n, const double *r, const double *theta, const double *phi, const double *t,
+                        const double *sr, const double *sth, const double *e, const double *lz,
+                        const double *q, double mass, double a, double r_horizon, double r_escape,
+                        double step, int32_t max_steps, int32_t *status, int32_t *steps, double *dist,
+                        double *rf, double *thf, double *phf, double *redshift, int threads) {
+  parallel_for(n, threads, [&](int64_t i) {
+    const bho::State<double> s{r[i], theta[i], phi[i], t[i], sr[i], sth[i]};
+    const bho::Consts<double> c{e[i], lz[i], q[i]};
+    const auto res = bho::kerr_trace<double>(s, c, mass, a, r_horizon, r_escape, step, max_steps);
+    if (status) status[i] = res.status;
+    if (steps) steps[i] = res.steps;
+    if (dist) dist[i] = res.totalDistance;
+    if (rf) rf[i] = res.r;
+    if (thf) thf[i] = res.theta;
+    if (phf) phf[i] = res.phi;
+    if (redshift) redshift[i] = res.redshift;
+  });
+  return 0;
+}
+
+// Known answers of kerr.h for geometric mass m: out = {r_plus, r_minus,
+// isco_pro, isco_retro, r_ph_pro, r_ph_retro, nt_isco, nt_eta_flux_peak}.
+int bho_kerr_radii(double m, double a, double *out) {
+  out[0] = bho::outer_horizon_geom(m, a);
+  const double disc = m * m - a * a;
+  out[1] = disc < 0 ? NAN : m - std::sqrt(disc);
+  out[2] = bho::isco_geom(m, a, true);
+  out[3] = bho::isco_geom(m, a, false);
+  out[4] = bho::photon_orbit_prograde_geom(m, a);
+  out[5] = bho::photon_orbit_retrograde_geom(m, a);
+  out[6] = bho::nt_isco(a / m);
+  out[7] = bho::nt_normalized_flux(1.5 * bho::nt_isco(a / m), a / m);
+  return 0;
+}
+
+double bho_nt_normalized_flux(double r, double a_star) { return bho::nt_normalized_flux(r, a_star); }
+double bho_nt_radiative_efficiency(double a_star) { return bho::nt_radiative_efficiency(a_star); }
+double bho_disk_g(double r, double a, double lam) { return bho::disk_g<double>(r, a, lam); }
+double bho_unit_mass(void) { return bho::kUnitMass; }
+
+}  // extern "C"
