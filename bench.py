@@ -91,6 +91,14 @@ class ClockSampler:
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
+    def wait_first_sample(self, timeout_s: float = 20.0) -> None:
+        """Block until nvidia-smi has printed a sample, so that its start-up
+        (NVML initialisation) is over before the timed region begins."""
+        t0 = time.perf_counter()
+        while self.proc is not None and not self.lines and time.perf_counter() - t0 < timeout_s:
+            time.sleep(0.05)
+        self.lines.clear()
+
     def stop(self) -> dict:
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
@@ -149,15 +157,15 @@ def run_ours(args, rank: int, world: int, dist):
         if dist is not None:
             dist.barrier()
 
+    sampler = ClockSampler(dev.index if "CUDA_VISIBLE_DEVICES" not in os.environ else 0)
+    sampler.start()
+    sampler.wait_first_sample()
     for _ in range(args.warmup):
         render()
     torch.cuda.synchronize(dev)
     barrier()
     torch.cuda.synchronize(dev)
-
-    sampler = ClockSampler(dev.index if "CUDA_VISIBLE_DEVICES" not in os.environ else 0)
-    sampler.start()
-    time.sleep(0.3)
+    sampler.lines.clear()
     per_launch = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                    for _ in scenes] for _ in range(args.steps)]
     t0 = torch.cuda.Event(enable_timing=True)
