@@ -182,6 +182,8 @@ def _declare(lib: C.CDLL) -> None:
     lib.bh_kerr_trace_image_host.argtypes = [C.POINTER(KerrScene), C.POINTER(KerrImageOut)]
     lib.bh_kerr_set_launch.restype = C.c_int
     lib.bh_kerr_set_launch.argtypes = [i32, i32]
+    lib.bh_kerr_trace_image_host_noalloc.restype = C.c_int
+    lib.bh_kerr_trace_image_host_noalloc.argtypes = [C.POINTER(KerrScene), C.POINTER(KerrImageOut), vp]
     lib.bh_measure_fma_peak.restype = C.c_int
     lib.bh_measure_fma_peak.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
 

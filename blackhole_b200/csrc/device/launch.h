@@ -62,6 +62,12 @@ int bhk_kerr_trace_rays(int64_t n, BhkStateSoA init, BhkConstsSoA c, double mass
                         double r_escape, double step, int32_t max_steps, int32_t *status, int32_t *steps,
                         double *dist, double *rf, double *thf, double *phf, double *redshift, void *stream);
 
+// Host layer (capi.cpp): scene validation + kernel parameters + persistent
+// grid shape, allocating nothing; and setting the thread's last error.
+struct BH_KerrScene;
+int bhh_prepare_image_launch(const struct BH_KerrScene *scene, BhkImageParams *p, BhkLaunch *L);
+int bhh_fail(const char *msg);
+
 // FMA-throughput probe (probe.cu).
 int bhk_fma_probe(int fp64, int iters, int repeats, double *tflops);
 

@@ -169,23 +169,42 @@ static BhkImageParams make_params(const BH_KerrScene *s) {
   return p;
 }
 
-int bh_kerr_trace_image(const BH_KerrScene *scene, const BH_KerrImageOut *out, void *stream) {
+// Validates the scene and fills the kernel parameters and the persistent
+// grid shape (SM count x resident CTAs per SM, capped by the pixel count).
+// Allocates nothing. Returns 0, or -1 with the error message set.
+int bhh_prepare_image_launch(const BH_KerrScene *scene, BhkImageParams *p, BhkLaunch *L) {
   if (bh_kerr_scene_validate(scene) != 0) return -1;
-  if (!out) return fail("output descriptor is NULL");
-  const BhkImageParams p = make_params(scene);
-  if (p.n_pix == 0) return 0;
+  *p = make_params(scene);
+  *L = BhkLaunch{0, 0};
+  if (p->n_pix == 0) return 0;
   if (scene->precision != BH_PRECISION_FP64) return fail("mixed precision tracer not built in this library");
-  DeviceScratch *ds = nullptr;
-  if (device_scratch(&ds) != 0) return -1;
+  int dev = 0, sms = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute(SM count)");
   const int block = g_block_override ? g_block_override : 128;
   int per_sm = 0;
-  if (bhk_trace_image_fp64_occupancy(p.integrator, block, &per_sm) != 0)
-    return fail("%s", bhk_last_error());
+  if (bhk_trace_image_fp64_occupancy(p->integrator, block, &per_sm) != 0) return fail("%s", bhk_last_error());
   if (g_ctas_per_sm_override) per_sm = std::min(per_sm, g_ctas_per_sm_override);
   if (per_sm < 1) return fail("kernel does not fit on an SM at %d threads per CTA", block);
-  const int64_t full = int64_t(ds->sms) * per_sm;
-  const int64_t need = (p.n_pix + block - 1) / block;
-  BhkLaunch L{int32_t(std::max<int64_t>(1, std::min(full, need))), block};
+  const int64_t full = int64_t(sms) * per_sm;
+  const int64_t need = (p->n_pix + block - 1) / block;
+  *L = BhkLaunch{int32_t(std::max<int64_t>(1, std::min(full, need))), block};
+  return 0;
+}
+
+// Records an error message from the device layer (noalloc.cu).
+int bhh_fail(const char *msg) { return fail("%s", msg); }
+
+int bh_kerr_trace_image(const BH_KerrScene *scene, const BH_KerrImageOut *out, void *stream) {
+  if (!out) return fail("output descriptor is NULL");
+  BhkImageParams p;
+  BhkLaunch L;
+  if (bhh_prepare_image_launch(scene, &p, &L) != 0) return -1;
+  if (p.n_pix == 0) return 0;
+  DeviceScratch *ds = nullptr;
+  if (device_scratch(&ds) != 0) return -1;
   const BhkImageOut o{out->cls,   out->steps,     out->n_cross,   out->r_hit,     out->phi_hit,
                       out->g,     out->flux,      out->intensity, out->theta_inf, out->phi_inf};
   if (bhk_trace_image_fp64(&p, &o, ds->counter, L, stream) != 0) return fail("%s", bhk_last_error());

@@ -109,6 +109,27 @@ def trace_image_host(s: KerrScene, fields=None) -> dict[str, np.ndarray]:
     return outs
 
 
+def trace_image_host_noalloc(s: KerrScene, fields=None, stream=None) -> dict[str, np.ndarray]:
+    """Trace into host arrays through bh_kerr_trace_image_host_noalloc.
+
+    Allocates no device memory: the outputs are staged in the library's fixed
+    32 MiB device scratch, so images whose outputs exceed it are rejected.
+    ``stream``: a torch.cuda.Stream, a raw cudaStream_t, or None for the
+    legacy default stream.
+    """
+    n = s.width * s.height
+    mc = s.max_crossings
+    dt = {"cls": np.int32, "steps": np.int32, "n_cross": np.int32}
+    fields = fields or _abi.OUT_FIELDS
+    outs = {}
+    for k in fields:
+        shape = (mc, n) if k in _abi.PLANE_FIELDS else (n,)
+        outs[k] = np.zeros(shape, dt.get(k, np.float64))
+    sp = None if stream is None else (stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+    check(_abi.load_library().bh_kerr_trace_image_host_noalloc(C.byref(s), C.byref(_out_struct(outs)), sp))
+    return outs
+
+
 def set_launch(block_threads: int = 0, ctas_per_sm: int = 0) -> None:
     """Override the persistent-grid shape (0 = automatic)."""
     check(_abi.load_library().bh_kerr_set_launch(block_threads, ctas_per_sm))

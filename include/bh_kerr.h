@@ -237,6 +237,39 @@ int bh_kerr_trace_image(const BH_KerrScene *scene, const BH_KerrImageOut *out, v
  */
 int bh_kerr_trace_image_host(const BH_KerrScene *scene, const BH_KerrImageOut *out_host);
 
+/**
+ * Size of the fixed device scratch of bh_kerr_trace_image_host_noalloc:
+ * 32 MiB, resident on every GPU that loads the library until process exit.
+ */
+#define BH_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
+
+/**
+ * Same as bh_kerr_trace_image_host, but allocates nothing. (It has no
+ * counterpart in the reference.)
+ *
+ * For callers that cannot allocate device memory: a plug-in running inside a
+ * host application that owns the GPU's memory (it reserves the device pool
+ * up front, or forbids cudaMalloc/cudaFree on its render thread because they
+ * can synchronise the whole device and stall its frame), or a real-time loop
+ * that must not block on an allocation. The caller passes the scene and HOST
+ * output buffers exactly as for bh_kerr_trace_image_host; the work counter
+ * and the device copies of the outputs live in one fixed device array of
+ * BH_NOALLOC_SCRATCH_BYTES. A call whose requested outputs (each rounded up
+ * to 256 bytes) plus 256 bytes exceed that size is rejected with -1 and a
+ * message; with every field and one disk crossing that is about 490,000
+ * pixels (700 x 700).
+ *
+ * stream: cudaStream_t to run on (NULL = legacy default stream); the call
+ * returns after that stream has finished the copies. It creates no stream
+ * and calls no cudaMalloc, cudaFree or allocating library routine.
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress, which also loads the library's device code); make
+ * that first call before any stream capture. Every call shares the array
+ * and overwrites the previous call's contents: calls whose GPU work overlaps
+ * race and must be serialised by the caller.
+ */
+int bh_kerr_trace_image_host_noalloc(const BH_KerrScene *scene, const BH_KerrImageOut *out_host, void *stream);
+
 /** Launch configuration of the image tracer (0 = automatic). */
 int bh_kerr_set_launch(int32_t block_threads, int32_t ctas_per_sm);
 

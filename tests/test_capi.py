@@ -19,6 +19,7 @@ def declared_functions(path: Path) -> list[str]:
     text = path.read_text()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     text = re.sub(r"//[^\n]*", "", text)
+    text = re.sub(r"^\s*#[^\n]*", "", text, flags=re.M)
     text = re.sub(r"typedef\s+struct\s*\w*\s*\{.*?\}\s*\w+\s*;", "", text, flags=re.S)
     text = re.sub(r"(struct|enum)\s+\w+\s*\{.*?\}\s*;", "", text, flags=re.S)
     names = re.findall(r"\b([a-zA-Z_]\w*)\s*\([^;{}]*\)\s*;", text)
