@@ -38,8 +38,9 @@ UNIT = "rays/s"
 
 # Algorithmic FLOPs (add, mul, div, sqrt each 1) per accepted integration
 # step, frozen from the oracle's counting scalar over seeded pixels of each
-# workload (tests/test_flop_constants.py re-derives them).
-FLOPS_PER_STEP = {"dp45": 566.0, "rk4": 211.0}
+# workload (tests/test_flop_constants.py re-derives them). The mixed path runs
+# the same algorithm, so the same count applies to it.
+FLOPS_PER_STEP = {"dp45": 509.0, "rk4": 209.0}
 
 WORKLOADS = {
     # name: (frames, width, integrator, max_crossings)
@@ -128,21 +129,13 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
-def run_ours(args, rank: int, world: int, dist):
+def time_precision(args, precision: str, dev, stream, dist):
+    """Warm up, then time ``args.steps`` renders of the workload at one precision."""
     import torch
 
-    from blackhole_b200 import _abi, kerr
+    from blackhole_b200 import kerr
 
-    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
-    torch.cuda.set_device(dev)
-    lib = _abi.load_library()
-    precision = 1 if args.precision == "mixed" else 0
-    scenes = scenes_for(args.workload, precision)
-    wl = WORKLOADS[args.workload]
-    integ = "dp45" if wl["integrator"] == 1 else "rk4"
-    n_frame = wl["width"] * wl["height"]
-    rays_per_step = n_frame * len(scenes)
-    stream = torch.cuda.Stream(device=dev)
+    scenes = scenes_for(args.workload, 1 if precision == "mixed" else 0)
     outs = [kerr.alloc_image_outputs(s, device=dev, fields=list(OUT_FIELDS_USED)) for s in scenes]
 
     def render(ev=None):
@@ -153,17 +146,14 @@ def run_ours(args, rank: int, world: int, dist):
             if ev is not None:
                 ev[i][1].record(stream)
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
     sampler = ClockSampler(dev.index if "CUDA_VISIBLE_DEVICES" not in os.environ else 0)
     sampler.start()
     sampler.wait_first_sample()
     for _ in range(args.warmup):
         render()
     torch.cuda.synchronize(dev)
-    barrier()
+    if dist is not None:
+        dist.barrier()
     torch.cuda.synchronize(dev)
     sampler.lines.clear()
     per_launch = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
@@ -176,35 +166,91 @@ def run_ours(args, rank: int, world: int, dist):
     t1.record(stream)
     torch.cuda.synchronize(dev)
     clocks = sampler.stop()
-    barrier()
+    if dist is not None:
+        dist.barrier()
     elapsed_ms = t0.elapsed_time(t1)
-    launch_ms = [a.elapsed_time(b) for step in per_launch for (a, b) in step]
-    total_steps = sum(int(o["steps"].sum().item()) for o in outs)  # accepted steps of one render
-
     if dist is not None:
         t = torch.tensor([elapsed_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         elapsed_ms = float(t.item())
+    launch_ms = [a.elapsed_time(b) for step in per_launch for (a, b) in step]
+    total_steps = sum(int(o["steps"].sum().item()) for o in outs)  # accepted steps of one render
+    return dict(scenes=scenes, outs=outs, elapsed_ms=elapsed_ms, launch_ms=launch_ms, total_steps=total_steps,
+                clocks=clocks)
 
-    value = rays_per_step * args.steps * world / (elapsed_ms * 1e-3)
-    ms_per_step = elapsed_ms / args.steps
+
+def accuracy(ref_outs, test_outs) -> dict:
+    """Class agreement and |dg|/g of ``test`` against ``ref`` over all frames:
+    g compared at the last recorded crossing of pixels whose class and
+    crossing count agree."""
+    import torch
+
+    agree = total = 0
+    dgs = []
+    for a, b in zip(ref_outs, test_outs):
+        same_cls = a["cls"] == b["cls"]
+        agree += int(same_cls.sum().item())
+        total += a["cls"].numel()
+        same = same_cls & (a["n_cross"] == b["n_cross"]) & (a["n_cross"] > 0)
+        idx = torch.nonzero(same).squeeze(1)
+        k = (a["n_cross"][idx] - 1).long()
+        ga = a["g"][k, idx]
+        gb = b["g"][k, idx]
+        dgs.append((gb - ga).abs() / ga.abs())
+    dg = torch.cat(dgs)
+    q = torch.quantile(dg[: 16_000_000].float(), torch.tensor([0.5, 0.999], device=dg.device)).tolist() \
+        if dg.numel() else [None, None]
+    return {"class_agreement": agree / total, "dg_over_g_median": q[0], "dg_over_g_p999": q[1],
+            "dg_over_g_max": float(dg.max().item()) if dg.numel() else None, "pixels_compared": int(dg.numel()),
+            "reference": "this run's FP64 path (bit-identical to the CPU oracle)"}
+
+
+def run_ours(args, rank: int, world: int, dist):
+    import torch
+
+    from blackhole_b200 import _abi
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    lib = _abi.load_library()
+    wl = WORKLOADS[args.workload]
+    integ = "dp45" if wl["integrator"] == 1 else "rk4"
+    n_frame = wl["width"] * wl["height"]
+    rays_per_step = n_frame * len(wl["frames"])
+    stream = torch.cuda.Stream(device=dev)
+
+    precisions = [args.precision]
+    if args.compare and args.precision != "fp64":
+        precisions = ["fp64", args.precision]
+    runs = {p: time_precision(args, p, dev, stream, dist) for p in precisions}
+    head = runs[args.precision]
+    value = rays_per_step * args.steps * world / (head["elapsed_ms"] * 1e-3)
+    extra = {}
+    if "fp64" in runs and args.precision != "fp64":
+        f = runs["fp64"]
+        extra["fp64_plain"] = {"value": rays_per_step * args.steps * world / (f["elapsed_ms"] * 1e-3),
+                               "unit": UNIT, "ms_per_step": f["elapsed_ms"] / args.steps,
+                               "steps_per_render": f["total_steps"], "clocks": f["clocks"]}
+        extra["speedup_vs_fp64_plain"] = value / extra["fp64_plain"]["value"]
+        extra["accuracy_vs_fp64"] = accuracy(f["outs"], head["outs"])
 
     # ---- end to end through the host-buffer C entry point (pinned host memory) ----
     e2e = None
     if rank == 0:
+        scenes = head["scenes"]
         pinned = []
         for s in scenes:
             d = {}
-            for f in OUT_FIELDS_USED:
-                shape = (s.max_crossings * n_frame,) if f in _abi.PLANE_FIELDS else (n_frame,)
-                dt = torch.int32 if f in _abi.INT_FIELDS else torch.float64
-                d[f] = torch.empty(shape, dtype=dt).pin_memory()
+            for fld in OUT_FIELDS_USED:
+                shape = (s.max_crossings * n_frame,) if fld in _abi.PLANE_FIELDS else (n_frame,)
+                dt = torch.int32 if fld in _abi.INT_FIELDS else torch.float64
+                d[fld] = torch.empty(shape, dtype=dt).pin_memory()
             pinned.append(d)
         structs = []
         for d in pinned:
             o = _abi.KerrImageOut()
-            for f, t in d.items():
-                setattr(o, f, t.data_ptr())
+            for fld, t in d.items():
+                setattr(o, fld, t.data_ptr())
             structs.append(o)
         d2h = sum(t.numel() * t.element_size() for d in pinned for t in d.values())
         h2d = C.sizeof(_abi.KerrScene) * len(scenes)
@@ -219,20 +265,24 @@ def run_ours(args, rank: int, world: int, dist):
         e2e = {"value": rays_per_step * e2e_steps / (w1 - w0), "unit": UNIT, "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "api": "bh_kerr_trace_image_host"}
 
-    # ---- roofline of the tracing kernel ----
+    # ---- roofline of the headline tracing kernel ----
+    fp64 = args.precision == "fp64"
     peak = C.c_double(0.0)
-    _abi.check(lib.bh_measure_fma_peak(1 if precision == 0 else 0, 5, C.byref(peak)))
-    mean_launch_s = statistics.mean(launch_ms) * 1e-3
-    flops_per_launch = FLOPS_PER_STEP[integ] * total_steps / len(scenes)
+    _abi.check(lib.bh_measure_fma_peak(1 if fp64 else 0, 5, C.byref(peak)))
+    mean_launch_s = statistics.mean(head["launch_ms"]) * 1e-3
+    flops_per_launch = FLOPS_PER_STEP[integ] * head["total_steps"] / len(head["scenes"])
     achieved = flops_per_launch / mean_launch_s / 1e12
-    roofline = {"bound": "fp64" if precision == 0 else "fp32", "achieved": achieved, "peak": peak.value,
+    kname = "k_trace_image_fp64" if fp64 else "k_trace_image_mixed"
+    roofline = {"bound": "fp64" if fp64 else "fp32", "achieved": achieved, "peak": peak.value,
                 "unit": "TFLOP/s", "frac": achieved / peak.value if peak.value else None, "traffic": None,
                 "peak_source": "measured FMA-pipe probe (bh_measure_fma_peak), FMA = 2 FLOPs",
-                "flops_per_step": FLOPS_PER_STEP[integ], "steps_per_launch": total_steps / len(scenes),
-                "kernel": f"k_trace_image_fp64<{1 if integ == 'dp45' else 0}>",
-                "launch_ms_mean": statistics.mean(launch_ms)}
-    return dict(value=value, ms_per_step=ms_per_step, e2e=e2e, roofline=roofline, clocks=clocks,
-                total_steps=total_steps, rays_per_step=rays_per_step, launches=len(scenes) * args.steps)
+                "flops_per_step": FLOPS_PER_STEP[integ], "steps_per_launch": head["total_steps"] / len(head["scenes"]),
+                "kernel": f"{kname}<{1 if integ == 'dp45' else 0}>",
+                "launch_ms_mean": statistics.mean(head["launch_ms"]),
+                "launch_ms_min": min(head["launch_ms"]), "launch_ms_max": max(head["launch_ms"])}
+    return dict(value=value, ms_per_step=head["elapsed_ms"] / args.steps, e2e=e2e, roofline=roofline,
+                clocks=head["clocks"], total_steps=head["total_steps"], rays_per_step=rays_per_step,
+                launches=sum(len(r["scenes"]) * args.steps for r in runs.values()), extra=extra)
 
 
 # ---------------------------------------------------------------------------
@@ -269,7 +319,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", choices=tuple(WORKLOADS), default="disk16")
-    ap.add_argument("--precision", choices=("fp64", "mixed"), default="fp64")
+    ap.add_argument("--precision", choices=("fp64", "mixed"), default="mixed")
+    ap.add_argument("--compare", action=argparse.BooleanOptionalAction, default=True,
+                    help="also time the FP64 plain path and report the accuracy against it")
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU baseline sampling")
     args = ap.parse_args()
 
@@ -307,6 +359,7 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
                 "data": "synthetic", "config": config, "precision": args.precision,
                 "steps_per_s": res["total_steps"] * args.steps * world / (res["ms_per_step"] * args.steps * 1e-3),
+                **res["extra"],
                 "e2e": res["e2e"], "roofline": res["roofline"], "cpu_baseline": cb, "clocks": res["clocks"],
                 "gpu_launches": res["launches"]}
         print(json.dumps(line))

@@ -30,7 +30,7 @@ typedef struct BhkImageParams {
   int32_t max_cross;       // 1..3
   int32_t form;            // 0 reference, 1 Carter
   int32_t integrator;      // 0 RK4, 1 DP45
-  int32_t pad;
+  int32_t precision;       // 0 FP64, 1 mixed
 } BhkImageParams;
 
 typedef struct BhkImageOut {
@@ -50,6 +50,11 @@ int bhk_trace_image_fp64(const BhkImageParams *p, const BhkImageOut *o, unsigned
 // Occupancy query: max resident CTAs per SM for the given block size.
 int bhk_trace_image_fp64_occupancy(int integrator, int block, int *blocks_per_sm);
 
+// Mixed-precision image tracer (trace_image_mixed.cu), same contract.
+int bhk_trace_image_mixed(const BhkImageParams *p, const BhkImageOut *o, unsigned long long *work_counter,
+                          BhkLaunch launch, void *stream);
+int bhk_trace_image_mixed_occupancy(int integrator, int block, int *blocks_per_sm);
+
 // Reference stepper kernels (src/physics/kerr.cpp semantics), FP64.
 typedef struct BhkStateSoA { double *r, *theta, *phi, *t, *sr, *sth; } BhkStateSoA;
 typedef struct BhkConstsSoA { const double *e, *lz, *q; } BhkConstsSoA;
@@ -66,6 +71,9 @@ int bhk_kerr_trace_rays(int64_t n, BhkStateSoA init, BhkConstsSoA c, double mass
 // grid shape, allocating nothing; and setting the thread's last error.
 struct BH_KerrScene;
 int bhh_prepare_image_launch(const struct BH_KerrScene *scene, BhkImageParams *p, BhkLaunch *L);
+// Launches the image kernel of p->precision (work counter zeroed on stream).
+int bhh_launch_image(const BhkImageParams *p, const BhkImageOut *o, unsigned long long *counter, BhkLaunch L,
+                     void *stream);
 int bhh_fail(const char *msg);
 
 // FMA-throughput probe (probe.cu).

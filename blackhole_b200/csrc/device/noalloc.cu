@@ -94,9 +94,8 @@ extern "C" int bh_kerr_trace_image_host_noalloc(const BH_KerrScene *scene, const
                       static_cast<double *>(d[6]),  static_cast<double *>(d[7]),  static_cast<double *>(d[8]),
                       static_cast<double *>(d[9])};
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  // bhk_trace_image_fp64 zeroes the work counter on s before the launch.
-  if (bhk_trace_image_fp64(&p, &o, reinterpret_cast<unsigned long long *>(b), L, stream) != 0)
-    return bhh_fail(bhk_last_error());
+  // bhh_launch_image zeroes the work counter on s before the launch.
+  if (bhh_launch_image(&p, &o, reinterpret_cast<unsigned long long *>(b), L, stream) != 0) return -1;
   for (int i = 0; i < 10; ++i) {
     if (!host[i]) continue;
     const cudaError_t e = cudaMemcpyAsync(host[i], d[i], bytes[i], cudaMemcpyDeviceToHost, s);

@@ -6,8 +6,8 @@
 // warp-aggregated atomicAdd (ballot + popc), so finished rays never idle a
 // lane while work remains. The integration follows the reference trace loop
 // order (src/physics/raytracer.h:338-365): step budget, horizon test, escape
-// test, step; then the equatorial-crossing test with bisection
-// (src/physics/event_detection.h:127-180 pattern).
+// test, step; then the equatorial-crossing test, refined on its bracket
+// (src/physics/event_detection.h:127-180 pattern) by Illinois regula falsi.
 //
 // Built with -fmad=false: bit-identical to the FP64 CPU oracle.
 #include <cuda_runtime.h>
@@ -69,24 +69,33 @@ __device__ __forceinline__ Yd sub_step(const BhkImageParams &p, const RayC &c, c
   return dp45(y, h, c, rhs(y, c), p.rtol, p.atol, false).y5;
 }
 
-// Bisection on the sub-step for u = 0 inside [0, h] from y0.
+// Root of u on the sub-step bracket [0, h] from y0 (u(h) = u1 of the other
+// sign): Illinois regula falsi, each trial one sub-step re-integrated from y0.
 template <int INTEG>
-__device__ __noinline__ Yd bisect_equator(const BhkImageParams &p, const RayC &c, const Yd &y0, double h) {
-  double la = 0.0, lb = h;
-  Yd sa = y0;
-  for (int i = 0; i < 60; ++i) {
-    const double lm = 0.5 * (la + lb);
-    const Yd sm = sub_step<INTEG>(p, c, sa, lm - la);
-    if (fabs(sm.u) < 1e-13) return sm;
-    if ((sa.u * sm.u) < 0.0) {
-      lb = lm;
+__device__ __noinline__ Yd refine_equator(const BhkImageParams &p, const RayC &c, const Yd &y0, double h,
+                                          double u1) {
+  double a = 0.0, fa = y0.u, b = h, fb = u1;
+  int side = 0;
+  Yd yc = y0;
+  for (int i = 0; i < 40; ++i) {
+    double t = (a * fb - b * fa) / (fb - fa);
+    if (!(t > a && t < b)) t = 0.5 * (a + b);
+    yc = sub_step<INTEG>(p, c, y0, t);
+    const double fc = yc.u;
+    if (fabs(fc) < 1e-13) return yc;
+    if ((fc * fb) > 0.0) {
+      b = t;
+      fb = fc;
+      if (side == -1) fa = 0.5 * fa;
+      side = -1;
     } else {
-      la = lm;
-      sa = sm;
+      a = t;
+      fa = fc;
+      if (side == 1) fb = 0.5 * fb;
+      side = 1;
     }
   }
-  const double lm = 0.5 * (la + lb);
-  return sub_step<INTEG>(p, c, sa, lm - la);
+  return yc;
 }
 
 // Records a crossing at yc when it lies on the disk; returns true when the
@@ -146,7 +155,7 @@ __device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOu
     Yd yn = rk4(R.y, h, R.c, rhs(R.y, R.c));
     ++R.steps;
     if ((R.y.u * yn.u) < 0.0) {
-      const Yd yc = bisect_equator<0>(p, R.c, R.y, h);
+      const Yd yc = refine_equator<0>(p, R.c, R.y, h, yn.u);
       if (on_crossing(p, o, R, yc)) return 1;
     }
     project(yn, R.c);
@@ -163,7 +172,7 @@ __device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOu
       ++R.steps;
       bool stop = false;
       if ((R.y.u * d.y5.u) < 0.0) {
-        const Yd yc = bisect_equator<1>(p, R.c, R.y, R.h);
+        const Yd yc = refine_equator<1>(p, R.c, R.y, R.h, d.y5.u);
         stop = on_crossing(p, o, R, yc);
       }
       R.y = d.y5;

@@ -1,0 +1,291 @@
+// trace_image_mixed.cu - mixed-precision image-plane Kerr tracer (sm_100a).
+//
+// Same persistent warp-refill structure and trace-loop order as the FP64
+// kernel (trace_image_fp64.cu), with the integration in FP32:
+//   * FP64: per-ray set-up (lambda, eta, q, K, initial momenta from R(r_obs)),
+//     the crossing radius and azimuth handed to the outputs, the redshift g,
+//     the Novikov-Thorne flux and the intensity.
+//   * FP32: every right-hand side, the Dormand-Prince / RK4 stages, the error
+//     estimate, the step controller, the first-integral projection and the
+//     crossing refinement.
+//   * Compensated FP32 (hi + lo with TwoSum) for the positions r, u, phi, so
+//     that thousands of small FP32 increments accumulate without drift.
+// The DP45 error estimate is formed from the stage derivatives (h sum e_j k_j),
+// never as a difference of two positions, so its FP32 rounding noise is
+// ~1e-7 of the step increment rather than of the position: rtol = 1e-8 is
+// honoured by the controller.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+
+#include "image_mixed.cuh"
+#include "launch.h"
+
+namespace bhm {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+struct RayMx {
+  RayCf c;
+  Yf y;
+  Lof lo;
+  Yf k1;       // DP45 FSAL stage
+  float h;     // DP45 trial step / unused for RK4
+  double lam;  // lambda in FP64 for g
+  double inten;
+  long long pix;
+  int steps;
+  int attempts;
+  int ncross;
+};
+
+__device__ __forceinline__ void split(double v, float &hi, float &lo) {
+  hi = (float)v;
+  lo = (float)(v - (double)hi);
+}
+
+__device__ __forceinline__ void init_ray(const BhkImageParams &p, long long pix, RayMx &R) {
+  const long long i = pix % p.width, j = pix / p.width;
+  const double alpha = p.alpha_min + ((double)i + 0.5) * p.dalpha;
+  const double beta = p.beta_min + ((double)j + 0.5) * p.dbeta;
+  const double a = p.a;
+  const double lam = -alpha * p.sin_o;
+  const double eta = beta * beta + (alpha * alpha - a * a) * p.cos_o * p.cos_o;
+  const double qTh = eta + lam * lam;
+  const double qR = (p.form == 1) ? eta : qTh;
+  const double K = qR + (lam - a) * (lam - a);
+  const double r0 = p.r_obs;
+  const double A = r0 * r0 + a * a - a * lam;
+  const double D = r0 * r0 - 2.0 * r0 + a * a;
+  const double Rv = A * A - D * K;
+  R.c.a = (float)a;
+  R.c.a2 = (float)(a * a);
+  R.c.lam = (float)lam;
+  R.c.qTh = (float)qTh;
+  R.c.K = (float)K;
+  R.c.a2_minus_alam = (float)(a * a - a * lam);
+  R.c.c_pu = (float)(a * a - qTh);
+  R.c.proj_u = (float)(1e-6 * (fabs(qTh) + a * a));
+  split(r0, R.y.r, R.lo.r);
+  split(p.cos_o, R.y.u, R.lo.u);
+  R.y.phi = 0.0f;
+  R.lo.phi = 0.0f;
+  R.y.pr = (float)(-sqrt(Rv < 0.0 ? 0.0 : Rv));
+  R.y.pu = (float)(beta * p.sin_o);
+  R.lam = lam;
+  R.inten = 0.0;
+  R.pix = pix;
+  R.steps = 0;
+  R.attempts = 0;
+  R.ncross = 0;
+  const float hh = (float)p.step_coeff * fminf(R.y.r, (float)p.step_rcap);
+  R.h = hh / fmaf(R.c.a2 * R.y.u, R.y.u, R.y.r * R.y.r);
+  R.k1 = rhs(R.y, R.c);
+}
+
+template <int INTEG>
+__device__ __forceinline__ Yf sub_inc(const BhkImageParams &p, const RayCf &c, const Yf &y, float h) {
+  if (INTEG == 0) return rk4_inc(y, h, c, rhs(y, c));
+  return dp45(y, h, c, rhs(y, c), (float)p.rtol, (float)p.atol, false).d;
+}
+
+// Crossing of u = 0 inside the sub-step bracket [0, h] from (y0, lo0):
+// Illinois regula falsi on u(t) = u0 + lo0.u + du(t); returns the FP64
+// radius and azimuth at the root.
+template <int INTEG>
+__device__ __noinline__ void refine_equator(const BhkImageParams &p, const RayCf &c, const Yf &y0, const Lof &lo0,
+                                            float h, float u1, double &r_c, double &phi_c) {
+  float a = 0.0f, fa = y0.u + lo0.u, b = h, fb = u1;
+  const float tol = 1e-7f * (fabsf(fa) + fabsf(fb));
+  int side = 0;
+  Yf d = sub_inc<INTEG>(p, c, y0, h);
+  for (int i = 0; i < 24; ++i) {
+    float t = __fdividef(fmaf(a, fb, -b * fa), fb - fa);
+    if (!(t > a && t < b)) t = 0.5f * (a + b);
+    d = sub_inc<INTEG>(p, c, y0, t);
+    const float fc = y0.u + (lo0.u + d.u);
+    if (fabsf(fc) <= tol) break;
+    if (fc * fb > 0.0f) {
+      b = t;
+      fb = fc;
+      if (side == -1) fa *= 0.5f;
+      side = -1;
+    } else {
+      a = t;
+      fa = fc;
+      if (side == 1) fb *= 0.5f;
+      side = 1;
+    }
+  }
+  r_c = (double)y0.r + ((double)lo0.r + (double)d.r);
+  phi_c = (double)y0.phi + ((double)lo0.phi + (double)d.phi);
+}
+
+__device__ __forceinline__ double disk_g(double r, double a, double lam) {
+  const double x = sqrt(r);
+  const double x3 = x * x * x;
+  const double v = x3 * (x3 - 3.0 * x + 2.0 * a);
+  if (v <= 0.0) return 0.0;
+  return sqrt(v) / (x3 + a - lam);
+}
+
+__device__ __forceinline__ bool on_crossing(const BhkImageParams &p, const BhkImageOut &o, RayMx &R, double r_c,
+                                            double phi_c) {
+  if (!(r_c >= p.r_in && r_c <= p.r_out)) return false;
+  const int k = R.ncross;
+  const long long off = (long long)k * p.n_pix + R.pix;
+  const double g = disk_g(r_c, p.a, R.lam);
+  if (o.r_hit) o.r_hit[off] = r_c;
+  if (o.phi_hit) o.phi_hit[off] = phi_c;
+  if (o.g) o.g[off] = g;
+  const double q = p.r_in / r_c;
+  const double g2 = g * g;
+  R.inten += g2 * g2 * q * q * q;
+  if (k == 0 && o.flux) {
+    double f = 0.0;
+    if (r_c >= p.nt_isco) {
+      const double t = 1.0 - sqrt(p.nt_isco / r_c);
+      f = fmin(1.0, (t > 0.0 ? t : 0.0) / (r_c * r_c * r_c) / p.nt_flux_peak);
+    }
+    o.flux[R.pix] = f;
+  }
+  R.ncross = k + 1;
+  return R.ncross >= p.max_cross;
+}
+
+__device__ __forceinline__ void finish(const BhkImageParams &p, const BhkImageOut &o, const RayMx &R, int cls) {
+  const long long pix = R.pix;
+  if (o.cls) o.cls[pix] = cls;
+  if (o.steps) o.steps[pix] = R.steps;
+  if (o.n_cross) o.n_cross[pix] = R.ncross;
+  if (o.intensity) o.intensity[pix] = R.inten;
+  if (R.ncross == 0 && o.flux) o.flux[pix] = 0.0;
+  for (int k = R.ncross; k < p.max_cross; ++k) {
+    const long long off = (long long)k * p.n_pix + pix;
+    if (o.r_hit) o.r_hit[off] = 0.0;
+    if (o.phi_hit) o.phi_hit[off] = 0.0;
+    if (o.g) o.g[off] = 0.0;
+  }
+  double th = 0.0, ph = 0.0;
+  if (cls == 2) {
+    const double u = to_f64(R.y.u, R.lo.u);
+    th = acos(fmin(1.0, fmax(-1.0, u)));
+    ph = to_f64(R.y.phi, R.lo.phi);
+  }
+  if (o.theta_inf) o.theta_inf[pix] = th;
+  if (o.phi_inf) o.phi_inf[pix] = ph;
+}
+
+// Applies an accepted increment d to the ray (compensated positions), tests
+// for an equatorial crossing and records it; returns true if the ray stops.
+template <int INTEG>
+__device__ __forceinline__ bool accept(const BhkImageParams &p, const BhkImageOut &o, RayMx &R, const Yf &d,
+                                       float h) {
+  const Yf y0 = R.y;
+  const Lof lo0 = R.lo;
+  comp_add(R.y.r, R.lo.r, d.r);
+  comp_add(R.y.u, R.lo.u, d.u);
+  comp_add(R.y.phi, R.lo.phi, d.phi);
+  R.y.pr += d.pr;
+  R.y.pu += d.pu;
+  ++R.steps;
+  bool stop = false;
+  if ((y0.u + lo0.u) * (R.y.u + R.lo.u) < 0.0f) {
+    double r_c, phi_c;
+    refine_equator<INTEG>(p, R.c, y0, lo0, h, R.y.u + R.lo.u, r_c, phi_c);
+    stop = on_crossing(p, o, R, r_c, phi_c);
+  }
+  project(R.y, R.c);
+  return stop;
+}
+
+template <int INTEG>
+__device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOut &o, RayMx &R, float r_hor,
+                                       float r_esc) {
+  if (INTEG == 0) {
+    if (R.steps >= p.max_steps) return 3;
+    if (R.y.r <= r_hor) return 0;
+    if (R.y.r >= r_esc) return 2;
+    const float hh = (float)p.step_coeff * fminf(R.y.r, (float)p.step_rcap);
+    const float h = __fdividef(hh, fmaf(R.c.a2 * R.y.u, R.y.u, R.y.r * R.y.r));
+    const Yf d = rk4_inc(R.y, h, R.c, rhs(R.y, R.c));
+    return accept<0>(p, o, R, d, h) ? 1 : -1;
+  } else {
+    const long long max_attempts = 4LL * p.max_steps + 64;
+    if (R.steps >= p.max_steps || R.attempts >= max_attempts) return 3;
+    if (R.y.r <= r_hor) return 0;
+    if (R.y.r >= r_esc) return 2;
+    ++R.attempts;
+    const DPf d = dp45(R.y, R.h, R.c, R.k1, (float)p.rtol, (float)p.atol, true);
+    if (d.err <= 1.0f) {
+      const float h = R.h;
+      const bool stop = accept<1>(p, o, R, d.d, h);
+      R.k1 = d.k7;
+      R.k1.r = R.y.pr;  // projection moved only the momenta
+      R.k1.u = R.y.pu;
+      R.h = h * step_factor(d.err, true);
+      if (stop) return 1;
+    } else {
+      R.h = R.h * step_factor(d.err, false);
+    }
+    return -1;
+  }
+}
+
+template <int INTEG>
+__global__ void __launch_bounds__(128) k_trace_image_mixed(const BhkImageParams p, const BhkImageOut o,
+                                                           unsigned long long *__restrict__ counter) {
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned lanemask_lt = (1u << lane) - 1u;
+  const float r_hor = (float)p.r_hor, r_esc = (float)p.r_esc;
+  RayMx R;
+  bool active = false;
+  bool exhausted = false;
+  for (;;) {
+    const unsigned need = __ballot_sync(kFull, !active && !exhausted);
+    if (need) {
+      const int leader = __ffs(need) - 1;
+      unsigned long long base = 0;
+      if ((int)lane == leader) base = atomicAdd(counter, (unsigned long long)__popc(need));
+      base = __shfl_sync(kFull, base, leader);
+      if (!active && !exhausted) {
+        const unsigned long long mine = base + (unsigned long long)__popc(need & lanemask_lt);
+        if (mine < (unsigned long long)p.n_pix) {
+          init_ray(p, (long long)mine, R);
+          active = true;
+        } else {
+          exhausted = true;
+        }
+      }
+    }
+    if (!__any_sync(kFull, active)) break;
+    if (active) {
+      const int cls = iterate<INTEG>(p, o, R, r_hor, r_esc);
+      if (cls >= 0) {
+        finish(p, o, R, cls);
+        active = false;
+      }
+    }
+  }
+}
+
+}  // namespace bhm
+
+extern "C" int bhk_trace_image_mixed(const BhkImageParams *p, const BhkImageOut *o, unsigned long long *counter,
+                                     BhkLaunch launch, void *stream) {
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s) != cudaSuccess) return -1;
+  if (p->integrator == 0)
+    bhm::k_trace_image_mixed<0><<<launch.grid, launch.block, 0, s>>>(*p, *o, counter);
+  else
+    bhm::k_trace_image_mixed<1><<<launch.grid, launch.block, 0, s>>>(*p, *o, counter);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+extern "C" int bhk_trace_image_mixed_occupancy(int integrator, int block, int *blocks_per_sm) {
+  const cudaError_t e =
+      (integrator == 0)
+          ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhm::k_trace_image_mixed<0>, block, 0)
+          : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhm::k_trace_image_mixed<1>, block, 0);
+  return e == cudaSuccess ? 0 : -1;
+}

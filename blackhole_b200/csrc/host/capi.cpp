@@ -166,6 +166,7 @@ static BhkImageParams make_params(const BH_KerrScene *s) {
   p.max_cross = s->max_crossings;
   p.form = s->potential_form;
   p.integrator = s->integrator;
+  p.precision = s->precision;
   return p;
 }
 
@@ -177,7 +178,6 @@ int bhh_prepare_image_launch(const BH_KerrScene *scene, BhkImageParams *p, BhkLa
   *p = make_params(scene);
   *L = BhkLaunch{0, 0};
   if (p->n_pix == 0) return 0;
-  if (scene->precision != BH_PRECISION_FP64) return fail("mixed precision tracer not built in this library");
   int dev = 0, sms = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
@@ -185,7 +185,10 @@ int bhh_prepare_image_launch(const BH_KerrScene *scene, BhkImageParams *p, BhkLa
   if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute(SM count)");
   const int block = g_block_override ? g_block_override : 128;
   int per_sm = 0;
-  if (bhk_trace_image_fp64_occupancy(p->integrator, block, &per_sm) != 0) return fail("%s", bhk_last_error());
+  const int occ_rc = (p->precision == BH_PRECISION_MIXED)
+                         ? bhk_trace_image_mixed_occupancy(p->integrator, block, &per_sm)
+                         : bhk_trace_image_fp64_occupancy(p->integrator, block, &per_sm);
+  if (occ_rc != 0) return cuda_fail(cudaGetLastError(), "occupancy query");
   if (g_ctas_per_sm_override) per_sm = std::min(per_sm, g_ctas_per_sm_override);
   if (per_sm < 1) return fail("kernel does not fit on an SM at %d threads per CTA", block);
   const int64_t full = int64_t(sms) * per_sm;
@@ -197,6 +200,17 @@ int bhh_prepare_image_launch(const BH_KerrScene *scene, BhkImageParams *p, BhkLa
 // Records an error message from the device layer (noalloc.cu).
 int bhh_fail(const char *msg) { return fail("%s", msg); }
 
+int bhh_launch_image(const BhkImageParams *p, const BhkImageOut *o, unsigned long long *counter, BhkLaunch L,
+                     void *stream) {
+  if (p->precision == BH_PRECISION_MIXED) {
+    if (bhk_trace_image_mixed(p, o, counter, L, stream) != 0)
+      return cuda_fail(cudaGetLastError(), "k_trace_image_mixed launch");
+    return 0;
+  }
+  if (bhk_trace_image_fp64(p, o, counter, L, stream) != 0) return fail("%s", bhk_last_error());
+  return 0;
+}
+
 int bh_kerr_trace_image(const BH_KerrScene *scene, const BH_KerrImageOut *out, void *stream) {
   if (!out) return fail("output descriptor is NULL");
   BhkImageParams p;
@@ -207,8 +221,7 @@ int bh_kerr_trace_image(const BH_KerrScene *scene, const BH_KerrImageOut *out, v
   if (device_scratch(&ds) != 0) return -1;
   const BhkImageOut o{out->cls,   out->steps,     out->n_cross,   out->r_hit,     out->phi_hit,
                       out->g,     out->flux,      out->intensity, out->theta_inf, out->phi_inf};
-  if (bhk_trace_image_fp64(&p, &o, ds->counter, L, stream) != 0) return fail("%s", bhk_last_error());
-  return 0;
+  return bhh_launch_image(&p, &o, ds->counter, L, stream);
 }
 
 // ---- host-buffer entry point ---------------------------------------------------

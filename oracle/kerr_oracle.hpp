@@ -24,8 +24,8 @@
 //     or Dormand & Prince (1980) 5(4) with the step controller of Hairer,
 //     Norsett & Wanner (1993) II.4 (safety 0.9, factor in [0.1, 2]) as the
 //     reference states it in src/physics/verified/rk4.h:254-265;
-//   - equatorial crossings refined by bisection, the pattern of
-//     bisectRadialCrossing (src/physics/event_detection.h:127-180);
+//   - equatorial crossings refined on a bracket like bisectRadialCrossing
+//     (src/physics/event_detection.h:127-180), with Illinois regula falsi;
 //   - Keplerian redshift g = 1 / (u^t (1 - Omega lambda)) with the
 //     Bardeen-Press-Teukolsky (1972) u^t and Omega (as in src/physics/iron_kline.h:25-40).
 // Templated on the scalar so that a counting scalar can count its FLOPs and
@@ -555,26 +555,40 @@ template <class T> inline T mino_step(const Scene &s, const Y<T> &y, T a) {
   return h / sigma;
 }
 
-// Locate the equatorial crossing inside a step of size h from y0 by bisection
-// on the sub-step, re-stepping from the left end (event_detection.h:127-180
-// pattern); returns the state at the crossing.
+// Locate the equatorial crossing u = 0 inside a step of size h from y0
+// (u(0) = y0.u and u(h) = u1 of opposite signs). The bracket [0, h] on the
+// sub-step is refined like bisectRadialCrossing (event_detection.h:127-180),
+// but with the Illinois variant of regula falsi (Dowell & Jarratt 1971):
+// the trial point interpolates the bracket's u values, and the value kept
+// twice in a row is halved, which keeps superlinear convergence (about 6
+// sub-steps to |u| < 1e-13 against about 40 for bisection). Every trial
+// re-integrates from y0 with one sub-step; returns the state at the root.
+inline constexpr int kRootMaxIter = 40;
+
 template <class T, class Stepper>
-inline Y<T> bisect_equator(const Y<T> &y0, T h, const Stepper &step) {
-  T la = T(0), lb = h;
-  Y<T> sa = y0;
-  for (int i = 0; i < 60; ++i) {
-    const T lm = T(0.5) * (la + lb);
-    const Y<T> sm = step(sa, lm - la);
-    if (s_abs(sm.u) < T(1e-13)) return sm;
-    if ((sa.u * sm.u) < T(0)) {
-      lb = lm;
+inline Y<T> refine_equator(const Y<T> &y0, T h, T u1, const Stepper &step) {
+  T a = T(0), fa = y0.u, b = h, fb = u1;
+  int side = 0;
+  Y<T> yc = y0;
+  for (int i = 0; i < kRootMaxIter; ++i) {
+    T c = (a * fb - b * fa) / (fb - fa);
+    if (!(c > a && c < b)) c = T(0.5) * (a + b);
+    yc = step(y0, c);
+    const T fc = yc.u;
+    if (s_abs(fc) < T(1e-13)) return yc;
+    if ((fc * fb) > T(0)) {
+      b = c;
+      fb = fc;
+      if (side == -1) fa = T(0.5) * fa;
+      side = -1;
     } else {
-      la = lm;
-      sa = sm;
+      a = c;
+      fa = fc;
+      if (side == 1) fb = T(0.5) * fb;
+      side = 1;
     }
   }
-  const T lm = T(0.5) * (la + lb);
-  return step(sa, lm - la);
+  return yc;
 }
 
 template <class T>
@@ -620,7 +634,7 @@ inline PixelResult<T> trace_pixel(const Scene &s, const SceneDerived<T> &d, T al
       Y<T> yn = img_rk4(y, h, f, f(y));
       ++out.steps;
       if ((y.u * yn.u) < T(0)) {
-        const Y<T> yc = bisect_equator(y, h, step);
+        const Y<T> yc = refine_equator(y, h, yn.u, step);
         if (in_disk(yc.r)) {
           record_crossing(s, d, c, yc, out);
           if (out.n_cross >= maxc) { out.cls = CLS_DISK; break; }
@@ -649,7 +663,7 @@ inline PixelResult<T> trace_pixel(const Scene &s, const SceneDerived<T> &d, T al
       if (err <= T(1)) {
         ++out.steps;
         if ((y.u * o.y5.u) < T(0)) {
-          const Y<T> yc = bisect_equator(y, h, step);
+          const Y<T> yc = refine_equator(y, h, o.y5.u, step);
           if (in_disk(yc.r)) {
             record_crossing(s, d, c, yc, out);
             if (out.n_cross >= maxc) { out.cls = CLS_DISK; stop = true; }

@@ -1,0 +1,86 @@
+"""Accuracy of the mixed-precision image tracer against the FP64 path.
+
+The FP64 path is bit-identical to the CPU oracle (test_gpu_image.py), so it
+stands in for the oracle at sizes the CPU would take minutes on. Tolerances
+are the targets stated for the mixed method: the same termination class on
+at least 99.9 % of pixels, and for pixels where both paths stop on the disk
+with the same number of crossings, median |dg|/g <= 1e-4 and max <= 1e-3.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from test_gpu_image import gpu_trace, scene
+
+pytestmark = pytest.mark.gpu
+
+CLASS_AGREEMENT = 0.999
+DG_MEDIAN = 1e-4
+DG_MAX = 1e-3
+
+
+def compare(s):
+    s64 = scene(**{**s.as_dict(), "precision": 0})
+    s32 = scene(**{**s.as_dict(), "precision": 1})
+    a = gpu_trace(s64)
+    b = gpu_trace(s32)
+    agree = float(np.mean(a["cls"] == b["cls"]))
+    same = (a["cls"] == b["cls"]) & (a["n_cross"] == b["n_cross"]) & (a["n_cross"] > 0)
+    k = a["n_cross"][same] - 1  # last recorded crossing
+    idx = np.nonzero(same)[0]
+    ga = a["g"][k, idx]
+    gb = b["g"][k, idx]
+    dg = np.abs(gb - ga) / np.abs(ga)
+    return a, b, agree, dg
+
+
+@pytest.mark.parametrize("spin,inc", [(0.0, 17.0), (0.5, 45.0), (0.9, 75.0), (0.998, 85.0), (0.9, 60.0)])
+def test_mixed_dp45_meets_accuracy_targets(cuda, spin, inc):
+    s = scene(width=160, height=160, spin=spin, theta_obs=math.radians(inc), integrator=1, max_crossings=3)
+    a, b, agree, dg = compare(s)
+    assert agree >= CLASS_AGREEMENT, agree
+    assert len(dg) > 0
+    assert np.median(dg) <= DG_MEDIAN, np.median(dg)
+    assert dg.max() <= DG_MAX, dg.max()
+
+
+def test_mixed_rk4_c0_meets_accuracy_targets(cuda):
+    s = scene(width=256, height=256)
+    a, b, agree, dg = compare(s)
+    assert agree >= CLASS_AGREEMENT, agree
+    assert np.median(dg) <= DG_MEDIAN, np.median(dg)
+    assert dg.max() <= DG_MAX, dg.max()
+
+
+def test_mixed_carter_form(cuda):
+    s = scene(width=128, height=96, integrator=1, potential_form=1, max_crossings=2)
+    a, b, agree, dg = compare(s)
+    assert agree >= CLASS_AGREEMENT, agree
+    assert np.median(dg) <= DG_MEDIAN and dg.max() <= DG_MAX
+
+
+def test_mixed_host_and_noalloc_entry_points(cuda):
+    from blackhole_b200 import kerr
+
+    s = scene(width=48, height=40, integrator=1, max_crossings=3, precision=1)
+    dev = gpu_trace(s)
+    host = kerr.trace_image_host(s)
+    noalloc = kerr.trace_image_host_noalloc(s)
+    for k in dev:
+        np.testing.assert_array_equal(host[k], dev[k], err_msg=k)
+        np.testing.assert_array_equal(noalloc[k], dev[k], err_msg=k)
+
+
+def test_mixed_edge_cases(cuda):
+    a = gpu_trace(scene(width=16, height=16, max_steps=0, precision=1))
+    assert (a["cls"] == 3).all() and (a["steps"] == 0).all()
+    a = gpu_trace(scene(width=8, height=8, escape_factor=0.5, precision=1))
+    assert (a["cls"] == 2).all()
+    for w, h in ((37, 23), (1, 1)):
+        a = gpu_trace(scene(width=w, height=h, integrator=1, precision=1))
+        assert a["cls"].shape == (w * h,) and (a["cls"] >= 0).all()
+    torch.cuda.synchronize()
