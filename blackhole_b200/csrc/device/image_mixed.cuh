@@ -20,7 +20,6 @@ struct RayCf {
   float a, a2, lam, qTh, K;
   float a2_minus_alam;   // a^2 - a lambda
   float c_pu;            // a^2 - q_Th
-  float proj_u;          // projection threshold tau (|q_Th| + a^2)
 };
 
 struct Yf {
@@ -36,7 +35,7 @@ __device__ __forceinline__ Yf rhs(const Yf &y, const RayCf &c) {
   const float A = fmaf(r, r, c.a2_minus_alam);
   const float D = fmaf(r, r - 2.0f, c.a2);
   const float u2 = u * u;
-  const float s2 = fmaxf(1.0f - u2, 1e-12f);
+  const float s2 = fmaxf((1.0f - u) * (1.0f + u), 1e-12f);  // no cancellation near the poles
   Yf d;
   d.r = y.pr;
   d.u = y.pu;
@@ -68,16 +67,30 @@ __device__ __forceinline__ float pot_U(float u, const RayCf &c) {
   return fmaf(fmaf(c.a2, u2, c.qTh), 1.0f - u2, -c.lam * c.lam);
 }
 
-constexpr float kProjTau = 1e-6f;
+// Constants of motion in FP64 for the first-integral projection.
+struct RayCd {
+  double a, lam, qTh, K;
+};
 
-// First-integral projection (see image_fp64.cuh); FP32 R and U have relative
-// noise ~1e-7 of their largest term, far below the threshold.
-__device__ __forceinline__ void project(Yf &y, const RayCf &c) {
-  const float Rv = pot_R(y.r, c);
-  const float r2 = y.r * y.r;
-  if (Rv > kProjTau * (r2 * r2)) y.pr = copysignf(sqrtf(Rv), y.pr);
-  const float Uv = pot_U(y.u, c);
-  if (Uv > c.proj_u) y.pu = copysignf(sqrtf(Uv), y.pu);
+constexpr double kProjTau = 1e-6;
+
+// First-integral projection (see image_fp64.cuh) with R and U evaluated in
+// FP64 from the compensated positions. In FP32 both potentials carry an
+// absolute error ~1e-7 of their largest term (A^2, resp. q + a^2), which near
+// a turning point, where R ~ 1e-4 r^4, would already move p_r by 4e-4; in
+// FP64 the reset is exact at the 1e-6 threshold of the FP64 path. Only the
+// square root's argument is FP64: the result is rounded to FP32 once.
+__device__ __forceinline__ void project(Yf &y, const Lof &lo, const RayCd &c) {
+  const double r = (double)y.r + (double)lo.r;
+  const double u = (double)y.u + (double)lo.u;
+  const double A = r * r + c.a * c.a - c.a * c.lam;
+  const double D = r * r - 2.0 * r + c.a * c.a;
+  const double Rv = A * A - D * c.K;
+  const double r2 = r * r;
+  if (Rv > kProjTau * (r2 * r2)) y.pr = copysignf(sqrtf((float)Rv), y.pr);
+  const double u2 = u * u;
+  const double Uv = (c.qTh + c.a * c.a * u2) * (1.0 - u2) - c.lam * c.lam;
+  if (Uv > kProjTau * (fabs(c.qTh) + c.a * c.a)) y.pu = copysignf(sqrtf((float)Uv), y.pu);
 }
 
 // hi + lo += d (TwoSum then renormalise): exact error-free accumulation of
@@ -157,7 +170,11 @@ __device__ __forceinline__ DPf dp45(const Yf &y, float h, const RayCf &c, const 
 #define BHM_E(f)                                                                                          \
   (h * fmaf(dpf::e1, k1.f,                                                                               \
             fmaf(dpf::e3, k3.f, fmaf(dpf::e4, k4.f, fmaf(dpf::e5, k5.f, fmaf(dpf::e6, k6.f, dpf::e7 * o.k7.f))))))
-#define BHM_Q(f) __fdividef(BHM_E(f), fmaf(rtol, fmaxf(fabsf(y.f), fabsf(y5.f)), atol))
+  // Error scale: atol + rtol max(|y|, |y5|), plus a floor of 1e-7 |y5 - y|.
+  // The FP32 estimate h sum e_j k_j carries rounding noise ~1e-8 |y5 - y|;
+  // where rtol |y| falls below that (momenta near a turning point, phi near
+  // its start value of 0) the floor keeps the controller from chasing it.
+#define BHM_Q(f) __fdividef(BHM_E(f), fmaf(1e-7f, fabsf(o.d.f), fmaf(rtol, fmaxf(fabsf(y.f), fabsf(y5.f)), atol)))
   const float q0 = BHM_Q(r), q1 = BHM_Q(u), q2 = BHM_Q(phi), q3 = BHM_Q(pr), q4 = BHM_Q(pu);
 #undef BHM_Q
 #undef BHM_E

@@ -6,14 +6,16 @@
 // warp-aggregated atomicAdd (ballot + popc), so finished rays never idle a
 // lane while work remains. The integration follows the reference trace loop
 // order (src/physics/raytracer.h:338-365): step budget, horizon test, escape
-// test, step; then the equatorial-crossing test, refined on its bracket
-// (src/physics/event_detection.h:127-180 pattern) by Illinois regula falsi.
+// test, step; then the equatorial-crossing test, located inside the step by
+// Hermite interpolation (hermite.cuh) on the bracket of the
+// src/physics/event_detection.h:127-180 pattern.
 //
 // Built with -fmad=false: bit-identical to the FP64 CPU oracle.
 #include <cuda_runtime.h>
 
 #include <cstdio>
 
+#include "hermite.cuh"
 #include "image_fp64.cuh"
 #include "launch.h"
 
@@ -63,56 +65,30 @@ __device__ __forceinline__ void init_ray(const BhkImageParams &p, long long pix,
   }
 }
 
-template <int INTEG>
-__device__ __forceinline__ Yd sub_step(const BhkImageParams &p, const RayC &c, const Yd &y, double h) {
-  if (INTEG == 0) return rk4(y, h, c, rhs(y, c));
-  return dp45(y, h, c, rhs(y, c), p.rtol, p.atol, false).y5;
+// Crossing of u = 0 inside the accepted step y0 -> y1 (y1 before the
+// projection) with k0 = rhs(y0), k1 = rhs(y1): Hermite interpolation.
+__device__ __forceinline__ void step_crossing(const Yd &y0, const Yd &k0, const Yd &y1, const Yd &k1, double h,
+                                              double &r_c, double &phi_c) {
+  const bhh_dev::Ends e{y0.r, y0.u, y0.phi, y0.pr, y0.pu, k0.pr, k0.pu, k0.phi,
+                        y1.r, y1.u, y1.phi, y1.pr, y1.pu, k1.pr, k1.pu, k1.phi};
+  bhh_dev::hermite_crossing(e, h, r_c, phi_c);
 }
 
-// Root of u on the sub-step bracket [0, h] from y0 (u(h) = u1 of the other
-// sign): Illinois regula falsi, each trial one sub-step re-integrated from y0.
-template <int INTEG>
-__device__ __noinline__ Yd refine_equator(const BhkImageParams &p, const RayC &c, const Yd &y0, double h,
-                                          double u1) {
-  double a = 0.0, fa = y0.u, b = h, fb = u1;
-  int side = 0;
-  Yd yc = y0;
-  for (int i = 0; i < 40; ++i) {
-    double t = (a * fb - b * fa) / (fb - fa);
-    if (!(t > a && t < b)) t = 0.5 * (a + b);
-    yc = sub_step<INTEG>(p, c, y0, t);
-    const double fc = yc.u;
-    if (fabs(fc) < 1e-13) return yc;
-    if ((fc * fb) > 0.0) {
-      b = t;
-      fb = fc;
-      if (side == -1) fa = 0.5 * fa;
-      side = -1;
-    } else {
-      a = t;
-      fa = fc;
-      if (side == 1) fb = 0.5 * fb;
-      side = 1;
-    }
-  }
-  return yc;
-}
-
-// Records a crossing at yc when it lies on the disk; returns true when the
-// ray stops there (last allowed crossing).
+// Records a crossing at (r_c, phi_c) when it lies on the disk; returns true
+// when the ray stops there (last allowed crossing).
 __device__ __forceinline__ bool on_crossing(const BhkImageParams &p, const BhkImageOut &o, RayFp64 &R,
-                                            const Yd &yc) {
-  if (!(yc.r >= p.r_in && yc.r <= p.r_out)) return false;
+                                            double r_c, double phi_c) {
+  if (!(r_c >= p.r_in && r_c <= p.r_out)) return false;
   const int k = R.ncross;
   const long long off = (long long)k * p.n_pix + R.pix;
-  const double g = disk_g(yc.r, p.a, R.c.lam);
-  if (o.r_hit) o.r_hit[off] = yc.r;
-  if (o.phi_hit) o.phi_hit[off] = yc.phi;
+  const double g = disk_g(r_c, p.a, R.c.lam);
+  if (o.r_hit) o.r_hit[off] = r_c;
+  if (o.phi_hit) o.phi_hit[off] = phi_c;
   if (o.g) o.g[off] = g;
-  const double q = p.r_in / yc.r;
+  const double q = p.r_in / r_c;
   const double g2 = g * g;
   R.inten = R.inten + ((((g2 * g2) * q) * q) * q);
-  if (k == 0 && o.flux) o.flux[R.pix] = nt_flux(yc.r, p.nt_isco, p.nt_flux_peak);
+  if (k == 0 && o.flux) o.flux[R.pix] = nt_flux(r_c, p.nt_isco, p.nt_flux_peak);
   R.ncross = k + 1;
   return R.ncross >= p.max_cross;
 }
@@ -152,11 +128,13 @@ __device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOu
     const double hh = p.step_coeff * dmin_(R.y.r, p.step_rcap);
     const double sigma = (R.y.r * R.y.r) + ((p.a2 * R.y.u) * R.y.u);
     const double h = hh / sigma;
-    Yd yn = rk4(R.y, h, R.c, rhs(R.y, R.c));
+    const Yd k0 = rhs(R.y, R.c);
+    Yd yn = rk4(R.y, h, R.c, k0);
     ++R.steps;
     if ((R.y.u * yn.u) < 0.0) {
-      const Yd yc = refine_equator<0>(p, R.c, R.y, h, yn.u);
-      if (on_crossing(p, o, R, yc)) return 1;
+      double r_c, phi_c;
+      step_crossing(R.y, k0, yn, rhs(yn, R.c), h, r_c, phi_c);
+      if (on_crossing(p, o, R, r_c, phi_c)) return 1;
     }
     project(yn, R.c);
     R.y = yn;
@@ -172,8 +150,9 @@ __device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOu
       ++R.steps;
       bool stop = false;
       if ((R.y.u * d.y5.u) < 0.0) {
-        const Yd yc = refine_equator<1>(p, R.c, R.y, R.h, d.y5.u);
-        stop = on_crossing(p, o, R, yc);
+        double r_c, phi_c;
+        step_crossing(R.y, R.k1, d.y5, d.k7, R.h, r_c, phi_c);
+        stop = on_crossing(p, o, R, r_c, phi_c);
       }
       R.y = d.y5;
       R.k1 = d.k7;

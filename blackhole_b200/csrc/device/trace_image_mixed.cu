@@ -3,11 +3,14 @@
 // Same persistent warp-refill structure and trace-loop order as the FP64
 // kernel (trace_image_fp64.cu), with the integration in FP32:
 //   * FP64: per-ray set-up (lambda, eta, q, K, initial momenta from R(r_obs)),
-//     the crossing radius and azimuth handed to the outputs, the redshift g,
-//     the Novikov-Thorne flux and the intensity.
+//     the first-integral projection's R(r) and U(u) (the Carter/energy
+//     constraint check of every accepted step), the crossing radius and
+//     azimuth handed to the outputs, the redshift g, the Novikov-Thorne flux
+//     and the intensity.
 //   * FP32: every right-hand side, the Dormand-Prince / RK4 stages, the error
-//     estimate, the step controller, the first-integral projection and the
-//     crossing refinement.
+//     estimate and the step controller. A detected equatorial crossing is
+//     located by the FP64 Hermite interpolation of hermite.cuh from the
+//     compensated step endpoints.
 //   * Compensated FP32 (hi + lo with TwoSum) for the positions r, u, phi, so
 //     that thousands of small FP32 increments accumulate without drift.
 // The DP45 error estimate is formed from the stage derivatives (h sum e_j k_j),
@@ -18,6 +21,7 @@
 
 #include <cstdio>
 
+#include "hermite.cuh"
 #include "image_mixed.cuh"
 #include "launch.h"
 
@@ -31,7 +35,7 @@ struct RayMx {
   Lof lo;
   Yf k1;       // DP45 FSAL stage
   float h;     // DP45 trial step / unused for RK4
-  double lam;  // lambda in FP64 for g
+  RayCd cd;    // FP64 constants: projection and g
   double inten;
   long long pix;
   int steps;
@@ -65,14 +69,16 @@ __device__ __forceinline__ void init_ray(const BhkImageParams &p, long long pix,
   R.c.K = (float)K;
   R.c.a2_minus_alam = (float)(a * a - a * lam);
   R.c.c_pu = (float)(a * a - qTh);
-  R.c.proj_u = (float)(1e-6 * (fabs(qTh) + a * a));
+  R.cd.a = a;
+  R.cd.lam = lam;
+  R.cd.qTh = qTh;
+  R.cd.K = K;
   split(r0, R.y.r, R.lo.r);
   split(p.cos_o, R.y.u, R.lo.u);
   R.y.phi = 0.0f;
   R.lo.phi = 0.0f;
   R.y.pr = (float)(-sqrt(Rv < 0.0 ? 0.0 : Rv));
   R.y.pu = (float)(beta * p.sin_o);
-  R.lam = lam;
   R.inten = 0.0;
   R.pix = pix;
   R.steps = 0;
@@ -81,44 +87,6 @@ __device__ __forceinline__ void init_ray(const BhkImageParams &p, long long pix,
   const float hh = (float)p.step_coeff * fminf(R.y.r, (float)p.step_rcap);
   R.h = hh / fmaf(R.c.a2 * R.y.u, R.y.u, R.y.r * R.y.r);
   R.k1 = rhs(R.y, R.c);
-}
-
-template <int INTEG>
-__device__ __forceinline__ Yf sub_inc(const BhkImageParams &p, const RayCf &c, const Yf &y, float h) {
-  if (INTEG == 0) return rk4_inc(y, h, c, rhs(y, c));
-  return dp45(y, h, c, rhs(y, c), (float)p.rtol, (float)p.atol, false).d;
-}
-
-// Crossing of u = 0 inside the sub-step bracket [0, h] from (y0, lo0):
-// Illinois regula falsi on u(t) = u0 + lo0.u + du(t); returns the FP64
-// radius and azimuth at the root.
-template <int INTEG>
-__device__ __noinline__ void refine_equator(const BhkImageParams &p, const RayCf &c, const Yf &y0, const Lof &lo0,
-                                            float h, float u1, double &r_c, double &phi_c) {
-  float a = 0.0f, fa = y0.u + lo0.u, b = h, fb = u1;
-  const float tol = 1e-7f * (fabsf(fa) + fabsf(fb));
-  int side = 0;
-  Yf d = sub_inc<INTEG>(p, c, y0, h);
-  for (int i = 0; i < 24; ++i) {
-    float t = __fdividef(fmaf(a, fb, -b * fa), fb - fa);
-    if (!(t > a && t < b)) t = 0.5f * (a + b);
-    d = sub_inc<INTEG>(p, c, y0, t);
-    const float fc = y0.u + (lo0.u + d.u);
-    if (fabsf(fc) <= tol) break;
-    if (fc * fb > 0.0f) {
-      b = t;
-      fb = fc;
-      if (side == -1) fa *= 0.5f;
-      side = -1;
-    } else {
-      a = t;
-      fa = fc;
-      if (side == 1) fb *= 0.5f;
-      side = 1;
-    }
-  }
-  r_c = (double)y0.r + ((double)lo0.r + (double)d.r);
-  phi_c = (double)y0.phi + ((double)lo0.phi + (double)d.phi);
 }
 
 __device__ __forceinline__ double disk_g(double r, double a, double lam) {
@@ -134,7 +102,7 @@ __device__ __forceinline__ bool on_crossing(const BhkImageParams &p, const BhkIm
   if (!(r_c >= p.r_in && r_c <= p.r_out)) return false;
   const int k = R.ncross;
   const long long off = (long long)k * p.n_pix + R.pix;
-  const double g = disk_g(r_c, p.a, R.lam);
+  const double g = disk_g(r_c, p.a, R.cd.lam);
   if (o.r_hit) o.r_hit[off] = r_c;
   if (o.phi_hit) o.phi_hit[off] = phi_c;
   if (o.g) o.g[off] = g;
@@ -178,9 +146,10 @@ __device__ __forceinline__ void finish(const BhkImageParams &p, const BhkImageOu
 
 // Applies an accepted increment d to the ray (compensated positions), tests
 // for an equatorial crossing and records it; returns true if the ray stops.
-template <int INTEG>
+// k0 = rhs(y0); k1 = rhs(y1) when the caller has it (DP45's FSAL stage),
+// else NULL and it is evaluated here only if a crossing needs it.
 __device__ __forceinline__ bool accept(const BhkImageParams &p, const BhkImageOut &o, RayMx &R, const Yf &d,
-                                       float h) {
+                                       float h, const Yf &k0, const Yf *k1) {
   const Yf y0 = R.y;
   const Lof lo0 = R.lo;
   comp_add(R.y.r, R.lo.r, d.r);
@@ -191,11 +160,18 @@ __device__ __forceinline__ bool accept(const BhkImageParams &p, const BhkImageOu
   ++R.steps;
   bool stop = false;
   if ((y0.u + lo0.u) * (R.y.u + R.lo.u) < 0.0f) {
+    const Yf kk = k1 ? *k1 : rhs(R.y, R.c);
+    const bhh_dev::Ends e{to_f64(y0.r, lo0.r),   to_f64(y0.u, lo0.u),   to_f64(y0.phi, lo0.phi),
+                          (double)y0.pr,         (double)y0.pu,         (double)k0.pr,
+                          (double)k0.pu,         (double)k0.phi,        to_f64(R.y.r, R.lo.r),
+                          to_f64(R.y.u, R.lo.u), to_f64(R.y.phi, R.lo.phi), (double)R.y.pr,
+                          (double)R.y.pu,        (double)kk.pr,         (double)kk.pu,
+                          (double)kk.phi};
     double r_c, phi_c;
-    refine_equator<INTEG>(p, R.c, y0, lo0, h, R.y.u + R.lo.u, r_c, phi_c);
+    bhh_dev::hermite_crossing(e, (double)h, r_c, phi_c);
     stop = on_crossing(p, o, R, r_c, phi_c);
   }
-  project(R.y, R.c);
+  project(R.y, R.lo, R.cd);
   return stop;
 }
 
@@ -208,8 +184,9 @@ __device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOu
     if (R.y.r >= r_esc) return 2;
     const float hh = (float)p.step_coeff * fminf(R.y.r, (float)p.step_rcap);
     const float h = __fdividef(hh, fmaf(R.c.a2 * R.y.u, R.y.u, R.y.r * R.y.r));
-    const Yf d = rk4_inc(R.y, h, R.c, rhs(R.y, R.c));
-    return accept<0>(p, o, R, d, h) ? 1 : -1;
+    const Yf k0 = rhs(R.y, R.c);
+    const Yf d = rk4_inc(R.y, h, R.c, k0);
+    return accept(p, o, R, d, h, k0, nullptr) ? 1 : -1;
   } else {
     const long long max_attempts = 4LL * p.max_steps + 64;
     if (R.steps >= p.max_steps || R.attempts >= max_attempts) return 3;
@@ -219,7 +196,7 @@ __device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOu
     const DPf d = dp45(R.y, R.h, R.c, R.k1, (float)p.rtol, (float)p.atol, true);
     if (d.err <= 1.0f) {
       const float h = R.h;
-      const bool stop = accept<1>(p, o, R, d.d, h);
+      const bool stop = accept(p, o, R, d.d, h, R.k1, &d.k7);
       R.k1 = d.k7;
       R.k1.r = R.y.pr;  // projection moved only the momenta
       R.k1.u = R.y.pu;

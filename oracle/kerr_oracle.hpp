@@ -24,8 +24,8 @@
 //     or Dormand & Prince (1980) 5(4) with the step controller of Hairer,
 //     Norsett & Wanner (1993) II.4 (safety 0.9, factor in [0.1, 2]) as the
 //     reference states it in src/physics/verified/rk4.h:254-265;
-//   - equatorial crossings refined on a bracket like bisectRadialCrossing
-//     (src/physics/event_detection.h:127-180), with Illinois regula falsi;
+//   - equatorial crossings located inside the accepted step by quintic
+//     Hermite interpolation, root bracketed as in event_detection.h:127-180;
 //   - Keplerian redshift g = 1 / (u^t (1 - Omega lambda)) with the
 //     Bardeen-Press-Teukolsky (1972) u^t and Omega (as in src/physics/iron_kline.h:25-40).
 // Templated on the scalar so that a counting scalar can count its FLOPs and
@@ -555,39 +555,83 @@ template <class T> inline T mino_step(const Scene &s, const Y<T> &y, T a) {
   return h / sigma;
 }
 
-// Locate the equatorial crossing u = 0 inside a step of size h from y0
-// (u(0) = y0.u and u(h) = u1 of opposite signs). The bracket [0, h] on the
-// sub-step is refined like bisectRadialCrossing (event_detection.h:127-180),
-// but with the Illinois variant of regula falsi (Dowell & Jarratt 1971):
-// the trial point interpolates the bracket's u values, and the value kept
-// twice in a row is halved, which keeps superlinear convergence (about 6
-// sub-steps to |u| < 1e-13 against about 40 for bisection). Every trial
-// re-integrates from y0 with one sub-step; returns the state at the root.
-inline constexpr int kRootMaxIter = 40;
+// ---------------------------------------------------------------------------
+// Equatorial crossing by Hermite interpolation of the accepted step.
+//
+// In the second-order form every position x in {r, u} has x' = p_x and
+// x'' = F_x(position) known at both ends of a step (F from the right-hand
+// side at y0 and at y1), so the quintic Hermite interpolant through (x, h x',
+// h^2 x'') at t = 0 and t = 1 approximates x(t0 + t h) with an error of
+// O(h^6) -- below the step's own truncation error -- without any further
+// integration. phi' is known at both ends: cubic Hermite. The root of u on
+// [0, 1] is bracketed by u0, u1 of opposite signs and found with the
+// Illinois variant of regula falsi (Dowell & Jarratt 1971) on the polynomial
+// (the bracketing pattern of bisectRadialCrossing, event_detection.h:127-180).
+// ---------------------------------------------------------------------------
+template <class T> struct Quintic { T c0, c1, c2, c3, c4, c5; };
 
-template <class T, class Stepper>
-inline Y<T> refine_equator(const Y<T> &y0, T h, T u1, const Stepper &step) {
-  T a = T(0), fa = y0.u, b = h, fb = u1;
+template <class T> inline Quintic<T> quintic_hermite(T p0, T v0, T a0, T p1, T v1, T a1) {
+  const T A = ((p1 - p0) - v0) - T(0.5) * a0;
+  const T B = (v1 - v0) - a0;
+  const T Cc = a1 - a0;
+  Quintic<T> q;
+  q.c0 = p0;
+  q.c1 = v0;
+  q.c2 = T(0.5) * a0;
+  q.c3 = (T(10) * A - T(4) * B) + T(0.5) * Cc;
+  q.c4 = (T(7) * B - T(15) * A) - Cc;
+  q.c5 = (T(6) * A - T(3) * B) + T(0.5) * Cc;
+  return q;
+}
+
+template <class T> inline T eval_quintic(const Quintic<T> &q, T t) {
+  return q.c0 + t * (q.c1 + t * (q.c2 + t * (q.c3 + t * (q.c4 + t * q.c5))));
+}
+
+template <class T> inline T eval_cubic_hermite(T p0, T v0, T p1, T v1, T t) {
+  const T A = (p1 - p0) - v0;
+  const T B = v1 - v0;
+  const T c2 = T(3) * A - B;
+  const T c3 = B - T(2) * A;
+  return p0 + t * (v0 + t * (c2 + t * c3));
+}
+
+inline constexpr int kRootMaxIter = 60;
+
+// Crossing state (r, phi) of the step y0 -> y1 of Mino size h, k0 = rhs(y0),
+// k1 = rhs(y1) (y1 before projection).
+template <class T>
+inline Y<T> hermite_crossing(const Y<T> &y0, const Y<T> &k0, const Y<T> &y1, const Y<T> &k1, T h) {
+  const T h2 = h * h;
+  const Quintic<T> qu = quintic_hermite(y0.u, h * y0.pu, h2 * k0.pu, y1.u, h * y1.pu, h2 * k1.pu);
+  T a = T(0), fa = y0.u, b = T(1), fb = y1.u;
+  const T tol = T(1e-15) * (s_abs(fa) + s_abs(fb));
   int side = 0;
-  Y<T> yc = y0;
+  T t = T(0.5);
   for (int i = 0; i < kRootMaxIter; ++i) {
-    T c = (a * fb - b * fa) / (fb - fa);
-    if (!(c > a && c < b)) c = T(0.5) * (a + b);
-    yc = step(y0, c);
-    const T fc = yc.u;
-    if (s_abs(fc) < T(1e-13)) return yc;
+    t = (a * fb - b * fa) / (fb - fa);
+    if (!(t > a && t < b)) t = T(0.5) * (a + b);
+    const T fc = eval_quintic(qu, t);
+    if (s_abs(fc) <= tol) break;
     if ((fc * fb) > T(0)) {
-      b = c;
+      b = t;
       fb = fc;
       if (side == -1) fa = T(0.5) * fa;
       side = -1;
     } else {
-      a = c;
+      a = t;
       fa = fc;
       if (side == 1) fb = T(0.5) * fb;
       side = 1;
     }
   }
+  const Quintic<T> qr = quintic_hermite(y0.r, h * y0.pr, h2 * k0.pr, y1.r, h * y1.pr, h2 * k1.pr);
+  Y<T> yc;
+  yc.r = eval_quintic(qr, t);
+  yc.u = eval_quintic(qu, t);
+  yc.phi = eval_cubic_hermite(y0.phi, h * k0.phi, y1.phi, h * k1.phi, t);
+  yc.pr = T(0);
+  yc.pu = T(0);
   return yc;
 }
 
@@ -625,16 +669,16 @@ inline PixelResult<T> trace_pixel(const Scene &s, const SceneDerived<T> &d, T al
   };
 
   if (s.integrator == 0) {
-    auto step = [&](const Y<T> &ya, T h) { return img_rk4(ya, h, f, f(ya)); };
     for (;;) {
       if (out.steps >= s.max_steps) { out.cls = CLS_MAX_STEPS; break; }
       if (y.r <= d.r_hor) { out.cls = CLS_CAPTURED; break; }
       if (y.r >= d.r_esc) { out.cls = CLS_ESCAPED; finish_escape(y); break; }
       const T h = mino_step(s, y, d.a);
-      Y<T> yn = img_rk4(y, h, f, f(y));
+      const Y<T> k0 = f(y);
+      Y<T> yn = img_rk4(y, h, f, k0);
       ++out.steps;
       if ((y.u * yn.u) < T(0)) {
-        const Y<T> yc = refine_equator(y, h, yn.u, step);
+        const Y<T> yc = hermite_crossing(y, k0, yn, f(yn), h);
         if (in_disk(yc.r)) {
           record_crossing(s, d, c, yc, out);
           if (out.n_cross >= maxc) { out.cls = CLS_DISK; break; }
@@ -645,9 +689,6 @@ inline PixelResult<T> trace_pixel(const Scene &s, const SceneDerived<T> &d, T al
     }
   } else {
     const T rtol = T(s.rtol), atol = T(s.atol);
-    auto step = [&](const Y<T> &ya, T h) {
-      return img_dp45(ya, h, f, f(ya), rtol, atol, false).y5;
-    };
     T h = mino_step(s, y, d.a);
     Y<T> k1 = f(y);
     int64_t attempts = 0;
@@ -663,7 +704,7 @@ inline PixelResult<T> trace_pixel(const Scene &s, const SceneDerived<T> &d, T al
       if (err <= T(1)) {
         ++out.steps;
         if ((y.u * o.y5.u) < T(0)) {
-          const Y<T> yc = refine_equator(y, h, o.y5.u, step);
+          const Y<T> yc = hermite_crossing(y, k1, o.y5, o.k7, h);
           if (in_disk(yc.r)) {
             record_crossing(s, d, c, yc, out);
             if (out.n_cross >= maxc) { out.cls = CLS_DISK; stop = true; }
