@@ -48,6 +48,7 @@ WORKLOADS = {
                    frames=[(a, i) for a in (0.0, 0.5, 0.9, 0.998) for i in (17.0, 45.0, 75.0, 85.0)]),
     "c0_256": dict(width=256, height=256, integrator=0, max_crossings=1, frames=[(0.9, 60.0)]),
     "disk1_512": dict(width=512, height=512, integrator=1, max_crossings=3, frames=[(0.9, 45.0)]),
+    "disk1_1024": dict(width=1024, height=1024, integrator=1, max_crossings=3, frames=[(0.9, 45.0)]),
     "disk_2048": dict(width=2048, height=2048, integrator=0, max_crossings=1, frames=[(0.9, 60.0)]),
 }
 OUT_FIELDS_USED = ("cls", "steps", "n_cross", "r_hit", "phi_hit", "g", "intensity", "theta_inf", "phi_inf")

@@ -66,7 +66,7 @@ __device__ __forceinline__ void hermite_crossing(const Ends &e, double h, double
     t = (a * fb - b * fa) / (fb - fa);
     if (!(t > a && t < b)) t = 0.5 * (a + b);
     const double fc = eval_quintic(qu, t);
-    if (fabs(fc) <= tol) break;
+    if (fabs(fc) <= tol || (b - a) <= 1e-14) break;
     if ((fc * fb) > 0.0) {
       b = t;
       fb = fc;

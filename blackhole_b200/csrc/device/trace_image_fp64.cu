@@ -57,6 +57,7 @@ __device__ __forceinline__ void init_ray(const BhkImageParams &p, long long pix,
   R.ncross = 0;
   R.inten = 0.0;
   R.pix = pix;
+  project(R.y, R.c);  // idempotent from here on (see iterate)
   if (p.integrator == 1) {
     const double hh = p.step_coeff * dmin_(R.y.r, p.step_rcap);
     const double sigma = (R.y.r * R.y.r) + ((p.a2 * R.y.u) * R.y.u);
@@ -146,25 +147,26 @@ __device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOu
     if (R.y.r >= p.r_esc) return 2;
     ++R.attempts;
     const DPRes d = dp45(R.y, R.h, R.c, R.k1, p.rtol, p.atol, true);
-    if (d.err <= 1.0) {
+    // Accepted and rejected lanes run the same instructions: a rejected lane
+    // keeps its state and re-projects it, which is exact no-op because every
+    // state is already on its first integrals (projected at set-up).
+    const bool acc = d.err <= 1.0;
+    bool stop = false;
+    if (acc) {
       ++R.steps;
-      bool stop = false;
       if ((R.y.u * d.y5.u) < 0.0) {
         double r_c, phi_c;
         step_crossing(R.y, R.k1, d.y5, d.k7, R.h, r_c, phi_c);
         stop = on_crossing(p, o, R, r_c, phi_c);
       }
-      R.y = d.y5;
-      R.k1 = d.k7;
-      project(R.y, R.c);
-      R.k1.r = R.y.pr;  // projection moves only the momenta
-      R.k1.u = R.y.pu;
-      R.h = R.h * step_factor(d.err, true);
-      if (stop) return 1;
-    } else {
-      R.h = R.h * step_factor(d.err, false);
     }
-    return -1;
+    R.y = acc ? d.y5 : R.y;
+    R.k1 = acc ? d.k7 : R.k1;
+    project(R.y, R.c);
+    R.k1.r = R.y.pr;  // projection moves only the momenta
+    R.k1.u = R.y.pu;
+    R.h = R.h * step_factor(d.err, acc);
+    return stop ? 1 : -1;
   }
 }
 

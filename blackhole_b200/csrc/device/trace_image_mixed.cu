@@ -84,6 +84,7 @@ __device__ __forceinline__ void init_ray(const BhkImageParams &p, long long pix,
   R.steps = 0;
   R.attempts = 0;
   R.ncross = 0;
+  project(R.y, R.lo, R.cd);  // idempotent from here on (see iterate)
   const float hh = (float)p.step_coeff * fminf(R.y.r, (float)p.step_rcap);
   R.h = hh / fmaf(R.c.a2 * R.y.u, R.y.u, R.y.r * R.y.r);
   R.k1 = rhs(R.y, R.c);
@@ -144,22 +145,25 @@ __device__ __forceinline__ void finish(const BhkImageParams &p, const BhkImageOu
   if (o.phi_inf) o.phi_inf[pix] = ph;
 }
 
-// Applies an accepted increment d to the ray (compensated positions), tests
-// for an equatorial crossing and records it; returns true if the ray stops.
-// k0 = rhs(y0); k1 = rhs(y1) when the caller has it (DP45's FSAL stage),
-// else NULL and it is evaluated here only if a crossing needs it.
+// Applies the increment d of an accepted step (acc) to the ray: compensated
+// positions, crossing test and record, projection; returns true if the ray
+// stops. A rejected attempt (acc false) runs the same instructions with a
+// zero increment -- adding 0 leaves a compensated pair unchanged and the
+// projection is idempotent on a projected state -- so accepted and rejected
+// lanes of a warp never diverge. k0 = rhs(y0); k1 = rhs(y1) when the caller
+// has it (DP45's FSAL stage), else NULL and evaluated only at a crossing.
 __device__ __forceinline__ bool accept(const BhkImageParams &p, const BhkImageOut &o, RayMx &R, const Yf &d,
-                                       float h, const Yf &k0, const Yf *k1) {
+                                       bool acc, float h, const Yf &k0, const Yf *k1) {
   const Yf y0 = R.y;
   const Lof lo0 = R.lo;
-  comp_add(R.y.r, R.lo.r, d.r);
-  comp_add(R.y.u, R.lo.u, d.u);
-  comp_add(R.y.phi, R.lo.phi, d.phi);
-  R.y.pr += d.pr;
-  R.y.pu += d.pu;
-  ++R.steps;
+  comp_add(R.y.r, R.lo.r, acc ? d.r : 0.0f);
+  comp_add(R.y.u, R.lo.u, acc ? d.u : 0.0f);
+  comp_add(R.y.phi, R.lo.phi, acc ? d.phi : 0.0f);
+  R.y.pr += acc ? d.pr : 0.0f;
+  R.y.pu += acc ? d.pu : 0.0f;
+  R.steps += acc ? 1 : 0;
   bool stop = false;
-  if ((y0.u + lo0.u) * (R.y.u + R.lo.u) < 0.0f) {
+  if (acc && (y0.u + lo0.u) * (R.y.u + R.lo.u) < 0.0f) {
     const Yf kk = k1 ? *k1 : rhs(R.y, R.c);
     const bhh_dev::Ends e{to_f64(y0.r, lo0.r),   to_f64(y0.u, lo0.u),   to_f64(y0.phi, lo0.phi),
                           (double)y0.pr,         (double)y0.pu,         (double)k0.pr,
@@ -177,7 +181,7 @@ __device__ __forceinline__ bool accept(const BhkImageParams &p, const BhkImageOu
 
 template <int INTEG>
 __device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOut &o, RayMx &R, float r_hor,
-                                       float r_esc) {
+                                       float r_esc, float rtol, float atol) {
   if (INTEG == 0) {
     if (R.steps >= p.max_steps) return 3;
     if (R.y.r <= r_hor) return 0;
@@ -186,26 +190,22 @@ __device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOu
     const float h = __fdividef(hh, fmaf(R.c.a2 * R.y.u, R.y.u, R.y.r * R.y.r));
     const Yf k0 = rhs(R.y, R.c);
     const Yf d = rk4_inc(R.y, h, R.c, k0);
-    return accept(p, o, R, d, h, k0, nullptr) ? 1 : -1;
+    return accept(p, o, R, d, true, h, k0, nullptr) ? 1 : -1;
   } else {
     const long long max_attempts = 4LL * p.max_steps + 64;
     if (R.steps >= p.max_steps || R.attempts >= max_attempts) return 3;
     if (R.y.r <= r_hor) return 0;
     if (R.y.r >= r_esc) return 2;
     ++R.attempts;
-    const DPf d = dp45(R.y, R.h, R.c, R.k1, (float)p.rtol, (float)p.atol, true);
-    if (d.err <= 1.0f) {
-      const float h = R.h;
-      const bool stop = accept(p, o, R, d.d, h, R.k1, &d.k7);
-      R.k1 = d.k7;
-      R.k1.r = R.y.pr;  // projection moved only the momenta
-      R.k1.u = R.y.pu;
-      R.h = h * step_factor(d.err, true);
-      if (stop) return 1;
-    } else {
-      R.h = R.h * step_factor(d.err, false);
-    }
-    return -1;
+    const DPf d = dp45(R.y, R.h, R.c, R.k1, rtol, atol, true);
+    const bool acc = d.err <= 1.0f;
+    const float h = R.h;
+    const bool stop = accept(p, o, R, d.d, acc, h, R.k1, &d.k7);
+    R.k1 = acc ? d.k7 : R.k1;
+    R.k1.r = R.y.pr;  // projection moved only the momenta
+    R.k1.u = R.y.pu;
+    R.h = h * step_factor(d.err, acc);
+    return stop ? 1 : -1;
   }
 }
 
@@ -215,6 +215,7 @@ __global__ void __launch_bounds__(128) k_trace_image_mixed(const BhkImageParams 
   const unsigned lane = threadIdx.x & 31u;
   const unsigned lanemask_lt = (1u << lane) - 1u;
   const float r_hor = (float)p.r_hor, r_esc = (float)p.r_esc;
+  const float rtol = (float)p.rtol, atol = (float)p.atol;
   RayMx R;
   bool active = false;
   bool exhausted = false;
@@ -237,7 +238,7 @@ __global__ void __launch_bounds__(128) k_trace_image_mixed(const BhkImageParams 
     }
     if (!__any_sync(kFull, active)) break;
     if (active) {
-      const int cls = iterate<INTEG>(p, o, R, r_hor, r_esc);
+      const int cls = iterate<INTEG>(p, o, R, r_hor, r_esc, rtol, atol);
       if (cls >= 0) {
         finish(p, o, R, cls);
         active = false;

@@ -566,7 +566,8 @@ template <class T> inline T mino_step(const Scene &s, const Y<T> &y, T a) {
 // integration. phi' is known at both ends: cubic Hermite. The root of u on
 // [0, 1] is bracketed by u0, u1 of opposite signs and found with the
 // Illinois variant of regula falsi (Dowell & Jarratt 1971) on the polynomial
-// (the bracketing pattern of bisectRadialCrossing, event_detection.h:127-180).
+// (the bracketing pattern of bisectRadialCrossing, event_detection.h:127-180),
+// stopping at |u| <= 1e-15 (|u0| + |u1|) or a bracket narrower than 1e-14.
 // ---------------------------------------------------------------------------
 template <class T> struct Quintic { T c0, c1, c2, c3, c4, c5; };
 
@@ -612,7 +613,7 @@ inline Y<T> hermite_crossing(const Y<T> &y0, const Y<T> &k0, const Y<T> &y1, con
     t = (a * fb - b * fa) / (fb - fa);
     if (!(t > a && t < b)) t = T(0.5) * (a + b);
     const T fc = eval_quintic(qu, t);
-    if (s_abs(fc) <= tol) break;
+    if (s_abs(fc) <= tol || (b - a) <= T(1e-14)) break;
     if ((fc * fb) > T(0)) {
       b = t;
       fb = fc;
@@ -661,6 +662,10 @@ inline PixelResult<T> trace_pixel(const Scene &s, const SceneDerived<T> &d, T al
   Y<T> y;
   init_ray(d, s, alpha, beta, c, y);
   const auto f = make_rhs(c);
+  // Start on the first integrals too: the projection is then idempotent on
+  // any state it has produced, so re-applying it to an unchanged state (a
+  // rejected DP45 attempt on the GPU) changes nothing.
+  f.project(y);
   const int maxc = std::max(1, std::min(3, int(s.max_crossings)));
   auto in_disk = [&](T r) { return r >= d.r_in && r <= d.r_out; };
   auto finish_escape = [&](const Y<T> &yy) {
