@@ -7,7 +7,8 @@
 //   r'  = p_r          p_r' = R'(r)/2 = 2 r A - (r - 1) K,  K = q_R + (lambda - a)^2
 //   u'  = p_u          p_u' = U'(u)/2 = u (a^2 - q_Th - 2 a^2 u^2),
 //                      U(u) = sin^2 Theta = (q_Th + a^2 u^2)(1 - u^2) - lambda^2
-//   phi' = -(lambda / sin^2 - a + a A / Delta)   (kerr.cpp:61, time-reversed)
+//   psi' = a - lambda / sin^2 - a (A + p_r) / Delta  (psi = phi - a G(r), G' = 1/Delta:
+//          kerr.cpp:61 time-reversed, made regular at the horizon)
 // Every expression is written in a fixed evaluation order and the translation
 // units that include this header are compiled with -fmad=false, so each FP64
 // operation rounds exactly once, as on the CPU: results are bit-identical to
@@ -40,8 +41,22 @@ __device__ __forceinline__ Yd rhs(const Yd &y, const RayC &c) {
   d.u = y.pu;
   d.pr = ((2.0 * r) * A) - ((r - 1.0) * c.K);
   d.pu = u * ((c.a2 - c.qTh) - ((2.0 * c.a2) * u2));
-  d.phi = -(((c.lam / s2) - c.a) + ((c.a * A) / D));
+  // horizon-regular azimuth psi = phi - a G(r), G' = 1/Delta: psi' = a -
+  // lambda/sin^2 - a (A + p_r)/Delta, with (A + p_r)/Delta = K/(A - p_r) on
+  // the first integral for ingoing rays (the rationalization of the
+  // reference's GPU step, src/cuda/device_physics.cuh:453-525)
+  const bool in = y.pr < 0.0;
+  const double num = in ? c.K : (A + y.pr);
+  const double den = in ? (A - y.pr) : D;
+  d.phi = (c.a - (c.lam / s2)) - (c.a * (num / den));
   return d;
+}
+
+// phi = psi + a (G(r) - G(r_obs)), G(r) = ln((r - r+)/(r - r-)) / (r+ - r-).
+__device__ __forceinline__ double phi_of_psi(double psi, double r, const BhkImageParams &p) {
+  if (p.a == 0.0) return psi;
+  const double q = ((r - p.r_plus) * (p.r_obs - p.r_minus)) / ((r - p.r_minus) * (p.r_obs - p.r_plus));
+  return psi + p.a * (log(q) / (p.r_plus - p.r_minus));
 }
 
 __device__ __forceinline__ Yd axpy(const Yd &y, double h, const Yd &k) {

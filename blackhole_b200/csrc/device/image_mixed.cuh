@@ -2,9 +2,8 @@
 //
 // Same Mino-time second-order system as image_fp64.cuh, evaluated in FP32:
 //   p_r' = 2 r A - (r - 1) K, p_u' = u (a^2 - q_Th - 2 a^2 u^2),
-//   phi' = -(lambda / sin^2 + a (2r - a lambda) / Delta)
-// (the reference's -a + a A/Delta rewritten with A - Delta = 2r - a lambda,
-// so the two quotients share one division). Positions r, u, phi carry an
+//   psi' = a - lambda / sin^2 - a (A + p_r) / Delta (horizon-regular azimuth,
+// rationalized for ingoing rays; both quotients share one division). Positions r, u, phi carry an
 // FP32 compensation term (TwoSum), so the accumulated position keeps ~48
 // bits while each step's increment is computed in FP32; the momenta are
 // reset to the first integrals every accepted step (projection), so they
@@ -41,8 +40,12 @@ __device__ __forceinline__ Yf rhs(const Yf &y, const RayCf &c) {
   d.u = y.pu;
   d.pr = fmaf(2.0f * r, A, -(r - 1.0f) * c.K);
   d.pu = u * fmaf(-2.0f * c.a2, u2, c.c_pu);
-  const float num = fmaf(c.lam, D, c.a * fmaf(2.0f, r, -c.a * c.lam) * s2);
-  d.phi = -__fdividef(num, s2 * D);
+  // psi' = a - lambda/s2 - a num/den (image_fp64.cuh), as one quotient:
+  // (s2 a (den - num) - lambda den) / (s2 den)
+  const bool in = y.pr < 0.0f;
+  const float num = in ? c.K : (A + y.pr);
+  const float den = in ? (A - y.pr) : D;
+  d.phi = __fdividef(fmaf(s2, c.a * (den - num), -c.lam * den), s2 * den);
   return d;
 }
 
@@ -174,8 +177,12 @@ __device__ __forceinline__ DPf dp45(const Yf &y, float h, const RayCf &c, const 
   // The FP32 estimate h sum e_j k_j carries rounding noise ~1e-8 |y5 - y|;
   // where rtol |y| falls below that (momenta near a turning point, phi near
   // its start value of 0) the floor keeps the controller from chasing it.
+  // Near a pole, lambda / sin^2 inherits the FP32 rounding of u as a
+  // relative error ~6e-8 / (1 - |u|), hence the wider floor for psi there.
 #define BHM_Q(f) __fdividef(BHM_E(f), fmaf(1e-7f, fabsf(o.d.f), fmaf(rtol, fmaxf(fabsf(y.f), fabsf(y5.f)), atol)))
-  const float q0 = BHM_Q(r), q1 = BHM_Q(u), q2 = BHM_Q(phi), q3 = BHM_Q(pr), q4 = BHM_Q(pu);
+  const float q0 = BHM_Q(r), q1 = BHM_Q(u), q3 = BHM_Q(pr), q4 = BHM_Q(pu);
+  const float pole = 1e-7f + __fdividef(1e-8f, fmaxf(1.0f - fabsf(y.u), 1e-7f));
+  const float q2 = __fdividef(BHM_E(phi), fmaf(pole, fabsf(o.d.phi), fmaf(rtol, fmaxf(fabsf(y.phi), fabsf(y5.phi)), atol)));
 #undef BHM_Q
 #undef BHM_E
   o.err = sqrtf(0.2f * fmaf(q0, q0, fmaf(q1, q1, fmaf(q2, q2, fmaf(q3, q3, q4 * q4)))));

@@ -15,6 +15,7 @@ extern "C" {
 typedef struct BhkImageParams {
   double a, a2;            // spin and spin^2
   double r_obs;
+  double r_plus, r_minus;  // outer / inner horizon (azimuth conversion)
   double r_hor;            // horizon_factor * r_+
   double r_esc;            // escape_factor * r_obs
   double r_in, r_out;      // disk edges

@@ -84,7 +84,7 @@ __device__ __forceinline__ bool on_crossing(const BhkImageParams &p, const BhkIm
   const long long off = (long long)k * p.n_pix + R.pix;
   const double g = disk_g(r_c, p.a, R.c.lam);
   if (o.r_hit) o.r_hit[off] = r_c;
-  if (o.phi_hit) o.phi_hit[off] = phi_c;
+  if (o.phi_hit) o.phi_hit[off] = phi_of_psi(phi_c, r_c, p);
   if (o.g) o.g[off] = g;
   const double q = p.r_in / r_c;
   const double g2 = g * g;
@@ -112,7 +112,7 @@ __device__ __forceinline__ void finish(const BhkImageParams &p, const BhkImageOu
   if (cls == 2) {
     const double u = R.y.u;
     th = acos((u < -1.0) ? -1.0 : ((1.0 < u) ? 1.0 : u));
-    ph = R.y.phi;
+    ph = phi_of_psi(R.y.phi, R.y.r, p);
   }
   if (o.theta_inf) o.theta_inf[pix] = th;
   if (o.phi_inf) o.phi_inf[pix] = ph;

@@ -90,6 +90,13 @@ __device__ __forceinline__ void init_ray(const BhkImageParams &p, long long pix,
   R.k1 = rhs(R.y, R.c);
 }
 
+// phi = psi + a (G(r) - G(r_obs)) at the outputs (image_fp64.cuh).
+__device__ __forceinline__ double phi_of_psi(double psi, double r, const BhkImageParams &p) {
+  if (p.a == 0.0) return psi;
+  const double q = ((r - p.r_plus) * (p.r_obs - p.r_minus)) / ((r - p.r_minus) * (p.r_obs - p.r_plus));
+  return psi + p.a * (log(q) / (p.r_plus - p.r_minus));
+}
+
 __device__ __forceinline__ double disk_g(double r, double a, double lam) {
   const double x = sqrt(r);
   const double x3 = x * x * x;
@@ -105,7 +112,7 @@ __device__ __forceinline__ bool on_crossing(const BhkImageParams &p, const BhkIm
   const long long off = (long long)k * p.n_pix + R.pix;
   const double g = disk_g(r_c, p.a, R.cd.lam);
   if (o.r_hit) o.r_hit[off] = r_c;
-  if (o.phi_hit) o.phi_hit[off] = phi_c;
+  if (o.phi_hit) o.phi_hit[off] = phi_of_psi(phi_c, r_c, p);
   if (o.g) o.g[off] = g;
   const double q = p.r_in / r_c;
   const double g2 = g * g;
@@ -139,7 +146,7 @@ __device__ __forceinline__ void finish(const BhkImageParams &p, const BhkImageOu
   if (cls == 2) {
     const double u = to_f64(R.y.u, R.lo.u);
     th = acos(fmin(1.0, fmax(-1.0, u)));
-    ph = to_f64(R.y.phi, R.lo.phi);
+    ph = phi_of_psi(to_f64(R.y.phi, R.lo.phi), to_f64(R.y.r, R.lo.r), p);
   }
   if (o.theta_inf) o.theta_inf[pix] = th;
   if (o.phi_inf) o.phi_inf[pix] = ph;

@@ -144,6 +144,8 @@ static BhkImageParams make_params(const BH_KerrScene *s) {
   p.a = s->spin;
   p.a2 = s->spin * s->spin;
   p.r_obs = s->r_obs;
+  p.r_plus = k.r_plus;
+  p.r_minus = k.r_minus;
   p.r_hor = k.r_hor;
   p.r_esc = k.r_esc;
   p.r_in = k.r_in;

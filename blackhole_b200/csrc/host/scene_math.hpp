@@ -50,12 +50,13 @@ inline double nt_isco(double aStar) {
 }
 
 struct SceneConstants {
-  double r_plus, r_hor, r_esc, r_in, sin_o, cos_o, nt_isco, nt_flux_peak;
+  double r_plus, r_minus, r_hor, r_esc, r_in, sin_o, cos_o, nt_isco, nt_flux_peak;
 };
 
 inline SceneConstants scene_constants(const BH_KerrScene &s) {
   SceneConstants k{};
   k.r_plus = outer_horizon(1.0, s.spin);
+  k.r_minus = 1.0 - std::sqrt(1.0 - s.spin * s.spin);
   k.r_hor = s.horizon_factor * k.r_plus;
   k.r_esc = s.escape_factor * s.r_obs;
   k.r_in = (s.disk_r_in > 0) ? s.disk_r_in : isco_prograde(1.0, s.spin);

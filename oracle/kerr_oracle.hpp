@@ -315,10 +315,19 @@ template <class T> inline T pot_U(T u, const RayConsts<T> &c) {
 }
 
 // Right-hand side in Mino time sigma for a ray traced BACKWARD from the
-// observer: r' = p_r, u' = p_u, p_r' = R'(r)/2, p_u' = U'(u)/2 and
-// phi' = -Phi with Phi = lam / sin^2 - a + a A / Delta the forward-time rate
-// of kerr.cpp:61 (E = 1); the minus sign reverses time along the ray so phi
-// is the physical azimuth of the emitter.
+// observer: r' = p_r, u' = p_u, p_r' = R'(r)/2, p_u' = U'(u)/2.
+//
+// Azimuth. With Phi = lam / sin^2 - a + a A / Delta the forward-time rate of
+// kerr.cpp:61 (E = 1), the emitter's azimuth obeys phi' = -Phi (time reversed
+// along the ray), which diverges as 1/Delta at the horizon. The state carries
+// instead psi = phi - a G(r), G' = 1/Delta (the horizon-regular azimuth the
+// reference's GPU step uses, src/cuda/device_physics.cuh:453-525):
+//   psi' = -lam / sin^2 + a - a (A + p_r) / Delta,
+// and on the first integral p_r^2 = R, A^2 - R = Delta K gives
+//   (A + p_r) / Delta = K / (A - p_r),
+// finite at the horizon for an ingoing ray (p_r < 0); that form is used there
+// and (A + p_r) / Delta for outgoing rays (which stay off the horizon).
+// phi = psi + a (G(r) - G(r_obs)) is restored at the outputs (phi_of_psi).
 template <class T> inline Y<T> img_rhs(const Y<T> &y, const RayConsts<T> &c) {
   const T r = y.r, u = y.u;
   const T a2 = c.a * c.a;
@@ -331,8 +340,18 @@ template <class T> inline Y<T> img_rhs(const Y<T> &y, const RayConsts<T> &c) {
   d.u = y.pu;
   d.pr = T(2) * r * A - (r - T(1)) * c.K;                  // R'(r) / 2
   d.pu = u * (a2 - c.qTh - T(2) * a2 * u2);                // U'(u) / 2
-  d.phi = -(c.lam / s2 - c.a + c.a * A / D);
+  const bool in = y.pr < T(0);
+  const T num = in ? c.K : (A + y.pr);
+  const T den = in ? (A - y.pr) : D;
+  d.phi = (c.a - c.lam / s2) - c.a * (num / den);
   return d;
+}
+
+// phi = psi + a (G(r) - G(r_obs)), G(r) = ln((r - r+) / (r - r-)) / (r+ - r-).
+template <class T> inline T phi_of_psi(T psi, T r, T r_obs, T a, T r_plus, T r_minus) {
+  if (a == T(0)) return psi;
+  const T q = ((r - r_plus) * (r_obs - r_minus)) / ((r - r_minus) * (r_obs - r_plus));
+  return psi + a * (T(std::log(double(q))) / (r_plus - r_minus));
 }
 
 template <class T> inline Y<T> y_axpy(const Y<T> &y, T h, const Y<T> &k) {
@@ -504,13 +523,14 @@ template <class T> struct PixelResult {
 
 // Derived per-scene constants.
 template <class T> struct SceneDerived {
-  T a, r_plus, r_hor, r_esc, r_in, r_out, sin_o, cos_o, u_o;
+  T a, r_plus, r_minus, r_hor, r_esc, r_in, r_out, sin_o, cos_o, u_o;
 };
 
 template <class T> inline SceneDerived<T> derive(const Scene &s) {
   SceneDerived<T> d{};
   d.a = T(s.spin);
   d.r_plus = outer_horizon_geom(T(1), d.a);
+  d.r_minus = T(1) - s_sqrt(T(1) - d.a * d.a);
   d.r_hor = T(s.horizon_factor) * d.r_plus;
   d.r_esc = T(s.escape_factor) * T(s.r_obs);
   d.r_in = (s.disk_r_in > 0) ? T(s.disk_r_in) : isco_geom(T(1), d.a, true);
@@ -641,7 +661,7 @@ inline void record_crossing(const Scene &s, const SceneDerived<T> &d, const RayC
                             PixelResult<T> &out) {
   const int k = out.n_cross;
   out.r_hit[k] = yc.r;
-  out.phi_hit[k] = yc.phi;
+  out.phi_hit[k] = phi_of_psi(yc.phi, yc.r, T(s.r_obs), d.a, d.r_plus, d.r_minus);
   out.g[k] = disk_g(yc.r, d.a, c.lam);
   const T q = d.r_in / yc.r;
   const T g2 = out.g[k] * out.g[k];
@@ -670,7 +690,7 @@ inline PixelResult<T> trace_pixel(const Scene &s, const SceneDerived<T> &d, T al
   auto in_disk = [&](T r) { return r >= d.r_in && r <= d.r_out; };
   auto finish_escape = [&](const Y<T> &yy) {
     out.theta_inf = s_acos(s_clamp(yy.u, T(-1), T(1)));
-    out.phi_inf = yy.phi;
+    out.phi_inf = phi_of_psi(yy.phi, yy.r, T(s.r_obs), d.a, d.r_plus, d.r_minus);
   };
 
   if (s.integrator == 0) {

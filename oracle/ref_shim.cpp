@@ -74,7 +74,14 @@ struct RefRhs {
     d.u = y.pu;
     d.pr = 0.5 * pR.dRdr;
     d.pu = -(y.u * pT.thetaPot) - (0.5 * sinTheta * pT.dThetadtheta);
-    d.phi = -((cR.lz / sin2) - a + (a * aFactor / deltaSafe));
+    // horizon-regular azimuth psi (kerr_oracle.hpp, img_rhs): the forward
+    // rate kerr.cpp:61 with a A / Delta replaced by a (A + p_r) / Delta, in
+    // its rationalized form K / (A - p_r) for ingoing rays
+    const double K = cR.q + (cR.lz - a) * (cR.lz - a);
+    const bool in = y.pr < 0.0;
+    const double num = in ? K : (aFactor + y.pr);
+    const double den = in ? (aFactor - y.pr) : deltaSafe;
+    d.phi = (a - (cR.lz / sin2)) - (a * (num / den));
     return d;
   }
   // First-integral projection with R from kerrPotentials and U = sin^2 Theta.

@@ -35,6 +35,7 @@ inline bool operator<(Counted a, Counted b) { ++g_counts.cmp; return a.v < b.v; 
 inline bool operator>(Counted a, Counted b) { ++g_counts.cmp; return a.v > b.v; }
 inline bool operator<=(Counted a, Counted b) { ++g_counts.cmp; return a.v <= b.v; }
 inline bool operator>=(Counted a, Counted b) { ++g_counts.cmp; return a.v >= b.v; }
+inline bool operator==(Counted a, Counted b) { ++g_counts.cmp; return a.v == b.v; }
 inline Counted s_sqrt(Counted x) { ++g_counts.sqrt; return Counted(std::sqrt(x.v)); }
 inline Counted s_sin(Counted x) { ++g_counts.trig; return Counted(std::sin(x.v)); }
 inline Counted s_cos(Counted x) { ++g_counts.trig; return Counted(std::cos(x.v)); }
