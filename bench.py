@@ -50,14 +50,31 @@ WORKLOADS = {
     "disk1_512": dict(width=512, height=512, integrator=1, max_crossings=3, frames=[(0.9, 45.0)]),
     "disk1_1024": dict(width=1024, height=1024, integrator=1, max_crossings=3, frames=[(0.9, 45.0)]),
     "disk_2048": dict(width=2048, height=2048, integrator=0, max_crossings=1, frames=[(0.9, 60.0)]),
+    "batch4096": dict(integrator=1, max_crossings=1, generator=batch_frames),
 }
 OUT_FIELDS_USED = ("cls", "steps", "n_cross", "r_hit", "phi_hit", "g", "intensity", "theta_inf", "phi_inf")
+
+
+def batch_frames(n: int = 4096, seed: int = 20261203):
+    """The uneven batch: per frame (own seed) a size from {64, 128, 256, 512}^2,
+    a ~ U[0, 0.998], inclination ~ U[5, 89] deg, r_obs ~ logU[100, 5000] M."""
+    frames = []
+    for i in range(n):
+        rng = np.random.default_rng([seed, i])
+        side = int(rng.choice([64, 128, 256, 512]))
+        frames.append(dict(width=side, height=side, spin=float(rng.uniform(0.0, 0.998)),
+                           theta_obs=math.radians(float(rng.uniform(5.0, 89.0))),
+                           r_obs=float(math.exp(rng.uniform(math.log(100.0), math.log(5000.0))))))
+    return frames
 
 
 def scenes_for(workload: str, precision: int):
     from blackhole_b200._abi import default_scene
 
     w = WORKLOADS[workload]
+    if "generator" in w:
+        return [default_scene(integrator=w["integrator"], max_crossings=w["max_crossings"], precision=precision, **f)
+                for f in w["generator"]()]
     out = []
     for spin, inc in w["frames"]:
         out.append(default_scene(width=w["width"], height=w["height"], spin=spin, theta_obs=math.radians(inc),
@@ -137,15 +154,18 @@ def time_precision(args, precision: str, dev, stream, dist):
     from blackhole_b200 import kerr
 
     scenes = scenes_for(args.workload, 1 if precision == "mixed" else 0)
-    outs = [kerr.alloc_image_outputs(s, device=dev, fields=list(OUT_FIELDS_USED)) for s in scenes]
+    # All frames of a step go out as one persistent launch, replayed from a
+    # CUDA graph; the per-step events bracket that one launch.
+    batch = kerr.TraceBatch(scenes, device=dev, fields=list(OUT_FIELDS_USED))
+    outs = batch.outs
+    tuned = batch.autotune(stream=stream) if args.autotune else batch.launch()
 
     def render(ev=None):
-        for i, s in enumerate(scenes):
-            if ev is not None:
-                ev[i][0].record(stream)
-            kerr.trace_image(s, outs[i], stream=stream)
-            if ev is not None:
-                ev[i][1].record(stream)
+        if ev is not None:
+            ev[0][0].record(stream)
+        batch.trace_graph(stream=stream)
+        if ev is not None:
+            ev[0][1].record(stream)
 
     sampler = ClockSampler(dev.index if "CUDA_VISIBLE_DEVICES" not in os.environ else 0)
     sampler.start()
@@ -157,8 +177,8 @@ def time_precision(args, precision: str, dev, stream, dist):
         dist.barrier()
     torch.cuda.synchronize(dev)
     sampler.lines.clear()
-    per_launch = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-                   for _ in scenes] for _ in range(args.steps)]
+    per_launch = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))]
+                  for _ in range(args.steps)]
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     t0.record(stream)
@@ -176,8 +196,9 @@ def time_precision(args, precision: str, dev, stream, dist):
         elapsed_ms = float(t.item())
     launch_ms = [a.elapsed_time(b) for step in per_launch for (a, b) in step]
     total_steps = sum(int(o["steps"].sum().item()) for o in outs)  # accepted steps of one render
+    frame_ms = batch.frame_times()  # completion of each frame within the last launch
     return dict(scenes=scenes, outs=outs, elapsed_ms=elapsed_ms, launch_ms=launch_ms, total_steps=total_steps,
-                clocks=clocks)
+                clocks=clocks, frame_ms=frame_ms, launch_cfg=tuned, batch=batch)
 
 
 def accuracy(ref_outs, test_outs) -> dict:
@@ -216,8 +237,6 @@ def run_ours(args, rank: int, world: int, dist):
     lib = _abi.load_library()
     wl = WORKLOADS[args.workload]
     integ = "dp45" if wl["integrator"] == 1 else "rk4"
-    n_frame = wl["width"] * wl["height"]
-    rays_per_step = n_frame * len(wl["frames"])
     stream = torch.cuda.Stream(device=dev)
 
     precisions = [args.precision]
@@ -225,8 +244,12 @@ def run_ours(args, rank: int, world: int, dist):
         precisions = ["fp64", args.precision]
     runs = {p: time_precision(args, p, dev, stream, dist) for p in precisions}
     head = runs[args.precision]
+    rays_per_step = sum(s.width * s.height for s in head["scenes"])
+    fm = head["frame_ms"]
+    extra = {"launch_config": head["launch_cfg"],
+             "frame_latency_ms": {"p50": float(np.percentile(fm, 50)), "p99": float(np.percentile(fm, 99)),
+                                  "max": float(fm.max()), "frames": int(len(fm))}}
     value = rays_per_step * args.steps * world / (head["elapsed_ms"] * 1e-3)
-    extra = {}
     if "fp64" in runs and args.precision != "fp64":
         f = runs["fp64"]
         extra["fp64_plain"] = {"value": rays_per_step * args.steps * world / (f["elapsed_ms"] * 1e-3),
@@ -237,11 +260,13 @@ def run_ours(args, rank: int, world: int, dist):
 
     # ---- end to end through the host-buffer C entry point (pinned host memory) ----
     e2e = None
-    if rank == 0:
+    out_bytes = sum(t.numel() * t.element_size() for o in head["outs"] for t in o.values())
+    if rank == 0 and out_bytes <= (4 << 30):  # pinned host copies of the outputs must stay modest
         scenes = head["scenes"]
         pinned = []
         for s in scenes:
             d = {}
+            n_frame = s.width * s.height
             for fld in OUT_FIELDS_USED:
                 shape = (s.max_crossings * n_frame,) if fld in _abi.PLANE_FIELDS else (n_frame,)
                 dt = torch.int32 if fld in _abi.INT_FIELDS else torch.float64
@@ -271,19 +296,19 @@ def run_ours(args, rank: int, world: int, dist):
     peak = C.c_double(0.0)
     _abi.check(lib.bh_measure_fma_peak(1 if fp64 else 0, 5, C.byref(peak)))
     mean_launch_s = statistics.mean(head["launch_ms"]) * 1e-3
-    flops_per_launch = FLOPS_PER_STEP[integ] * head["total_steps"] / len(head["scenes"])
+    flops_per_launch = FLOPS_PER_STEP[integ] * head["total_steps"]
     achieved = flops_per_launch / mean_launch_s / 1e12
-    kname = "k_trace_image_fp64" if fp64 else "k_trace_image_mixed"
+    kname = "k_trace_batch_fp64" if fp64 else "k_trace_batch_mixed"
     roofline = {"bound": "fp64" if fp64 else "fp32", "achieved": achieved, "peak": peak.value,
                 "unit": "TFLOP/s", "frac": achieved / peak.value if peak.value else None, "traffic": None,
                 "peak_source": "measured FMA-pipe probe (bh_measure_fma_peak), FMA = 2 FLOPs",
-                "flops_per_step": FLOPS_PER_STEP[integ], "steps_per_launch": head["total_steps"] / len(head["scenes"]),
+                "flops_per_step": FLOPS_PER_STEP[integ], "steps_per_launch": head["total_steps"],
                 "kernel": f"{kname}<{1 if integ == 'dp45' else 0}>",
                 "launch_ms_mean": statistics.mean(head["launch_ms"]),
                 "launch_ms_min": min(head["launch_ms"]), "launch_ms_max": max(head["launch_ms"])}
     return dict(value=value, ms_per_step=head["elapsed_ms"] / args.steps, e2e=e2e, roofline=roofline,
                 clocks=head["clocks"], total_steps=head["total_steps"], rays_per_step=rays_per_step,
-                launches=sum(len(r["scenes"]) * args.steps for r in runs.values()), extra=extra)
+                launches=len(runs) * args.steps, extra=extra)
 
 
 # ---------------------------------------------------------------------------
@@ -324,15 +349,24 @@ def main():
     ap.add_argument("--compare", action=argparse.BooleanOptionalAction, default=True,
                     help="also time the FP64 plain path and report the accuracy against it")
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU baseline sampling")
+    ap.add_argument("--autotune", action=argparse.BooleanOptionalAction, default=True,
+                    help="autotune the persistent-grid shape before timing")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", 1))
     rank = int(os.environ.get("RANK", 0))
     wl = WORKLOADS[args.workload]
-    config = {"workload": args.workload, "frames": len(wl["frames"]), "width": wl["width"], "height": wl["height"],
-              "integrator": "dp45" if wl["integrator"] == 1 else "rk4", "rtol": 1e-8, "atol": 1e-10,
-              "max_crossings": wl["max_crossings"], "r_obs": 1000.0, "image_plane_M": [-12, 12],
-              "parallelism": f"replicas{world}", "l2": "outputs written once per step (1.7 GB > L2); no inputs"}
+    if "generator" in wl:
+        config = {"workload": args.workload, "frames": 4096, "sizes": [64, 128, 256, 512], "spin": [0, 0.998],
+                  "theta_obs_deg": [5, 89], "r_obs": "logU[100, 5000]", "seed": "per frame",
+                  "integrator": "dp45" if wl["integrator"] == 1 else "rk4", "rtol": 1e-8, "atol": 1e-10,
+                  "max_crossings": wl["max_crossings"], "image_plane_M": [-12, 12]}
+    else:
+        config = {"workload": args.workload, "frames": len(wl["frames"]), "width": wl["width"], "height": wl["height"],
+                  "integrator": "dp45" if wl["integrator"] == 1 else "rk4", "rtol": 1e-8, "atol": 1e-10,
+                  "max_crossings": wl["max_crossings"], "r_obs": 1000.0, "image_plane_M": [-12, 12]}
+    config.update({"parallelism": f"replicas{world}", "launch": "one persistent launch per step (CUDA graph)",
+                   "l2": "no inputs; outputs written once per step, larger than L2"})
 
     if args.impl == "reference":
         if rank != 0:

@@ -102,6 +102,13 @@ class KerrRaytracerParams(C.Structure):
     ]
 
 
+class KerrLaunchConfig(C.Structure):
+    """struct BH_KerrLaunchConfig."""
+
+    _fields_ = [("block_threads", C.c_int32), ("ctas_per_sm", C.c_int32), ("refill_steps", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
 OUT_FIELDS = [name for name, _ in KerrImageOut._fields_]
 INT_FIELDS = ("cls", "steps", "n_cross")
 PLANE_FIELDS = ("r_hit", "phi_hit", "g")
@@ -184,6 +191,25 @@ def _declare(lib: C.CDLL) -> None:
     lib.bh_kerr_set_launch.argtypes = [i32, i32]
     lib.bh_kerr_trace_image_host_noalloc.restype = C.c_int
     lib.bh_kerr_trace_image_host_noalloc.argtypes = [C.POINTER(KerrScene), C.POINTER(KerrImageOut), vp]
+    lib.bh_kerr_batch_create.restype = vp
+    lib.bh_kerr_batch_create.argtypes = [C.POINTER(KerrScene), C.POINTER(KerrImageOut), i32]
+    for fn in ("bh_kerr_batch_trace", "bh_kerr_batch_trace_graph"):
+        getattr(lib, fn).restype = C.c_int
+        getattr(lib, fn).argtypes = [vp, vp]
+    lib.bh_kerr_batch_set_launch.restype = C.c_int
+    lib.bh_kerr_batch_set_launch.argtypes = [vp, C.POINTER(KerrLaunchConfig)]
+    lib.bh_kerr_batch_get_launch.restype = C.c_int
+    lib.bh_kerr_batch_get_launch.argtypes = [vp, C.POINTER(KerrLaunchConfig)]
+    lib.bh_kerr_batch_autotune.restype = C.c_int
+    lib.bh_kerr_batch_autotune.argtypes = [vp, i64, vp, C.POINTER(KerrLaunchConfig)]
+    lib.bh_kerr_batch_frame_times.restype = C.c_int
+    lib.bh_kerr_batch_frame_times.argtypes = [vp, vp]
+    lib.bh_kerr_batch_frames.restype = i32
+    lib.bh_kerr_batch_frames.argtypes = [vp]
+    lib.bh_kerr_batch_pixels.restype = i64
+    lib.bh_kerr_batch_pixels.argtypes = [vp]
+    lib.bh_kerr_batch_destroy.restype = None
+    lib.bh_kerr_batch_destroy.argtypes = [vp]
     lib.bh_measure_fma_peak.restype = C.c_int
     lib.bh_measure_fma_peak.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
 

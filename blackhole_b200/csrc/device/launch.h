@@ -43,7 +43,36 @@ typedef struct BhkImageOut {
 typedef struct BhkLaunch {
   int32_t grid;      // CTAs
   int32_t block;     // threads per CTA
+  int32_t refill;    // integration steps between two refills of finished lanes (>= 1)
+  int32_t pad;
 } BhkLaunch;
+
+// One frame of a batch as the device sees it.
+typedef struct BhkFrame {
+  BhkImageParams p;
+  BhkImageOut o;
+} BhkFrame;
+
+// A batch of frames traced by one persistent launch. All pointers are device
+// pointers owned by the host-side batch object.
+typedef struct BhkBatchDev {
+  const BhkFrame *frames;          // [n_frames]
+  const long long *prefix;         // [n_frames + 1] first pixel of each frame in the work order
+  unsigned int *done;              // [n_frames] finished pixels of the current trace
+  unsigned long long *end_ns;      // [n_frames] %globaltimer when the frame's last pixel finished
+  unsigned long long *start_ns;    // [1] earliest %globaltimer at which a CTA started
+  long long n_total;               // sum of the frames' pixels
+  int32_t n_frames;
+  int32_t pad;
+} BhkBatchDev;
+
+// Persistent batch tracers (all frames share integrator and precision).
+int bhk_trace_batch_fp64(const BhkBatchDev *b, int integrator, unsigned long long *work_counter, BhkLaunch L,
+                         void *stream);
+int bhk_trace_batch_mixed(const BhkBatchDev *b, int integrator, unsigned long long *work_counter, BhkLaunch L,
+                          void *stream);
+int bhk_trace_batch_fp64_occupancy(int integrator, int block, int *blocks_per_sm);
+int bhk_trace_batch_mixed_occupancy(int integrator, int block, int *blocks_per_sm);
 
 // FP64 image tracer. work_counter: one zeroed-on-stream 64-bit device word.
 int bhk_trace_image_fp64(const BhkImageParams *p, const BhkImageOut *o, unsigned long long *work_counter,
@@ -72,6 +101,8 @@ int bhk_kerr_trace_rays(int64_t n, BhkStateSoA init, BhkConstsSoA c, double mass
 // grid shape, allocating nothing; and setting the thread's last error.
 struct BH_KerrScene;
 int bhh_prepare_image_launch(const struct BH_KerrScene *scene, BhkImageParams *p, BhkLaunch *L);
+// Validates one scene and fills its kernel parameters (no device call).
+int bhh_make_params(const struct BH_KerrScene *scene, BhkImageParams *p);
 // Launches the image kernel of p->precision (work counter zeroed on stream).
 int bhh_launch_image(const BhkImageParams *p, const BhkImageOut *o, unsigned long long *counter, BhkLaunch L,
                      void *stream);

@@ -15,6 +15,7 @@
 
 #include <cstdio>
 
+#include "frame_source.cuh"
 #include "hermite.cuh"
 #include "image_fp64.cuh"
 #include "launch.h"
@@ -30,6 +31,7 @@ struct RayFp64 {
   double h;     // DP45: next trial step
   double inten;
   long long pix;
+  int f;  // frame of the current ray (batch launches)
   int steps;
   int attempts;
   int ncross;
@@ -170,11 +172,14 @@ __device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOu
   }
 }
 
-template <int INTEG>
-__global__ void __launch_bounds__(128) k_trace_image_fp64(const BhkImageParams p, const BhkImageOut o,
-                                                          unsigned long long *__restrict__ counter) {
+// The persistent loop shared by the single-frame and batch kernels. Every
+// `refill` integration steps, the lanes whose ray finished take new work
+// items with one warp-aggregated atomicAdd on the counter (ballot + popc).
+template <int INTEG, class Src>
+__device__ __forceinline__ void trace_loop(const Src &src, unsigned long long *__restrict__ counter, int refill) {
   const unsigned lane = threadIdx.x & 31u;
   const unsigned lanemask_lt = (1u << lane) - 1u;
+  const unsigned long long total = (unsigned long long)src.total();
   RayFp64 R;
   bool active = false;
   bool exhausted = false;
@@ -187,8 +192,11 @@ __global__ void __launch_bounds__(128) k_trace_image_fp64(const BhkImageParams p
       base = __shfl_sync(kFull, base, leader);
       if (!active && !exhausted) {
         const unsigned long long mine = base + (unsigned long long)__popc(need & lanemask_lt);
-        if (mine < (unsigned long long)p.n_pix) {
-          init_ray(p, (long long)mine, R);
+        if (mine < total) {
+          long long pix;
+          const int f = src.frame_of((long long)mine, pix);
+          init_ray(src.params(f), pix, R);
+          R.f = f;
           active = true;
         } else {
           exhausted = true;
@@ -196,14 +204,32 @@ __global__ void __launch_bounds__(128) k_trace_image_fp64(const BhkImageParams p
       }
     }
     if (!__any_sync(kFull, active)) break;
-    if (active) {
-      const int cls = iterate<INTEG>(p, o, R);
-      if (cls >= 0) {
-        finish(p, o, R, cls);
-        active = false;
+    for (int k = 0; k < refill; ++k) {
+      if (active) {
+        const BhkImageParams &P = src.params(R.f);
+        const int cls = iterate<INTEG>(P, src.out(R.f), R);
+        if (cls >= 0) {
+          finish(P, src.out(R.f), R, cls);
+          src.pixel_done(R.f);
+          active = false;
+        }
       }
     }
   }
+}
+
+template <int INTEG>
+__global__ void __launch_bounds__(128, 4) k_trace_image_fp64(const __grid_constant__ BhkImageParams p,
+                                                          const __grid_constant__ BhkImageOut o,
+                                                          unsigned long long *__restrict__ counter, int refill) {
+  trace_loop<INTEG>(bhsrc::SingleSrc{p, o}, counter, refill);
+}
+
+template <int INTEG>
+__global__ void __launch_bounds__(128, 4) k_trace_batch_fp64(const __grid_constant__ BhkBatchDev b,
+                                                          unsigned long long *__restrict__ counter, int refill) {
+  if (threadIdx.x == 0) atomicMin(b.start_ns, bhsrc::globaltimer_ns());
+  trace_loop<INTEG>(bhsrc::BatchSrc{b}, counter, refill);
 }
 
 }  // namespace bhk
@@ -224,9 +250,9 @@ extern "C" int bhk_trace_image_fp64(const BhkImageParams *p, const BhkImageOut *
   cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s);
   if (e != cudaSuccess) return set_err(e, "work-counter reset");
   if (p->integrator == 0)
-    bhk::k_trace_image_fp64<0><<<launch.grid, launch.block, 0, s>>>(*p, *o, counter);
+    bhk::k_trace_image_fp64<0><<<launch.grid, launch.block, 0, s>>>(*p, *o, counter, launch.refill);
   else
-    bhk::k_trace_image_fp64<1><<<launch.grid, launch.block, 0, s>>>(*p, *o, counter);
+    bhk::k_trace_image_fp64<1><<<launch.grid, launch.block, 0, s>>>(*p, *o, counter, launch.refill);
   e = cudaGetLastError();
   if (e != cudaSuccess) return set_err(e, "k_trace_image_fp64 launch");
   return 0;
@@ -237,6 +263,30 @@ extern "C" int bhk_trace_image_fp64_occupancy(int integrator, int block, int *bl
                       ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhk::k_trace_image_fp64<0>,
                                                                       block, 0)
                       : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhk::k_trace_image_fp64<1>,
+                                                                      block, 0);
+  if (e != cudaSuccess) return set_err(e, "occupancy query");
+  return 0;
+}
+
+extern "C" int bhk_trace_batch_fp64(const BhkBatchDev *b, int integrator, unsigned long long *counter, BhkLaunch L,
+                                    void *stream) {
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return set_err(e, "work-counter reset");
+  if (integrator == 0)
+    bhk::k_trace_batch_fp64<0><<<L.grid, L.block, 0, s>>>(*b, counter, L.refill);
+  else
+    bhk::k_trace_batch_fp64<1><<<L.grid, L.block, 0, s>>>(*b, counter, L.refill);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(e, "k_trace_batch_fp64 launch");
+  return 0;
+}
+
+extern "C" int bhk_trace_batch_fp64_occupancy(int integrator, int block, int *blocks_per_sm) {
+  cudaError_t e = (integrator == 0)
+                      ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhk::k_trace_batch_fp64<0>,
+                                                                      block, 0)
+                      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhk::k_trace_batch_fp64<1>,
                                                                       block, 0);
   if (e != cudaSuccess) return set_err(e, "occupancy query");
   return 0;

@@ -21,6 +21,7 @@
 
 #include <cstdio>
 
+#include "frame_source.cuh"
 #include "hermite.cuh"
 #include "image_mixed.cuh"
 #include "launch.h"
@@ -37,7 +38,9 @@ struct RayMx {
   float h;     // DP45 trial step / unused for RK4
   RayCd cd;    // FP64 constants: projection and g
   double inten;
+  float r_hor, r_esc, rtol, atol;  // frame constants used every iteration
   long long pix;
+  int f;  // frame of the current ray (batch launches)
   int steps;
   int attempts;
   int ncross;
@@ -84,6 +87,10 @@ __device__ __forceinline__ void init_ray(const BhkImageParams &p, long long pix,
   R.steps = 0;
   R.attempts = 0;
   R.ncross = 0;
+  R.r_hor = (float)p.r_hor;
+  R.r_esc = (float)p.r_esc;
+  R.rtol = (float)p.rtol;
+  R.atol = (float)p.atol;
   project(R.y, R.lo, R.cd);  // idempotent from here on (see iterate)
   const float hh = (float)p.step_coeff * fminf(R.y.r, (float)p.step_rcap);
   R.h = hh / fmaf(R.c.a2 * R.y.u, R.y.u, R.y.r * R.y.r);
@@ -187,8 +194,8 @@ __device__ __forceinline__ bool accept(const BhkImageParams &p, const BhkImageOu
 }
 
 template <int INTEG>
-__device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOut &o, RayMx &R, float r_hor,
-                                       float r_esc, float rtol, float atol) {
+__device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOut &o, RayMx &R) {
+  const float r_hor = R.r_hor, r_esc = R.r_esc;
   if (INTEG == 0) {
     if (R.steps >= p.max_steps) return 3;
     if (R.y.r <= r_hor) return 0;
@@ -204,7 +211,7 @@ __device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOu
     if (R.y.r <= r_hor) return 0;
     if (R.y.r >= r_esc) return 2;
     ++R.attempts;
-    const DPf d = dp45(R.y, R.h, R.c, R.k1, rtol, atol, true);
+    const DPf d = dp45(R.y, R.h, R.c, R.k1, R.rtol, R.atol, true);
     const bool acc = d.err <= 1.0f;
     const float h = R.h;
     const bool stop = accept(p, o, R, d.d, acc, h, R.k1, &d.k7);
@@ -216,13 +223,13 @@ __device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOu
   }
 }
 
-template <int INTEG>
-__global__ void __launch_bounds__(128) k_trace_image_mixed(const BhkImageParams p, const BhkImageOut o,
-                                                           unsigned long long *__restrict__ counter) {
+// The persistent loop shared by the single-frame and batch kernels (see
+// trace_image_fp64.cu).
+template <int INTEG, class Src>
+__device__ __forceinline__ void trace_loop(const Src &src, unsigned long long *__restrict__ counter, int refill) {
   const unsigned lane = threadIdx.x & 31u;
   const unsigned lanemask_lt = (1u << lane) - 1u;
-  const float r_hor = (float)p.r_hor, r_esc = (float)p.r_esc;
-  const float rtol = (float)p.rtol, atol = (float)p.atol;
+  const unsigned long long total = (unsigned long long)src.total();
   RayMx R;
   bool active = false;
   bool exhausted = false;
@@ -235,8 +242,11 @@ __global__ void __launch_bounds__(128) k_trace_image_mixed(const BhkImageParams 
       base = __shfl_sync(kFull, base, leader);
       if (!active && !exhausted) {
         const unsigned long long mine = base + (unsigned long long)__popc(need & lanemask_lt);
-        if (mine < (unsigned long long)p.n_pix) {
-          init_ray(p, (long long)mine, R);
+        if (mine < total) {
+          long long pix;
+          const int f = src.frame_of((long long)mine, pix);
+          init_ray(src.params(f), pix, R);
+          R.f = f;
           active = true;
         } else {
           exhausted = true;
@@ -244,14 +254,32 @@ __global__ void __launch_bounds__(128) k_trace_image_mixed(const BhkImageParams 
       }
     }
     if (!__any_sync(kFull, active)) break;
-    if (active) {
-      const int cls = iterate<INTEG>(p, o, R, r_hor, r_esc, rtol, atol);
-      if (cls >= 0) {
-        finish(p, o, R, cls);
-        active = false;
+    for (int k = 0; k < refill; ++k) {
+      if (active) {
+        const BhkImageParams &P = src.params(R.f);
+        const int cls = iterate<INTEG>(P, src.out(R.f), R);
+        if (cls >= 0) {
+          finish(P, src.out(R.f), R, cls);
+          src.pixel_done(R.f);
+          active = false;
+        }
       }
     }
   }
+}
+
+template <int INTEG>
+__global__ void __launch_bounds__(128) k_trace_image_mixed(const __grid_constant__ BhkImageParams p,
+                                                           const __grid_constant__ BhkImageOut o,
+                                                           unsigned long long *__restrict__ counter, int refill) {
+  trace_loop<INTEG>(bhsrc::SingleSrc{p, o}, counter, refill);
+}
+
+template <int INTEG>
+__global__ void __launch_bounds__(128) k_trace_batch_mixed(const __grid_constant__ BhkBatchDev b,
+                                                           unsigned long long *__restrict__ counter, int refill) {
+  if (threadIdx.x == 0) atomicMin(b.start_ns, bhsrc::globaltimer_ns());
+  trace_loop<INTEG>(bhsrc::BatchSrc{b}, counter, refill);
 }
 
 }  // namespace bhm
@@ -261,9 +289,9 @@ extern "C" int bhk_trace_image_mixed(const BhkImageParams *p, const BhkImageOut 
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s) != cudaSuccess) return -1;
   if (p->integrator == 0)
-    bhm::k_trace_image_mixed<0><<<launch.grid, launch.block, 0, s>>>(*p, *o, counter);
+    bhm::k_trace_image_mixed<0><<<launch.grid, launch.block, 0, s>>>(*p, *o, counter, launch.refill);
   else
-    bhm::k_trace_image_mixed<1><<<launch.grid, launch.block, 0, s>>>(*p, *o, counter);
+    bhm::k_trace_image_mixed<1><<<launch.grid, launch.block, 0, s>>>(*p, *o, counter, launch.refill);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
@@ -272,5 +300,24 @@ extern "C" int bhk_trace_image_mixed_occupancy(int integrator, int block, int *b
       (integrator == 0)
           ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhm::k_trace_image_mixed<0>, block, 0)
           : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhm::k_trace_image_mixed<1>, block, 0);
+  return e == cudaSuccess ? 0 : -1;
+}
+
+extern "C" int bhk_trace_batch_mixed(const BhkBatchDev *b, int integrator, unsigned long long *counter, BhkLaunch L,
+                                     void *stream) {
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s) != cudaSuccess) return -1;
+  if (integrator == 0)
+    bhm::k_trace_batch_mixed<0><<<L.grid, L.block, 0, s>>>(*b, counter, L.refill);
+  else
+    bhm::k_trace_batch_mixed<1><<<L.grid, L.block, 0, s>>>(*b, counter, L.refill);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+extern "C" int bhk_trace_batch_mixed_occupancy(int integrator, int block, int *blocks_per_sm) {
+  const cudaError_t e =
+      (integrator == 0)
+          ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhm::k_trace_batch_mixed<0>, block, 0)
+          : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhm::k_trace_batch_mixed<1>, block, 0);
   return e == cudaSuccess ? 0 : -1;
 }

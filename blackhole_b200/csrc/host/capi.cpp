@@ -172,13 +172,19 @@ static BhkImageParams make_params(const BH_KerrScene *s) {
   return p;
 }
 
+int bhh_make_params(const BH_KerrScene *scene, BhkImageParams *p) {
+  if (bh_kerr_scene_validate(scene) != 0) return -1;
+  *p = make_params(scene);
+  return 0;
+}
+
 // Validates the scene and fills the kernel parameters and the persistent
 // grid shape (SM count x resident CTAs per SM, capped by the pixel count).
 // Allocates nothing. Returns 0, or -1 with the error message set.
 int bhh_prepare_image_launch(const BH_KerrScene *scene, BhkImageParams *p, BhkLaunch *L) {
   if (bh_kerr_scene_validate(scene) != 0) return -1;
   *p = make_params(scene);
-  *L = BhkLaunch{0, 0};
+  *L = BhkLaunch{0, 0, 1, 0};
   if (p->n_pix == 0) return 0;
   int dev = 0, sms = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -195,7 +201,7 @@ int bhh_prepare_image_launch(const BH_KerrScene *scene, BhkImageParams *p, BhkLa
   if (per_sm < 1) return fail("kernel does not fit on an SM at %d threads per CTA", block);
   const int64_t full = int64_t(sms) * per_sm;
   const int64_t need = (p->n_pix + block - 1) / block;
-  *L = BhkLaunch{int32_t(std::max<int64_t>(1, std::min(full, need))), block};
+  *L = BhkLaunch{int32_t(std::max<int64_t>(1, std::min(full, need))), block, 1, 0};
   return 0;
 }
 

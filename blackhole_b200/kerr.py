@@ -135,6 +135,77 @@ def set_launch(block_threads: int = 0, ctas_per_sm: int = 0) -> None:
     check(_abi.load_library().bh_kerr_set_launch(block_threads, ctas_per_sm))
 
 
+class TraceBatch:
+    """Many frames of uneven size traced by one persistent launch
+    (BH_KerrBatch). All scenes share integrator and precision.
+
+    ``outs``: one dict of device tensors per frame (allocated when None).
+    """
+
+    def __init__(self, scenes, outs=None, device="cuda", fields=None):
+        self.scenes = list(scenes)
+        if not self.scenes:
+            raise ValueError("a batch needs at least one frame")
+        self.outs = outs if outs is not None else [alloc_image_outputs(s, device=device, fields=fields)
+                                                   for s in self.scenes]
+        n = len(self.scenes)
+        sarr = (KerrScene * n)(*self.scenes)
+        oarr = (KerrImageOut * n)(*[_out_struct(o) for o in self.outs])
+        lib = _abi.load_library()
+        h = lib.bh_kerr_batch_create(sarr, oarr, n)
+        if not h:
+            raise RuntimeError(lib.bh_last_error().decode())
+        self._h = h
+        self._lib = lib
+
+    def __len__(self):
+        return len(self.scenes)
+
+    @property
+    def pixels(self) -> int:
+        return int(self._lib.bh_kerr_batch_pixels(self._h))
+
+    def trace(self, stream=None):
+        check(self._lib.bh_kerr_batch_trace(self._h, _stream_ptr(stream)))
+        return self.outs
+
+    def trace_graph(self, stream=None):
+        """Trace through a captured CUDA graph (captured on first use)."""
+        check(self._lib.bh_kerr_batch_trace_graph(self._h, _stream_ptr(stream)))
+        return self.outs
+
+    def set_launch(self, block_threads=0, ctas_per_sm=0, refill_steps=1):
+        cfg = _abi.KerrLaunchConfig(block_threads, ctas_per_sm, refill_steps, 0)
+        check(self._lib.bh_kerr_batch_set_launch(self._h, C.byref(cfg)))
+
+    def launch(self) -> dict:
+        cfg = _abi.KerrLaunchConfig()
+        check(self._lib.bh_kerr_batch_get_launch(self._h, C.byref(cfg)))
+        return {"block_threads": cfg.block_threads, "ctas_per_sm": cfg.ctas_per_sm, "refill_steps": cfg.refill_steps}
+
+    def autotune(self, max_pixels=0, stream=None) -> dict:
+        cfg = _abi.KerrLaunchConfig()
+        check(self._lib.bh_kerr_batch_autotune(self._h, max_pixels, _stream_ptr(stream), C.byref(cfg)))
+        return {"block_threads": cfg.block_threads, "ctas_per_sm": cfg.ctas_per_sm, "refill_steps": cfg.refill_steps}
+
+    def frame_times(self) -> np.ndarray:
+        """Per-frame completion times (ms after the launch started) of the last trace."""
+        out = np.zeros(len(self.scenes), np.float32)
+        check(self._lib.bh_kerr_batch_frame_times(self._h, out.ctypes.data))
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.bh_kerr_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown
+            pass
+
+
 # --------------------------------------------------------------------------
 # src/physics API, batched
 # --------------------------------------------------------------------------

@@ -273,6 +273,66 @@ int bh_kerr_trace_image_host_noalloc(const BH_KerrScene *scene, const BH_KerrIma
 /** Launch configuration of the image tracer (0 = automatic). */
 int bh_kerr_set_launch(int32_t block_threads, int32_t ctas_per_sm);
 
+/* ---------------------------------------------------------------------------
+ * 3. Batches: many frames of uneven size in one persistent launch
+ * ------------------------------------------------------------------------- */
+
+/** Opaque batch of frames (device frame table, work counter, per-frame timers). */
+typedef struct BH_KerrBatch BH_KerrBatch;
+
+/** Persistent-grid shape of a batch (0 = automatic for block / ctas_per_sm). */
+typedef struct BH_KerrLaunchConfig {
+    int32_t block_threads;  /**< 32..128, multiple of 32 */
+    int32_t ctas_per_sm;    /**< resident CTAs per SM (<= occupancy limit) */
+    int32_t refill_steps;   /**< integration steps between refills of finished lanes (>= 1) */
+    int32_t reserved;
+} BH_KerrLaunchConfig;
+
+/**
+ * Create a batch of n_frames frames on the current device. scenes[i] and
+ * outs[i] (DEVICE output pointers, as for bh_kerr_trace_image) describe frame
+ * i; all frames must share integrator and precision, everything else (size,
+ * spin, inclination, observer radius, window, tolerances, disk) may differ.
+ * The frame table is copied to the device now; returns NULL on error.
+ */
+BH_KerrBatch *bh_kerr_batch_create(const BH_KerrScene *scenes, const BH_KerrImageOut *outs, int32_t n_frames);
+
+/** Trace every frame of the batch in one persistent launch (asynchronous). */
+int bh_kerr_batch_trace(BH_KerrBatch *batch, void *stream);
+
+/**
+ * Same as bh_kerr_batch_trace through a CUDA graph: the first call captures
+ * the launch (on stream, which must not be the legacy default stream), later
+ * calls replay it. Changing the launch configuration drops the graph.
+ */
+int bh_kerr_batch_trace_graph(BH_KerrBatch *batch, void *stream);
+
+/** Set / get the persistent-grid shape used by the next trace. */
+int bh_kerr_batch_set_launch(BH_KerrBatch *batch, const BH_KerrLaunchConfig *cfg);
+int bh_kerr_batch_get_launch(const BH_KerrBatch *batch, BH_KerrLaunchConfig *cfg);
+
+/**
+ * Autotune the grid shape: time the candidate configurations (block size,
+ * resident CTAs per SM, refill interval) on the batch's first frames, up to
+ * max_pixels pixels (0: 4 Mi), keep the fastest and return it in best.
+ * Synchronous; overwrites those frames' outputs.
+ */
+int bh_kerr_batch_autotune(BH_KerrBatch *batch, int64_t max_pixels, void *stream, BH_KerrLaunchConfig *best);
+
+/**
+ * Completion time of each frame in the last trace, in milliseconds after the
+ * launch's first CTA started (0 for frames without pixels). Synchronises with
+ * the device. frame_ms: host array of n_frames floats.
+ */
+int bh_kerr_batch_frame_times(BH_KerrBatch *batch, float *frame_ms);
+
+/** Number of frames and total pixels of the batch. */
+int32_t bh_kerr_batch_frames(const BH_KerrBatch *batch);
+int64_t bh_kerr_batch_pixels(const BH_KerrBatch *batch);
+
+/** Free the batch (NULL is allowed). */
+void bh_kerr_batch_destroy(BH_KerrBatch *batch);
+
 /**
  * Measured FMA-pipe peak of the current device in TFLOP/s (fp64 != 0: FP64,
  * else FP32): best of `repeats` launches of independent FMA chains covering
