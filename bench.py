@@ -50,7 +50,7 @@ WORKLOADS = {
     "disk1_512": dict(width=512, height=512, integrator=1, max_crossings=3, frames=[(0.9, 45.0)]),
     "disk1_1024": dict(width=1024, height=1024, integrator=1, max_crossings=3, frames=[(0.9, 45.0)]),
     "disk_2048": dict(width=2048, height=2048, integrator=0, max_crossings=1, frames=[(0.9, 60.0)]),
-    "batch4096": dict(integrator=1, max_crossings=1, generator=batch_frames),
+    "batch4096": dict(integrator=1, max_crossings=1, generator=lambda: batch_frames()),
 }
 OUT_FIELDS_USED = ("cls", "steps", "n_cross", "r_hit", "phi_hit", "g", "intensity", "theta_inf", "phi_inf")
 
