@@ -109,6 +109,12 @@ class KerrLaunchConfig(C.Structure):
                 ("reserved", C.c_int32)]
 
 
+class AdamConfig(C.Structure):
+    """struct BH_AdamConfig."""
+
+    _fields_ = [("lr", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float)]
+
+
 OUT_FIELDS = [name for name, _ in KerrImageOut._fields_]
 INT_FIELDS = ("cls", "steps", "n_cross")
 PLANE_FIELDS = ("r_hit", "phi_hit", "g")
@@ -212,6 +218,32 @@ def _declare(lib: C.CDLL) -> None:
     lib.bh_kerr_batch_destroy.argtypes = [vp]
     lib.bh_measure_fma_peak.restype = C.c_int
     lib.bh_measure_fma_peak.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
+    # include/bh_surrogate.h
+    lib.bh_surrogate_param_count.restype = i64
+    lib.bh_surrogate_param_count.argtypes = []
+    lib.bh_surrogate_create.restype = vp
+    lib.bh_surrogate_create.argtypes = [i64, C.c_uint64]
+    lib.bh_surrogate_destroy.restype = None
+    lib.bh_surrogate_destroy.argtypes = [vp]
+    for fn in ("bh_surrogate_get_params", "bh_surrogate_set_params"):
+        getattr(lib, fn).restype = C.c_int
+        getattr(lib, fn).argtypes = [vp, vp, i64]
+    lib.bh_surrogate_features.restype = C.c_int
+    lib.bh_surrogate_features.argtypes = [vp, i64, vp, vp]
+    lib.bh_surrogate_forward.restype = C.c_int
+    lib.bh_surrogate_forward.argtypes = [vp, vp, i64, vp, vp]
+    lib.bh_surrogate_gradients.restype = C.c_int
+    lib.bh_surrogate_gradients.argtypes = [vp, vp, vp, i64, vp, vp, vp]
+    lib.bh_surrogate_train_step.restype = C.c_int
+    lib.bh_surrogate_train_step.argtypes = [vp, vp, vp, i64, C.POINTER(AdamConfig), vp, vp]
+    lib.bh_surrogate_device_error.restype = C.c_int
+    lib.bh_surrogate_device_error.argtypes = [vp]
+    lib.bh_surrogate_make_targets.restype = C.c_int
+    lib.bh_surrogate_make_targets.argtypes = [C.POINTER(KerrImageOut), i64, C.c_int, vp, vp]
+    lib.bh_surrogate_grid_inputs.restype = C.c_int
+    lib.bh_surrogate_grid_inputs.argtypes = [C.POINTER(KerrScene), vp, vp]
+    lib.bh_bf16_gemm.restype = C.c_int
+    lib.bh_bf16_gemm.argtypes = [vp, vp, i64, C.c_int, C.c_int, vp, vp]
 
 
 def check(rc: int) -> None:

@@ -1,0 +1,425 @@
+// surrogate_api.cpp - C++23 host side of include/bh_surrogate.h.
+//
+// Owns the network's FP32 master parameters, Adam moments, BF16 weight
+// copies (W_l and W_l^T) and the training activations, and sequences the
+// GEMM and element-wise kernels of csrc/device/surrogate.cu for inference,
+// gradients and training steps. Nothing here computes on the host except
+// the seeded weight initialisation.
+#include <cuda_bf16.h>
+#include <cuda_runtime_api.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "../../../include/bh_surrogate.h"
+#include "../device/launch.h"
+#include "../device/surrogate_net.h"
+
+using bf16 = __nv_bfloat16;
+
+struct BH_Surrogate {
+  int device = -1;
+  int64_t max_batch = 0;
+  int64_t n_params = 0;
+  int64_t step = 0;
+  std::vector<void *> allocs;
+  float *w = nullptr, *m = nullptr, *v = nullptr, *grad = nullptr;
+  bf16 *wb[BHS_LAYERS] = {}, *wt[BHS_LAYERS] = {};
+  // training activations, batch-major [B][.] and transposed [.][B]
+  bf16 *F = nullptr, *FT = nullptr;
+  bf16 *h[4] = {}, *ht[4] = {};
+  float *y[4] = {};
+  float *out = nullptr;
+  bf16 *dout = nullptr, *dout_t = nullptr;
+  bf16 *dy[4] = {}, *dyt[4] = {};
+  float *part[BHS_LAYERS] = {};
+  float *loss = nullptr;
+  int *err = nullptr;
+  // inference chunk buffers (grow-only)
+  int64_t inf_rows = 0;
+  bf16 *iF = nullptr, *iA = nullptr, *iB = nullptr;
+};
+
+namespace {
+
+constexpr int kDwChunks = 8;  // 64-row K chunks per split of the batch reduction
+constexpr int64_t kInferChunk = 131072;
+
+int fail_msg(const char *fmt, ...) __attribute__((format(printf, 1, 2)));
+int fail_msg(const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  return bhh_fail(buf);
+}
+
+int cuda_check(cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return 0;
+  return fail_msg("%s: %s", what, cudaGetErrorString(e));
+}
+
+template <class T>
+int alloc(BH_Surrogate *s, T **p, size_t count, const char *what) {
+  void *q = nullptr;
+  if (int rc = cuda_check(cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T)), what)) return rc;
+  s->allocs.push_back(q);
+  *p = static_cast<T *>(q);
+  return 0;
+}
+
+int64_t dw_splits(int64_t batch) {
+  const int64_t chunks = (batch + 63) / 64;
+  return (chunks + kDwChunks - 1) / kDwChunks;
+}
+
+uint64_t splitmix(uint64_t &x) {
+  uint64_t z = (x += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// Uniform weights of variance 1/fan_in (fan_in = the used input width),
+// zero for the padded feature columns, smaller for the head, zero biases.
+std::vector<float> init_params(uint64_t seed) {
+  std::vector<float> p(static_cast<size_t>(bhs_param_count()), 0.0f);
+  uint64_t st = seed ^ 0x5DEECE66Dull;
+  for (int l = 0; l < BHS_LAYERS; ++l) {
+    const int K = bhs_layer_k(l), N = bhs_layer_n(l);
+    const int used = l == 0 ? BHS_FEATURES_USED : K;
+    const double scale = std::sqrt(3.0 / used) * (l == BHS_LAYERS - 1 ? 0.5 : 1.0);
+    float *W = p.data() + bhs_weight_offset(l);
+    for (int n = 0; n < N; ++n)
+      for (int k = 0; k < used; ++k) {
+        const double u = static_cast<double>(splitmix(st) >> 11) * (1.0 / 9007199254740992.0);
+        W[static_cast<size_t>(n) * K + k] = static_cast<float>((2.0 * u - 1.0) * scale);
+      }
+  }
+  return p;
+}
+
+int refresh(BH_Surrogate *s, cudaStream_t st) {
+  if (bhs_launch_refresh_bf16(s->w, s->wb, s->wt, st) != 0) return fail_msg("surrogate: weight refresh launch failed");
+  return 0;
+}
+
+int gemm(BH_Surrogate *s, const BhsGemm &g, cudaStream_t st, const char *what) {
+  if (bhs_launch_gemm(&g, s->err, st) != 0)
+    return fail_msg("surrogate: GEMM launch failed (%s: M=%lld N=%d K=%d)", what, static_cast<long long>(g.M), g.N,
+                    g.K);
+  return 0;
+}
+
+BhsGemm make_gemm(const void *A, int lda, const void *B, int ldb, int64_t M, int N, int K, int epi) {
+  BhsGemm g{};
+  g.A = A;
+  g.B = B;
+  g.M = M;
+  g.N = N;
+  g.K = K;
+  g.lda = lda;
+  g.ldb = ldb;
+  g.epilogue = epi;
+  return g;
+}
+
+// Forward (saving what backward needs), loss, backward, gradient collection.
+int forward_backward(BH_Surrogate *s, const float *inputs, const float *targets, int64_t B, float *loss4,
+                     cudaStream_t st) {
+  if (B <= 0 || B > s->max_batch || B % 128 != 0)
+    return fail_msg("surrogate: batch %lld must be a positive multiple of 128 up to %lld", static_cast<long long>(B),
+                    static_cast<long long>(s->max_batch));
+  if (int rc = cuda_check(cudaMemsetAsync(s->loss, 0, 4 * sizeof(float), st), "cudaMemsetAsync(loss)")) return rc;
+  if (bhs_launch_features(inputs, B, s->F, s->FT, B, st) != 0) return fail_msg("surrogate: feature launch failed");
+  for (int l = 0; l < 4; ++l) {
+    const bf16 *X = l == 0 ? s->F : s->h[l - 1];
+    const int K = bhs_layer_k(l);
+    BhsGemm g = make_gemm(X, K, s->wb[l], K, B, BHS_HIDDEN, K, BHS_EPI_HIDDEN);
+    g.bias = s->w + bhs_bias_offset(l);
+    g.out = s->h[l];
+    g.out_t = s->ht[l];
+    g.y_out = s->y[l];
+    g.ld_t = B;
+    if (int rc = gemm(s, g, st, "forward")) return rc;
+  }
+  {
+    BhsGemm g = make_gemm(s->h[3], BHS_HIDDEN, s->wb[4], BHS_HIDDEN, B, BHS_HEAD, BHS_HIDDEN, BHS_EPI_HEAD);
+    g.bias = s->w + bhs_bias_offset(4);
+    g.out = s->out;
+    if (int rc = gemm(s, g, st, "head")) return rc;
+  }
+  if (bhs_launch_loss(s->out, targets, B, s->dout, s->dout_t, s->loss, st) != 0)
+    return fail_msg("surrogate: loss launch failed");
+  {  // head: dW4^T = H4^T dout, dY4 = (dout W4) * SiLU'(Y4)
+    BhsGemm g = make_gemm(s->ht[3], static_cast<int>(B), s->dout_t, static_cast<int>(B), BHS_HIDDEN, BHS_HEAD,
+                          static_cast<int>(B), BHS_EPI_F32);
+    g.kchunks_per_split = kDwChunks;
+    g.out = s->part[4];
+    if (int rc = gemm(s, g, st, "dW4")) return rc;
+    BhsGemm d = make_gemm(s->dout, BHS_HEAD_PAD, s->wt[4], BHS_HEAD_PAD, B, BHS_HIDDEN, BHS_HEAD_PAD,
+                          BHS_EPI_BACKWARD);
+    d.Y = s->y[3];
+    d.out = s->dy[3];
+    d.out_t = s->dyt[3];
+    d.ld_t = B;
+    if (int rc = gemm(s, d, st, "dH4")) return rc;
+  }
+  for (int l = 3; l >= 0; --l) {
+    const int K = bhs_layer_k(l);
+    const bf16 *XT = l == 0 ? s->FT : s->ht[l - 1];
+    BhsGemm g = make_gemm(s->dyt[l], static_cast<int>(B), XT, static_cast<int>(B), BHS_HIDDEN, K,
+                          static_cast<int>(B), BHS_EPI_F32);
+    g.kchunks_per_split = kDwChunks;
+    g.out = s->part[l];
+    if (int rc = gemm(s, g, st, "dW")) return rc;
+    if (l == 0) break;
+    BhsGemm d = make_gemm(s->dy[l], BHS_HIDDEN, s->wt[l], BHS_HIDDEN, B, BHS_HIDDEN, BHS_HIDDEN, BHS_EPI_BACKWARD);
+    d.Y = s->y[l - 1];
+    d.out = s->dy[l - 1];
+    d.out_t = s->dyt[l - 1];
+    d.ld_t = B;
+    if (int rc = gemm(s, d, st, "dH")) return rc;
+  }
+  const bf16 *dyt[BHS_LAYERS] = {s->dyt[0], s->dyt[1], s->dyt[2], s->dyt[3], s->dout_t};
+  if (bhs_launch_bias_grads(dyt, B, s->grad, st) != 0) return fail_msg("surrogate: bias-gradient launch failed");
+  const float *parts[BHS_LAYERS] = {s->part[0], s->part[1], s->part[2], s->part[3], s->part[4]};
+  const int sp = static_cast<int>(dw_splits(B));
+  const int splits[BHS_LAYERS] = {sp, sp, sp, sp, sp};
+  if (bhs_launch_collect_dw(parts, splits, s->grad, st) != 0) return fail_msg("surrogate: dW collection failed");
+  if (loss4)
+    if (int rc = cuda_check(cudaMemcpyAsync(loss4, s->loss, 4 * sizeof(float), cudaMemcpyDeviceToDevice, st),
+                            "cudaMemcpyAsync(loss)"))
+      return rc;
+  return 0;
+}
+
+int grow_inference(BH_Surrogate *s, int64_t rows) {
+  if (rows <= s->inf_rows) return 0;
+  for (void *p : {static_cast<void *>(s->iF), static_cast<void *>(s->iA), static_cast<void *>(s->iB)}) {
+    if (!p) continue;
+    auto it = std::find(s->allocs.begin(), s->allocs.end(), p);
+    if (it != s->allocs.end()) s->allocs.erase(it);
+    cudaFree(p);
+  }
+  s->iF = s->iA = s->iB = nullptr;
+  s->inf_rows = 0;
+  if (int rc = alloc(s, &s->iF, static_cast<size_t>(rows) * BHS_FEATURES, "cudaMalloc(inference features)")) return rc;
+  if (int rc = alloc(s, &s->iA, static_cast<size_t>(rows) * BHS_HIDDEN, "cudaMalloc(inference activations)"))
+    return rc;
+  if (int rc = alloc(s, &s->iB, static_cast<size_t>(rows) * BHS_HIDDEN, "cudaMalloc(inference activations)"))
+    return rc;
+  s->inf_rows = rows;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int64_t bh_surrogate_param_count(void) { return bhs_param_count(); }
+
+void bh_surrogate_destroy(BH_Surrogate *s) {
+  if (!s) return;
+  int cur = -1;
+  cudaGetDevice(&cur);
+  if (s->device >= 0) cudaSetDevice(s->device);
+  for (void *p : s->allocs) cudaFree(p);
+  if (cur >= 0) cudaSetDevice(cur);
+  delete s;
+}
+
+BH_Surrogate *bh_surrogate_create(int64_t max_batch, uint64_t seed) {
+  if (max_batch < 128 || max_batch % 128 != 0) {
+    fail_msg("surrogate: max_batch must be a positive multiple of 128, got %lld", static_cast<long long>(max_batch));
+    return nullptr;
+  }
+  auto *s = new BH_Surrogate();
+  s->max_batch = max_batch;
+  s->n_params = bhs_param_count();
+  const size_t B = static_cast<size_t>(max_batch);
+  const size_t P = static_cast<size_t>(s->n_params);
+  auto bad = [&]() {
+    bh_surrogate_destroy(s);
+    return static_cast<BH_Surrogate *>(nullptr);
+  };
+  if (cuda_check(cudaGetDevice(&s->device), "cudaGetDevice")) return bad();
+  if (alloc(s, &s->w, P, "cudaMalloc(params)") || alloc(s, &s->m, P, "cudaMalloc(adam m)") ||
+      alloc(s, &s->v, P, "cudaMalloc(adam v)") || alloc(s, &s->grad, P, "cudaMalloc(grad)"))
+    return bad();
+  for (int l = 0; l < BHS_LAYERS; ++l) {
+    const size_t nk = static_cast<size_t>(bhs_layer_n(l)) * bhs_layer_k(l);
+    if (alloc(s, &s->wb[l], nk, "cudaMalloc(bf16 weights)")) return bad();
+    const size_t tsz = l == BHS_LAYERS - 1 ? static_cast<size_t>(BHS_HIDDEN) * BHS_HEAD_PAD : nk;
+    if (alloc(s, &s->wt[l], tsz, "cudaMalloc(bf16 weights^T)")) return bad();
+  }
+  if (alloc(s, &s->F, B * BHS_FEATURES, "cudaMalloc(features)") ||
+      alloc(s, &s->FT, B * BHS_FEATURES, "cudaMalloc(features^T)"))
+    return bad();
+  for (int i = 0; i < 4; ++i) {
+    if (alloc(s, &s->h[i], B * BHS_HIDDEN, "cudaMalloc(H)") || alloc(s, &s->ht[i], B * BHS_HIDDEN, "cudaMalloc(H^T)") ||
+        alloc(s, &s->y[i], B * BHS_HIDDEN, "cudaMalloc(Y)") || alloc(s, &s->dy[i], B * BHS_HIDDEN, "cudaMalloc(dY)") ||
+        alloc(s, &s->dyt[i], B * BHS_HIDDEN, "cudaMalloc(dY^T)"))
+      return bad();
+  }
+  if (alloc(s, &s->out, B * BHS_HEAD, "cudaMalloc(head)") ||
+      alloc(s, &s->dout, B * BHS_HEAD_PAD, "cudaMalloc(dout)") ||
+      alloc(s, &s->dout_t, B * BHS_HEAD, "cudaMalloc(dout^T)"))
+    return bad();
+  const size_t sp = static_cast<size_t>(dw_splits(max_batch));
+  for (int l = 0; l < BHS_LAYERS; ++l) {
+    const size_t per = l == BHS_LAYERS - 1 ? static_cast<size_t>(BHS_HIDDEN) * BHS_HEAD
+                                           : static_cast<size_t>(BHS_HIDDEN) * bhs_layer_k(l);
+    if (alloc(s, &s->part[l], sp * per, "cudaMalloc(dW partials)")) return bad();
+  }
+  if (alloc(s, &s->loss, 4, "cudaMalloc(loss)") || alloc(s, &s->err, 1, "cudaMalloc(error flag)")) return bad();
+  // Zero what is only partly written: padded dout columns, W4^T padding, moments, flags.
+  if (cuda_check(cudaMemset(s->dout, 0, B * BHS_HEAD_PAD * sizeof(bf16)), "cudaMemset") ||
+      cuda_check(cudaMemset(s->wt[BHS_LAYERS - 1], 0, static_cast<size_t>(BHS_HIDDEN) * BHS_HEAD_PAD * sizeof(bf16)),
+                 "cudaMemset") ||
+      cuda_check(cudaMemset(s->m, 0, P * sizeof(float)), "cudaMemset") ||
+      cuda_check(cudaMemset(s->v, 0, P * sizeof(float)), "cudaMemset") ||
+      cuda_check(cudaMemset(s->err, 0, sizeof(int)), "cudaMemset"))
+    return bad();
+  const std::vector<float> init = init_params(seed);
+  if (bh_surrogate_set_params(s, init.data(), s->n_params) != 0) return bad();
+  return s;
+}
+
+int bh_surrogate_get_params(const BH_Surrogate *s, float *host, int64_t n) {
+  if (!s || !host || n != s->n_params) return fail_msg("surrogate: get_params needs %lld values", s ? static_cast<long long>(s->n_params) : 0LL);
+  return cuda_check(cudaMemcpy(host, s->w, static_cast<size_t>(n) * sizeof(float), cudaMemcpyDeviceToHost),
+                    "cudaMemcpy(params)");
+}
+
+int bh_surrogate_set_params(BH_Surrogate *s, const float *host, int64_t n) {
+  if (!s || !host || n != s->n_params) return fail_msg("surrogate: set_params needs %lld values", s ? static_cast<long long>(s->n_params) : 0LL);
+  if (int rc = cuda_check(cudaMemcpy(s->w, host, static_cast<size_t>(n) * sizeof(float), cudaMemcpyHostToDevice),
+                          "cudaMemcpy(params)"))
+    return rc;
+  if (int rc = refresh(s, nullptr)) return rc;
+  s->step = 0;
+  if (int rc = cuda_check(cudaMemset(s->m, 0, static_cast<size_t>(n) * sizeof(float)), "cudaMemset")) return rc;
+  if (int rc = cuda_check(cudaMemset(s->v, 0, static_cast<size_t>(n) * sizeof(float)), "cudaMemset")) return rc;
+  return cuda_check(cudaDeviceSynchronize(), "set_params");
+}
+
+int bh_surrogate_features(const float *inputs, int64_t n, void *features, void *stream) {
+  if (n < 0 || (n > 0 && (!inputs || !features))) return fail_msg("surrogate: bad feature arguments");
+  if (bhs_launch_features(inputs, n, static_cast<bf16 *>(features), nullptr, 0, static_cast<cudaStream_t>(stream)))
+    return fail_msg("surrogate: feature launch failed");
+  return 0;
+}
+
+int bh_surrogate_forward(BH_Surrogate *s, const float *inputs, int64_t n, float *head, void *stream) {
+  if (!s || n < 0 || (n > 0 && (!inputs || !head))) return fail_msg("surrogate: bad forward arguments");
+  if (n == 0) return 0;
+  const int64_t chunk = std::min<int64_t>(n, kInferChunk);
+  if (int rc = grow_inference(s, chunk)) return rc;
+  auto st = static_cast<cudaStream_t>(stream);
+  for (int64_t r0 = 0; r0 < n; r0 += chunk) {
+    const int64_t rows = std::min(chunk, n - r0);
+    if (bhs_launch_features(inputs + 4 * r0, rows, s->iF, nullptr, 0, st))
+      return fail_msg("surrogate: feature launch failed");
+    const bf16 *X = s->iF;
+    bf16 *bufs[2] = {s->iA, s->iB};
+    for (int l = 0; l < 4; ++l) {
+      const int K = bhs_layer_k(l);
+      BhsGemm g = make_gemm(X, K, s->wb[l], K, rows, BHS_HIDDEN, K, BHS_EPI_HIDDEN);
+      g.bias = s->w + bhs_bias_offset(l);
+      g.out = bufs[l & 1];
+      if (int rc = gemm(s, g, st, "inference")) return rc;
+      X = bufs[l & 1];
+    }
+    BhsGemm g = make_gemm(X, BHS_HIDDEN, s->wb[4], BHS_HIDDEN, rows, BHS_HEAD, BHS_HIDDEN, BHS_EPI_HEAD);
+    g.bias = s->w + bhs_bias_offset(4);
+    g.out = head + BHS_HEAD * r0;
+    if (int rc = gemm(s, g, st, "inference head")) return rc;
+  }
+  return 0;
+}
+
+int bh_surrogate_gradients(BH_Surrogate *s, const float *inputs, const float *targets, int64_t batch, float *grad,
+                           float *loss4, void *stream) {
+  if (!s || !inputs || !targets || !grad) return fail_msg("surrogate: bad gradient arguments");
+  auto st = static_cast<cudaStream_t>(stream);
+  if (int rc = forward_backward(s, inputs, targets, batch, loss4, st)) return rc;
+  return cuda_check(cudaMemcpyAsync(grad, s->grad, static_cast<size_t>(s->n_params) * sizeof(float),
+                                    cudaMemcpyDeviceToDevice, st),
+                    "cudaMemcpyAsync(grad)");
+}
+
+int bh_surrogate_train_step(BH_Surrogate *s, const float *inputs, const float *targets, int64_t batch,
+                            const BH_AdamConfig *adam, float *loss4, void *stream) {
+  if (!s || !inputs || !targets || !adam) return fail_msg("surrogate: bad train-step arguments");
+  if (!(adam->lr > 0.0f) || !(adam->beta1 >= 0.0f && adam->beta1 < 1.0f) || !(adam->beta2 >= 0.0f && adam->beta2 < 1.0f) ||
+      !(adam->eps > 0.0f))
+    return fail_msg("surrogate: Adam needs lr > 0, betas in [0, 1), eps > 0");
+  auto st = static_cast<cudaStream_t>(stream);
+  if (int rc = forward_backward(s, inputs, targets, batch, loss4, st)) return rc;
+  s->step += 1;
+  const double t = static_cast<double>(s->step);
+  const float lr_t = static_cast<float>(adam->lr * std::sqrt(1.0 - std::pow(adam->beta2, t)) /
+                                        (1.0 - std::pow(adam->beta1, t)));
+  if (bhs_launch_adam(s->w, s->grad, s->m, s->v, s->n_params, lr_t, adam->beta1, adam->beta2, adam->eps, s->wb, s->wt,
+                      st) != 0)
+    return fail_msg("surrogate: Adam launch failed");
+  return 0;
+}
+
+int bh_surrogate_device_error(BH_Surrogate *s) {
+  if (!s) return fail_msg("surrogate: NULL handle");
+  if (int rc = cuda_check(cudaDeviceSynchronize(), "cudaDeviceSynchronize")) return rc;
+  int code = 0;
+  if (int rc = cuda_check(cudaMemcpy(&code, s->err, sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy(error flag)"))
+    return rc;
+  if (code) cudaMemset(s->err, 0, sizeof(int));
+  return code;
+}
+
+int bh_surrogate_make_targets(const BH_KerrImageOut *o, int64_t n, int max_crossings, float *targets, void *stream) {
+  if (!o || !targets || n < 0 || max_crossings < 1 || max_crossings > BH_MAX_CROSSINGS)
+    return fail_msg("surrogate: bad make_targets arguments");
+  if (!o->cls || !o->n_cross || !o->r_hit || !o->phi_hit || !o->g || !o->theta_inf || !o->phi_inf)
+    return fail_msg("surrogate: make_targets needs cls, n_cross, r_hit, phi_hit, g, theta_inf and phi_inf");
+  if (bhs_launch_make_targets(static_cast<const int *>(o->cls), static_cast<const int *>(o->n_cross),
+                              static_cast<const double *>(o->r_hit), static_cast<const double *>(o->phi_hit),
+                              static_cast<const double *>(o->g), static_cast<const double *>(o->theta_inf),
+                              static_cast<const double *>(o->phi_inf), n, max_crossings, targets,
+                              static_cast<cudaStream_t>(stream)))
+    return fail_msg("surrogate: target launch failed");
+  return 0;
+}
+
+int bh_surrogate_grid_inputs(const BH_KerrScene *sc, float *inputs, void *stream) {
+  if (!sc || !inputs) return fail_msg("surrogate: bad grid_inputs arguments");
+  if (bh_kerr_scene_validate(sc) != 0) return -1;
+  const int64_t n = static_cast<int64_t>(sc->width) * sc->height;
+  const double da = (sc->alpha_max - sc->alpha_min) / sc->width;
+  const double db = (sc->beta_max - sc->beta_min) / sc->height;
+  if (bhs_launch_grid_inputs(sc->spin, std::cos(sc->theta_obs), sc->alpha_min, da, sc->beta_min, db, sc->width, n,
+                             inputs, static_cast<cudaStream_t>(stream)))
+    return fail_msg("surrogate: grid-input launch failed");
+  return 0;
+}
+
+int bh_bf16_gemm(const void *A, const void *B, int64_t M, int N, int K, float *C, void *stream) {
+  if (!A || !B || !C || M < 0 || K <= 0 || K % 8 != 0) return fail_msg("bf16 gemm: bad arguments");
+  if (!(N == 16 || N == 192 || (N > 0 && N % 256 == 0))) return fail_msg("bf16 gemm: N must be 16, 192 or k*256");
+  static int *err = nullptr;
+  if (!err) {
+    if (int rc = cuda_check(cudaMalloc(&err, sizeof(int)), "cudaMalloc(error flag)")) return rc;
+    cudaMemset(err, 0, sizeof(int));
+  }
+  BhsGemm g = make_gemm(A, K, B, K, M, N, K, BHS_EPI_F32);
+  g.out = C;
+  if (bhs_launch_gemm(&g, err, static_cast<cudaStream_t>(stream)) != 0) return fail_msg("bf16 gemm: launch failed");
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,96 @@
+/*
+ * bh_surrogate.h -- learned transfer function for Kerr image-plane rays.
+ *
+ * No counterpart in the reference: the reference's renderer always
+ * integrates every pixel (src/cuda/device_physics.cuh:912-1017,
+ * src/physics/raytracer.h:324-378). This interface adds a small MLP that maps
+ * (alpha, beta, spin, cos theta_obs) to the ray's termination class (captured,
+ * disk, escaped), the radius and azimuth of its first two disk crossings, the
+ * redshift g of the first, and its escape direction. The network is trained
+ * on rays the integrator itself traces (bh_kerr_trace_image /
+ * bh_kerr_batch_*) by BF16 tensor-core kernels (tcgen05, FP32 accumulation):
+ * forward, backward and Adam all run on the GPU.
+ *
+ * Conventions follow bh_kerr.h: 0 = success, -1 = error with a message in
+ * bh_last_error(); device pointers unless a name says host; a NULL stream is
+ * the legacy default stream. Inputs are FP32 [n][4] rows (alpha, beta, spin,
+ * cos theta_obs). Head outputs are FP32 [n][16] rows:
+ *   0..2  class logits (captured, disk, escaped)
+ *   3     ln r1 - 2     4, 5  cos phi1, sin phi1
+ *   6     ln r2 - 2     7, 8  cos phi2, sin phi2
+ *   9     g1 - 1        10    cos theta_inf     11, 12  cos phi_inf, sin phi_inf
+ *   13..15 unused
+ * Training targets are FP32 [n][16] rows (bh_surrogate_make_targets):
+ *   0 opaque-disk class (0, 1, 2; -1 = not used), 1 disk crossings (0..2),
+ *   2..11 the regression targets of head outputs 3..12, 12..15 zero.
+ */
+#ifndef BH_SURROGATE_H
+#define BH_SURROGATE_H
+
+#include <stdint.h>
+
+#include "bh_kerr.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct BH_Surrogate BH_Surrogate;
+
+typedef struct BH_AdamConfig {
+    float lr;
+    float beta1;
+    float beta2;
+    float eps;
+} BH_AdamConfig;
+
+/* Number of FP32 parameters: per layer l = 0..4, W_l [N_l][K_l] then b_l [N_l];
+ * K = 192, 256, 256, 256, 256 and N = 256, 256, 256, 256, 16. */
+int64_t bh_surrogate_param_count(void);
+
+/* A network with seeded random weights on the current device, with training
+ * buffers for batches of up to max_batch rows (a multiple of 128). */
+BH_Surrogate* bh_surrogate_create(int64_t max_batch, uint64_t seed);
+void bh_surrogate_destroy(BH_Surrogate* s); /* NULL-safe */
+
+int bh_surrogate_get_params(const BH_Surrogate* s, float* host_params, int64_t n);
+int bh_surrogate_set_params(BH_Surrogate* s, const float* host_params, int64_t n);
+
+/* Input features (BF16 [n][192]) of n rows; diagnostic. */
+int bh_surrogate_features(const float* inputs, int64_t n, void* features_bf16, void* stream);
+
+/* Head outputs [n][16] for n rows (inference, any n). */
+int bh_surrogate_forward(BH_Surrogate* s, const float* inputs, int64_t n, float* head, void* stream);
+
+/* Loss gradient w.r.t. every parameter (FP32, bh_surrogate_param_count()
+ * values) for one batch; loss4 (4 floats, may be NULL) receives the sums of
+ * cross entropy, squared regression error, correctly classified rows and
+ * classified rows. Parameters are not changed. */
+int bh_surrogate_gradients(BH_Surrogate* s, const float* inputs, const float* targets, int64_t batch,
+                           float* grad, float* loss4, void* stream);
+
+/* One Adam step on one batch (forward, backward, update). */
+int bh_surrogate_train_step(BH_Surrogate* s, const float* inputs, const float* targets, int64_t batch,
+                            const BH_AdamConfig* adam, float* loss4, void* stream);
+
+/* Synchronise the device and return the first kernel error code recorded by
+ * a bounded wait since the last call (0 = none). */
+int bh_surrogate_device_error(BH_Surrogate* s);
+
+/* Training targets from integrator outputs (device planes as written by
+ * bh_kerr_trace_image with the given max_crossings). */
+int bh_surrogate_make_targets(const BH_KerrImageOut* outs, int64_t n, int max_crossings, float* targets,
+                              void* stream);
+
+/* Inputs [width * height][4] of a scene's pixel centres. */
+int bh_surrogate_grid_inputs(const BH_KerrScene* scene, float* inputs, void* stream);
+
+/* C = A * B^T in FP32 for BF16 A [M][K], B [N][K] (K a multiple of 8;
+ * N = 16, 192 or a multiple of 256): the tensor-core GEMM the network uses. */
+int bh_bf16_gemm(const void* A, const void* B, int64_t M, int N, int K, float* C, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BH_SURROGATE_H */
