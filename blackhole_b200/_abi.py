@@ -115,6 +115,19 @@ class AdamConfig(C.Structure):
     _fields_ = [("lr", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float)]
 
 
+class SurrogatePolicy(C.Structure):
+    """struct BH_SurrogatePolicy."""
+
+    _fields_ = [("min_confidence", C.c_float), ("verify", C.c_int32), ("critical_band", C.c_double)]
+
+
+class SurrogateStats(C.Structure):
+    """struct BH_SurrogateStats."""
+
+    _fields_ = [(n, C.c_int64) for n in ("pixels", "accepted", "low_confidence", "critical_band", "solve_failed",
+                                         "disagreement")]
+
+
 OUT_FIELDS = [name for name, _ in KerrImageOut._fields_]
 INT_FIELDS = ("cls", "steps", "n_cross")
 PLANE_FIELDS = ("r_hit", "phi_hit", "g")
@@ -242,6 +255,13 @@ def _declare(lib: C.CDLL) -> None:
     lib.bh_surrogate_make_targets.argtypes = [C.POINTER(KerrImageOut), i64, C.c_int, vp, vp]
     lib.bh_surrogate_grid_inputs.restype = C.c_int
     lib.bh_surrogate_grid_inputs.argtypes = [C.POINTER(KerrScene), vp, vp]
+    lib.bh_surrogate_policy_defaults.restype = None
+    lib.bh_surrogate_policy_defaults.argtypes = [C.POINTER(SurrogatePolicy)]
+    lib.bh_surrogate_trace_image.restype = C.c_int
+    lib.bh_surrogate_trace_image.argtypes = [vp, C.POINTER(KerrScene), C.POINTER(KerrImageOut),
+                                             C.POINTER(SurrogatePolicy), vp]
+    lib.bh_surrogate_last_stats.restype = C.c_int
+    lib.bh_surrogate_last_stats.argtypes = [vp, C.POINTER(SurrogateStats)]
     lib.bh_bf16_gemm.restype = C.c_int
     lib.bh_bf16_gemm.argtypes = [vp, vp, i64, C.c_int, C.c_int, vp, vp]
 

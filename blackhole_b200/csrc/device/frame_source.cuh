@@ -31,6 +31,23 @@ struct SingleSrc {
   __device__ __forceinline__ void pixel_done(int) const {}
 };
 
+// The pixels of one frame named by a device list whose length a previous
+// kernel wrote (the surrogate renderer's integrator fallback).
+struct ListSrc {
+  const BhkImageParams &p;
+  const BhkImageOut &o;
+  const int *list;
+  const unsigned int *count;
+  __device__ __forceinline__ long long total() const { return (long long)*count; }
+  __device__ __forceinline__ int frame_of(long long w, long long &pix) const {
+    pix = list[w];
+    return 0;
+  }
+  __device__ __forceinline__ const BhkImageParams &params(int) const { return p; }
+  __device__ __forceinline__ const BhkImageOut &out(int) const { return o; }
+  __device__ __forceinline__ void pixel_done(int) const {}
+};
+
 struct BatchSrc {
   const BhkBatchDev &b;
   __device__ __forceinline__ long long total() const { return b.n_total; }

@@ -84,6 +84,18 @@ int bhk_trace_image_fp64_occupancy(int integrator, int block, int *blocks_per_sm
 int bhk_trace_image_mixed(const BhkImageParams *p, const BhkImageOut *o, unsigned long long *work_counter,
                           BhkLaunch launch, void *stream);
 int bhk_trace_image_mixed_occupancy(int integrator, int block, int *blocks_per_sm);
+// Mixed-precision tracer over the pixels named by a device list of *count
+// entries (count written by an earlier kernel on the same stream).
+int bhk_trace_list_mixed(const BhkImageParams *p, const BhkImageOut *o, const int *list, const unsigned int *count,
+                         unsigned long long *work_counter, BhkLaunch L, void *stream);
+
+// Surrogate renderer (surrogate_render.cu): per-pixel acceptance of the
+// network's head outputs [n_pix][16], exact refinement of accepted disk hits,
+// and the list of pixels left to the integrator. stats[5] += pixels accepted,
+// low confidence, critical band, solve failed, disagreement.
+int bhk_surrogate_refine(const BhkImageParams *p, const BhkImageOut *o, const float *head, float min_conf,
+                         double band, int verify, int *list, unsigned int *count, unsigned int *stats,
+                         void *stream);
 
 // Reference stepper kernels (src/physics/kerr.cpp semantics), FP64.
 typedef struct BhkStateSoA { double *r, *theta, *phi, *t, *sr, *sth; } BhkStateSoA;

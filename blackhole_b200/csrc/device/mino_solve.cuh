@@ -1,0 +1,365 @@
+// mino_solve.cuh - exact equatorial crossings of a Kerr image-plane ray
+// without stepping (FP64, host and device).
+//
+// The image tracer integrates r'' = R'(r)/2, u'' = U'(u)/2 in Mino time tau
+// with p_r^2 = R, p_u^2 = U (u = cos theta). Both motions separate, so the
+// Mino times of the equatorial crossings and the radius reached at a given
+// Mino time follow from one-dimensional integrals:
+//
+// * theta: U = (z+ - u^2)(a^2 u^2 + w) with z+ w = q_Th - lambda^2. With
+//   u = sqrt(z+) sin(chi), d tau = d chi / sqrt(w + a^2 z+ sin^2 chi): the
+//   crossings (chi = n pi) are at tau_1 + 2(n-1)K, from Legendre's integral
+//   of the first kind, evaluated with Carlson's R_F (B. C. Carlson, "Numerical
+//   computation of real or complex elliptic integrals", Numer. Algorithms 10
+//   (1995) 13-26, duplication algorithm).
+// * r: x = 1/r, P(x) = x^4 R(1/x) = 1 + p2 x^2 + p1 x^3 + p0 x^4. A ray with a
+//   turning point x_tp (smallest positive root of P below 1/r+) is described
+//   by sigma with x = x_tp - sigma^2 (sigma < 0 inbound, > 0 outbound), so
+//   d tau / d sigma = 2 / sqrt(P(x) / (x_tp - x)) is smooth and positive
+//   through the turning point; a ray without one uses x itself, d tau / dx =
+//   1 / sqrt(P(x)). tau(sigma) is then a smooth increasing function evaluated
+//   by composite 16-point Gauss-Legendre quadrature and inverted by
+//   bracketed Newton iteration.
+//
+// Accuracy degrades where P has a near-double root (rays next to the
+// critical curve): classify() reports a first-order image-plane distance to
+// the critical curve so callers can send those rays to the integrator.
+#pragma once
+
+#include <cmath>
+
+#ifdef __CUDACC__
+#define BHM_HD __host__ __device__ __forceinline__
+#else
+#define BHM_HD inline
+#endif
+
+namespace bhmino {
+
+// Gauss-Legendre, 16 points on [-1, 1]: the 8 positive nodes and weights.
+struct GlNode {
+  double x, w;
+};
+#ifdef __CUDACC__
+__constant__
+#endif
+    static const GlNode kGl16[8] = {
+        {9.50125098376374405e-02, 1.89450610455068641e-01}, {2.81603550779258915e-01, 1.82603415044923639e-01},
+        {4.58016777657227370e-01, 1.69156519395002647e-01}, {6.17876244402643771e-01, 1.49595988816576708e-01},
+        {7.55404408355002999e-01, 1.24628971255534071e-01}, {8.65631202387831755e-01, 9.51585116824926053e-02},
+        {9.44575023073232600e-01, 6.22535239386474565e-02}, {9.89400934991649939e-01, 2.71524594117541762e-02}};
+
+// Carlson's symmetric integral R_F(x, y, z) = 1/2 int_0^inf dt / sqrt((t+x)(t+y)(t+z)),
+// x, y, z >= 0 with at most one zero.
+BHM_HD double carlson_rf(double x, double y, double z) {
+  for (int it = 0; it < 60; ++it) {
+    const double sx = sqrt(x), sy = sqrt(y), sz = sqrt(z);
+    const double lam = sx * sy + sy * sz + sz * sx;
+    x = 0.25 * (x + lam);
+    y = 0.25 * (y + lam);
+    z = 0.25 * (z + lam);
+    const double A = (x + y + z) * (1.0 / 3.0);
+    const double dx = 1.0 - x / A, dy = 1.0 - y / A;
+    const double dz = -(dx + dy);
+    if (fmax(fabs(dx), fmax(fabs(dy), fabs(dz))) < 1e-3) {
+      const double e2 = dx * dy - dz * dz, e3 = dx * dy * dz;
+      return (1.0 - 0.1 * e2 + e3 * (1.0 / 14.0) + e2 * e2 * (1.0 / 24.0) - e2 * e3 * (3.0 / 44.0)) / sqrt(A);
+    }
+  }
+  return NAN;
+}
+
+struct ThetaMotion {
+  bool crosses;   // U(0) > 0: the ray reaches the equator
+  double tau1;    // Mino time of the first crossing
+  double period;  // 2K: Mino time between crossings
+};
+
+// u0 = cos theta_obs, pu0 = du/dtau at the observer.
+BHM_HD ThetaMotion theta_motion(double a2, double qTh, double lam, double u0, double pu0) {
+  ThetaMotion t{false, INFINITY, INFINITY};
+  const double c0 = qTh - lam * lam;  // U(0)
+  if (!(c0 > 0.0)) return t;
+  const double b2 = a2 - qTh;
+  const double sq = sqrt(b2 * b2 + 4.0 * a2 * c0);
+  const double zp = (b2 > 0.0) ? (b2 + sq) / (2.0 * a2) : 2.0 * c0 / (sq - b2);
+  const double w = c0 / zp;
+  const double m = a2 * zp;
+  double s = fabs(u0) / sqrt(zp);  // sin chi_obs
+  s = fmin(s, 1.0);
+  const double phi_obs = s * carlson_rf(w * (1.0 - s * s), w + m * s * s, w);
+  const double K = carlson_rf(0.0, w + m, w);
+  const bool toward = (pu0 * u0) < 0.0;
+  t.crosses = true;
+  t.tau1 = toward ? phi_obs : 2.0 * K - phi_obs;
+  t.period = 2.0 * K;
+  return t;
+}
+
+struct Radial {
+  int kind;            // 1: turning point (escapes), 0: none (falls in), -1: not handled
+  double p2, p1, p0;   // R = r^4 + p2 r^2 + p1 r + p0
+  double x_tp;         // kind 1: 1 / r_tp
+  double q3, q2, q1, q0;  // kind 1: P(x) / (x_tp - x)
+  double v_obs;        // variable at the observer (kind 1: -sqrt(x_tp - x_obs); kind 0: x_obs)
+  double v_end;        // variable where the tracer stops (escape or horizon)
+  double r_min;        // largest local minimum of R (0 if none above r+)
+  double R_min;        // R there
+};
+
+BHM_HD double poly_R(const Radial& q, double r) {
+  const double r2 = r * r;
+  return (r2 + q.p2) * r2 + q.p1 * r + q.p0;
+}
+
+// Largest real root of R'(r) / 4 = r^3 + (p2/2) r + p1/4.
+BHM_HD double largest_dR_root(double p2, double p1) {
+  const double p = 0.5 * p2, qq = 0.25 * p1;
+  const double disc = qq * qq * 0.25 + p * p * p * (1.0 / 27.0);
+  if (disc < 0.0) {  // three real roots (p < 0)
+    const double rr = sqrt(-p * (1.0 / 3.0));
+    double c = (-0.5 * qq) / (rr * rr * rr);
+    c = fmax(-1.0, fmin(1.0, c));
+    return 2.0 * rr * cos(acos(c) * (1.0 / 3.0));
+  }
+  const double sd = sqrt(disc);
+  return cbrt(-0.5 * qq + sd) + cbrt(-0.5 * qq - sd);
+}
+
+BHM_HD double integrand(const Radial& q, double v) {
+  if (q.kind == 1) {
+    const double x = q.x_tp - v * v;
+    const double pt = ((q.q3 * x + q.q2) * x + q.q1) * x + q.q0;
+    return 2.0 / sqrt(pt);
+  }
+  const double x = v;
+  const double x2 = x * x;
+  const double P = 1.0 + x2 * (q.p2 + x * (q.p1 + x * q.p0));
+  return 1.0 / sqrt(P);
+}
+
+BHM_HD double radius_of(const Radial& q, double v) { return q.kind == 1 ? 1.0 / (q.x_tp - v * v) : 1.0 / v; }
+
+// int_{v0}^{v1} integrand, composite Gauss-Legendre-16 with panels <= hmax.
+BHM_HD double integrate(const Radial& q, double v0, double v1, double hmax) {
+  const double len = v1 - v0;
+  if (len == 0.0) return 0.0;
+  int n = (int)ceil(fabs(len) / hmax);
+  n = n < 1 ? 1 : (n > 64 ? 64 : n);
+  const double h = len / n;
+  double sum = 0.0;
+  for (int p = 0; p < n; ++p) {
+    const double c = v0 + (p + 0.5) * h, hh = 0.5 * h;
+    double s = 0.0;
+    for (int k = 0; k < 8; ++k) {
+      s += kGl16[k].w * (integrand(q, c - hh * kGl16[k].x) + integrand(q, c + hh * kGl16[k].x));
+    }
+    sum += s * hh;
+  }
+  return sum;
+}
+
+// Radial set-up. C = K of the tracer (q_R + (lambda - a)^2); a2_alam = a^2 - a lambda.
+BHM_HD Radial radial_motion(double a2, double a2_alam, double C, double r_obs, double r_plus, double r_hor,
+                            double r_esc) {
+  Radial q{};
+  q.p2 = 2.0 * a2_alam - C;
+  q.p1 = 2.0 * C;
+  q.p0 = a2_alam * a2_alam - a2 * C;
+  q.kind = -1;
+  if (q.p0 > 0.0) return q;  // q_R < 0: more than two roots possible above r+
+  const double rm = largest_dR_root(q.p2, q.p1);
+  q.r_min = 0.0;
+  q.R_min = 0.0;
+  if (rm > r_plus) {
+    q.r_min = rm;
+    q.R_min = poly_R(q, rm);
+  }
+  if (q.r_min > 0.0 && q.R_min < 0.0) {
+    // Largest root of R: Newton from the right on the convex branch.
+    const double d2 = 12.0 * rm * rm + 2.0 * q.p2;
+    double r = rm + sqrt(-2.0 * q.R_min / fmax(d2, 1e-300));
+    for (int it = 0; it < 100; ++it) {
+      const double r2 = r * r;
+      const double R = (r2 + q.p2) * r2 + q.p1 * r + q.p0;
+      const double dR = 4.0 * r2 * r + 2.0 * q.p2 * r + q.p1;
+      const double dr = R / dR;
+      r -= dr;
+      if (fabs(dr) <= 1e-15 * r) break;
+    }
+    if (!(r > r_hor) || !(r < r_obs)) return q;  // turning point inside the horizon cut or beyond the observer
+    q.kind = 1;
+    q.x_tp = 1.0 / r;
+    // P(x) = (x - x_tp) Q(x) (synthetic division, remainder dropped); P / (x_tp - x) = -Q.
+    const double b3 = q.p0;
+    const double b2 = q.p1 + q.x_tp * b3;
+    const double b1 = q.p2 + q.x_tp * b2;
+    const double b0 = q.x_tp * b1;
+    q.q3 = -b3;
+    q.q2 = -b2;
+    q.q1 = -b1;
+    q.q0 = -b0;
+    q.v_obs = -sqrt(q.x_tp - 1.0 / r_obs);
+    q.v_end = sqrt(q.x_tp - 1.0 / r_esc);
+  } else {
+    q.kind = 0;
+    q.v_obs = 1.0 / r_obs;
+    q.v_end = 1.0 / r_hor;
+  }
+  return q;
+}
+
+// Solve tau(v) = T for v in [lo, hi] with tau(lo) = tlo <= T <= tau(hi) = thi.
+BHM_HD bool solve_tau(const Radial& q, double T, double lo, double tlo, double hi, double thi, double seed,
+                      double hmax, double& v_out, double& t_out) {
+  double v = (seed > lo && seed < hi) ? seed : lo + (hi - lo) * ((T - tlo) / (thi - tlo));
+  if (!(v > lo && v < hi)) v = 0.5 * (lo + hi);
+  double tv = (v - lo < hi - v) ? tlo + integrate(q, lo, v, hmax) : thi - integrate(q, v, hi, hmax);
+  for (int it = 0; it < 60; ++it) {
+    if (tv < T) {
+      lo = v;
+      tlo = tv;
+    } else {
+      hi = v;
+      thi = tv;
+    }
+    double vn = v + (T - tv) / integrand(q, v);
+    if (!(vn > lo && vn < hi)) vn = 0.5 * (lo + hi);
+    const double step = vn - v;
+    const double tn = tv + integrate(q, v, vn, hmax);
+    v = vn;
+    tv = tn;
+    if (fabs(step) <= 1e-14 * fmax(1e-3, fabs(v)) || hi - lo <= 1e-15) {
+      v_out = v;
+      t_out = tv;
+      return true;
+    }
+  }
+  return false;
+}
+
+struct Crossings {
+  int status;      // 0 ok, -1 radial form not handled, -2 no convergence
+  int kind;        // radial kind (1 escapes, 0 falls in)
+  int n_hits;      // disk hits found (<= max_hits)
+  double r[3];     // their radii
+  double r_min;    // largest local minimum of R above r+ (0 if none) ...
+  double R_min;    // ... and R there: near zero next to the critical curve
+};
+
+// Disk crossings (r_in <= r <= r_out) of a ray in the order the tracer finds
+// them, up to max_hits (<= 3), from the ray's constants: spin a, lambda,
+// q_Th (theta potential) and C = q_R + (lambda - a)^2 (radial potential),
+// u0 = cos theta_obs and pu0 = du/dtau at the observer. r_seed > 0 is a guess
+// of the first hit radius that starts the Newton iterations.
+BHM_HD Crossings crossings(double a, double lam, double qTh, double C, double r_obs, double r_plus, double r_hor,
+                           double r_esc, double r_in, double r_out, double u0, double pu0, double r_seed,
+                           int max_hits, double hmax) {
+  Crossings c{};
+  c.status = 0;
+  c.n_hits = 0;
+  const double a2 = a * a;
+  const double a2_alam = a2 - a * lam;
+  const Radial q = radial_motion(a2, a2_alam, C, r_obs, r_plus, r_hor, r_esc);
+  c.kind = q.kind;
+  c.r_min = q.r_min;
+  c.R_min = q.R_min;
+  if (q.kind < 0) {
+    c.status = -1;
+    return c;
+  }
+  const ThetaMotion th = theta_motion(a2, qTh, lam, u0, pu0);
+  if (!th.crosses) return c;
+  const double t_end = integrate(q, q.v_obs, q.v_end, hmax);
+  double seed_v[2] = {NAN, NAN};
+  if (r_seed > 0.0) {
+    if (q.kind == 1) {
+      const double s = sqrt(fmax(0.0, q.x_tp - 1.0 / r_seed));
+      seed_v[0] = -s;
+      seed_v[1] = s;
+    } else {
+      seed_v[0] = 1.0 / r_seed;
+    }
+  }
+  double lo = q.v_obs, tlo = 0.0;
+  for (int n = 0; n < 64; ++n) {
+    const double T = th.tau1 + n * th.period;
+    if (!(T < t_end)) break;
+    double seed = NAN;
+    if (seed_v[0] > lo && seed_v[0] < q.v_end)
+      seed = seed_v[0];
+    else if (seed_v[1] > lo && seed_v[1] < q.v_end)
+      seed = seed_v[1];
+    double v, tv;
+    if (!solve_tau(q, T, lo, tlo, q.v_end, t_end, seed, hmax, v, tv)) {
+      c.status = -2;
+      return c;
+    }
+    const double r = radius_of(q, v);
+    if (r >= r_in && r <= r_out) {
+      c.r[c.n_hits++] = r;
+      if (c.n_hits >= max_hits) break;
+    }
+    lo = v;
+    tlo = tv;
+  }
+  return c;
+}
+
+// u = cos theta reached at Mino time tau from (u0, pu0) (the ray must cross
+// the equator: theta_motion(...).crosses). chi increases monotonically:
+// u = sqrt(z+) sin chi, Phi(chi) = int_0^chi dchi / sqrt(w + m sin^2 chi).
+BHM_HD double u_at(double a2, double qTh, double lam, double u0, double pu0, double tau) {
+  const double c0 = qTh - lam * lam;
+  const double b2 = a2 - qTh;
+  const double sq = sqrt(b2 * b2 + 4.0 * a2 * c0);
+  const double zp = (b2 > 0.0) ? (b2 + sq) / (2.0 * a2) : 2.0 * c0 / (sq - b2);
+  const double w = c0 / zp, m = a2 * zp, rz = sqrt(zp);
+  const double s0 = fmax(-1.0, fmin(1.0, u0 / rz));
+  const double K = carlson_rf(0.0, w + m, w);
+  const double phi_x = s0 * carlson_rf(w * (1.0 - s0 * s0), w + m * s0 * s0, w);  // odd in s0
+  const double phi_start = (pu0 >= 0.0) ? phi_x : 2.0 * K - phi_x;
+  double total = phi_start + tau;
+  const double n = floor(total / (2.0 * K));
+  double rem = total - n * 2.0 * K;  // in [0, 2K)
+  const bool second = rem > K;
+  if (second) rem = 2.0 * K - rem;   // chi' -> pi - chi' has the same sine
+  // Phi(chi) = rem on [0, pi/2]: bracketed Newton.
+  double lo = 0.0, hi = 1.5707963267948966, chi = rem * sqrt(w + 0.5 * m);
+  chi = fmin(fmax(chi, lo), hi);
+  for (int it = 0; it < 60; ++it) {
+    const double s = sin(chi), c = cos(chi);
+    const double f = s * carlson_rf(w * c * c, w + m * s * s, w) - rem;
+    if (f < 0.0) lo = chi; else hi = chi;
+    double nc = chi - f * sqrt(w + m * s * s);
+    if (!(nc > lo && nc < hi)) nc = 0.5 * (lo + hi);
+    const double step = nc - chi;
+    chi = nc;
+    if (fabs(step) < 1e-15) break;
+  }
+  const double sgn = (fmod(n, 2.0) != 0.0) ? -1.0 : 1.0;
+  return sgn * rz * sin(chi);
+}
+
+// Mino time at which the tracer stops (escape or horizon radius).
+BHM_HD double tau_end(const Radial& q, double hmax) { return integrate(q, q.v_obs, q.v_end, hmax); }
+
+// First-order image-plane distance (M) from pixel (alpha, beta) to the
+// critical curve: |R(r_min)| over the (alpha, beta) gradient of R at fixed
+// r = r_min (the envelope of R's minimum). carter selects q_R = eta
+// (textbook) instead of the reference's q_R = eta + lambda^2.
+BHM_HD double critical_distance(double r_min, double R_min, double a, double lam, bool carter, double sin_o,
+                                double cos_o, double alpha, double beta) {
+  if (!(r_min > 0.0)) return INFINITY;
+  const double r = r_min;
+  const double A = r * r + a * a - a * lam;
+  const double D = r * r - 2.0 * r + a * a;
+  const double dC_dlam = (carter ? 0.0 : 2.0 * lam) + 2.0 * (lam - a);
+  const double dR_dlam = -2.0 * a * A - D * dC_dlam;
+  const double dR_deta = -D;
+  const double gx = -dR_dlam * sin_o + dR_deta * 2.0 * alpha * cos_o * cos_o;
+  const double gy = dR_deta * 2.0 * beta;
+  return fabs(R_min) / fmax(sqrt(gx * gx + gy * gy), 1e-300);
+}
+
+}  // namespace bhmino

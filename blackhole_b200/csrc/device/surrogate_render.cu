@@ -1,0 +1,154 @@
+// surrogate_render.cu - per-pixel decision of the surrogate renderer.
+//
+// Input: the network's head outputs for every pixel of a frame. Each pixel
+// either takes the network's answer -- refined exactly where the answer is a
+// disk hit -- or joins the list of pixels the integrator retraces:
+//   1. class confidence below the threshold          -> integrator
+//   2. within the stated image-plane distance of the
+//      critical curve (first-order, from the minimum
+//      of the radial potential)                       -> integrator
+//   3. radial potential of a form not handled, or the
+//      exact solve does not converge                  -> integrator
+//   4. the exact solve disagrees with the network's
+//      class                                          -> integrator
+// Accepted disk pixels get r_hit from the Mino-time solve seeded with the
+// network's radius, and g, flux and intensity from r_hit exactly as the
+// tracer computes them; escaped pixels get theta_inf from the exact polar
+// motion at the escape radius; phi_hit and phi_inf are the network's.
+#include <cuda_runtime.h>
+
+#include "image_fp64.cuh"
+#include "launch.h"
+#include "mino_solve.cuh"
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr double kPanel = 0.125;  // Gauss-Legendre panel width of the Mino-time quadrature
+
+__device__ __forceinline__ void warp_count(unsigned *stats, int slot, bool pred) {
+  const unsigned m = __ballot_sync(kFull, pred);
+  if ((threadIdx.x & 31u) == 0 && m) atomicAdd(stats + slot, (unsigned)__popc(m));
+}
+
+__global__ void __launch_bounds__(128) k_surrogate_refine(const __grid_constant__ BhkImageParams p,
+                                                          const __grid_constant__ BhkImageOut o,
+                                                          const float *__restrict__ head, float min_conf,
+                                                          double band, int verify, int *__restrict__ list,
+                                                          unsigned int *__restrict__ count,
+                                                          unsigned int *__restrict__ stats) {
+  const long long pix = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = pix < p.n_pix;
+  int reason = 0;  // 0 accepted, 1 confidence, 2 critical band, 3 solve, 4 disagreement
+  if (live) {
+    const long long i = pix % p.width, j = pix / p.width;
+    const double alpha = p.alpha_min + ((double)i + 0.5) * p.dalpha;
+    const double beta = p.beta_min + ((double)j + 0.5) * p.dbeta;
+    const double a = p.a;
+    const double lam = -alpha * p.sin_o;
+    const double eta = beta * beta + (alpha * alpha - a * a) * p.cos_o * p.cos_o;
+    const double qTh = eta + lam * lam;
+    const double qR = (p.form == 1) ? eta : qTh;
+    const double C = qR + (lam - a) * (lam - a);
+    const double pu0 = beta * p.sin_o;
+
+    const float *h = head + pix * 16;
+    const float m = fmaxf(h[0], fmaxf(h[1], h[2]));
+    const float e0 = __expf(h[0] - m), e1 = __expf(h[1] - m), e2 = __expf(h[2] - m);
+    const float Z = e0 + e1 + e2;
+    const int nn_cls = (e1 >= e0 && e1 >= e2) ? 1 : ((e2 >= e0) ? 2 : 0);
+    const float conf = fmaxf(e0, fmaxf(e1, e2)) / Z;
+
+    if (!(conf >= min_conf)) {
+      reason = 1;
+    } else {
+      const bhmino::Radial q = bhmino::radial_motion(p.a2, p.a2 - a * lam, C, p.r_obs, p.r_plus, p.r_hor, p.r_esc);
+      const double d = bhmino::critical_distance(q.r_min, q.R_min, a, lam, p.form == 1, p.sin_o, p.cos_o, alpha,
+                                                 beta);
+      if (q.kind < 0) {
+        reason = 3;
+      } else if (d < band) {
+        reason = 2;
+      } else {
+        int cls = q.kind == 1 ? 2 : 0;  // radial kind: escapes or falls in
+        int nhit = 0;
+        double rh[3] = {0.0, 0.0, 0.0};
+        bool solved = true;
+        if (nn_cls == 1 || verify >= 2) {
+          const double r_seed = exp((double)h[3] + 2.0);
+          const bhmino::Crossings c =
+              bhmino::crossings(a, lam, qTh, C, p.r_obs, p.r_plus, p.r_hor, p.r_esc, p.r_in, p.r_out, p.cos_o, pu0,
+                                r_seed, p.max_cross, kPanel);
+          solved = c.status == 0;
+          nhit = c.n_hits;
+          for (int k = 0; k < 3; ++k) rh[k] = c.r[k];
+          if (nhit >= p.max_cross) cls = 1;
+        }
+        const int opaque_cls = nhit > 0 ? 1 : cls;
+        if (!solved) {
+          reason = 3;
+        } else if (verify >= 1 && opaque_cls != nn_cls) {
+          reason = 4;
+        } else if (nhit > 0 && cls == 2) {
+          reason = 4;  // passed the disk and escaped: the network has no escape direction for it
+        } else {
+          double th_inf = 0.0, ph_inf = 0.0;
+          if (cls == 2) {
+            const bhmino::ThetaMotion tm = bhmino::theta_motion(p.a2, qTh, lam, p.cos_o, pu0);
+            if (tm.crosses) {
+              const double te = bhmino::tau_end(q, kPanel);
+              const double u = bhmino::u_at(p.a2, qTh, lam, p.cos_o, pu0, te);
+              th_inf = acos(fmin(1.0, fmax(-1.0, u)));
+            } else {
+              th_inf = acos(fmin(1.0, fmax(-1.0, (double)h[10])));
+            }
+            ph_inf = atan2((double)h[12], (double)h[11]);
+          }
+          double inten = 0.0;
+          for (int k = 0; k < p.max_cross; ++k) {
+            const long long off = (long long)k * p.n_pix + pix;
+            double r = 0.0, g = 0.0, ph = 0.0;
+            if (k < nhit) {
+              r = rh[k];
+              g = bhk::disk_g(r, a, lam);
+              const double qq = p.r_in / r;
+              inten += g * g * g * g * qq * qq * qq;
+              ph = (k == 0) ? atan2((double)h[5], (double)h[4]) : ((k == 1) ? atan2((double)h[8], (double)h[7]) : 0.0);
+            }
+            if (o.r_hit) o.r_hit[off] = r;
+            if (o.g) o.g[off] = g;
+            if (o.phi_hit) o.phi_hit[off] = ph;
+          }
+          if (o.cls) o.cls[pix] = cls;
+          if (o.steps) o.steps[pix] = 0;
+          if (o.n_cross) o.n_cross[pix] = nhit;
+          if (o.flux) o.flux[pix] = nhit > 0 ? bhk::nt_flux(rh[0], p.nt_isco, p.nt_flux_peak) : 0.0;
+          if (o.intensity) o.intensity[pix] = inten;
+          if (o.theta_inf) o.theta_inf[pix] = th_inf;
+          if (o.phi_inf) o.phi_inf[pix] = ph_inf;
+        }
+      }
+    }
+  }
+  // Append the pixels the integrator must retrace (one atomic per warp).
+  const bool fb = live && reason != 0;
+  const unsigned mask = __ballot_sync(kFull, fb);
+  const unsigned lane = threadIdx.x & 31u;
+  unsigned base = 0;
+  if (lane == 0 && mask) base = atomicAdd(count, (unsigned)__popc(mask));
+  base = __shfl_sync(kFull, base, 0);
+  if (fb) list[base + __popc(mask & ((1u << lane) - 1u))] = (int)pix;
+  for (int r = 0; r < 5; ++r) warp_count(stats, r, live && reason == r);
+}
+
+}  // namespace
+
+extern "C" int bhk_surrogate_refine(const BhkImageParams *p, const BhkImageOut *o, const float *head, float min_conf,
+                                    double band, int verify, int *list, unsigned int *count, unsigned int *stats,
+                                    void *stream) {
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (p->n_pix <= 0) return 0;
+  const long long blocks = (p->n_pix + 127) / 128;
+  k_surrogate_refine<<<(unsigned)blocks, 128, 0, s>>>(*p, *o, head, min_conf, band, verify, list, count, stats);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}

@@ -276,6 +276,15 @@ __global__ void __launch_bounds__(128) k_trace_image_mixed(const __grid_constant
 }
 
 template <int INTEG>
+__global__ void __launch_bounds__(128) k_trace_list_mixed(const __grid_constant__ BhkImageParams p,
+                                                          const __grid_constant__ BhkImageOut o,
+                                                          const int *__restrict__ list,
+                                                          const unsigned int *__restrict__ count,
+                                                          unsigned long long *__restrict__ counter, int refill) {
+  trace_loop<INTEG>(bhsrc::ListSrc{p, o, list, count}, counter, refill);
+}
+
+template <int INTEG>
 __global__ void __launch_bounds__(128) k_trace_batch_mixed(const __grid_constant__ BhkBatchDev b,
                                                            unsigned long long *__restrict__ counter, int refill) {
   if (threadIdx.x == 0) atomicMin(b.start_ns, bhsrc::globaltimer_ns());
@@ -301,6 +310,18 @@ extern "C" int bhk_trace_image_mixed_occupancy(int integrator, int block, int *b
           ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhm::k_trace_image_mixed<0>, block, 0)
           : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhm::k_trace_image_mixed<1>, block, 0);
   return e == cudaSuccess ? 0 : -1;
+}
+
+extern "C" int bhk_trace_list_mixed(const BhkImageParams *p, const BhkImageOut *o, const int *list,
+                                    const unsigned int *count, unsigned long long *counter, BhkLaunch L,
+                                    void *stream) {
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s) != cudaSuccess) return -1;
+  if (p->integrator == 0)
+    bhm::k_trace_list_mixed<0><<<L.grid, L.block, 0, s>>>(*p, *o, list, count, counter, L.refill);
+  else
+    bhm::k_trace_list_mixed<1><<<L.grid, L.block, 0, s>>>(*p, *o, list, count, counter, L.refill);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
 extern "C" int bhk_trace_batch_mixed(const BhkBatchDev *b, int integrator, unsigned long long *counter, BhkLaunch L,

@@ -42,6 +42,13 @@ struct BH_Surrogate {
   // inference chunk buffers (grow-only)
   int64_t inf_rows = 0;
   bf16 *iF = nullptr, *iA = nullptr, *iB = nullptr;
+  // renderer buffers (grow-only)
+  int64_t ren_pixels = 0;
+  float *r_inputs = nullptr, *r_head = nullptr;
+  int *r_list = nullptr;
+  unsigned int *r_counts = nullptr;  // [0] list length, [1..5] stats
+  unsigned long long *r_counter = nullptr;
+  int64_t last_pixels = 0;
 };
 
 namespace {
@@ -405,6 +412,84 @@ int bh_surrogate_grid_inputs(const BH_KerrScene *sc, float *inputs, void *stream
   if (bhs_launch_grid_inputs(sc->spin, std::cos(sc->theta_obs), sc->alpha_min, da, sc->beta_min, db, sc->width, n,
                              inputs, static_cast<cudaStream_t>(stream)))
     return fail_msg("surrogate: grid-input launch failed");
+  return 0;
+}
+
+void bh_surrogate_policy_defaults(BH_SurrogatePolicy *p) {
+  if (!p) return;
+  p->min_confidence = 0.99f;
+  p->verify = 1;
+  p->critical_band = 0.05;
+}
+
+int bh_surrogate_trace_image(BH_Surrogate *s, const BH_KerrScene *scene, const BH_KerrImageOut *out,
+                             const BH_SurrogatePolicy *policy, void *stream) {
+  if (!s || !scene || !out) return fail_msg("surrogate render: NULL argument");
+  BH_SurrogatePolicy pol;
+  bh_surrogate_policy_defaults(&pol);
+  if (policy) pol = *policy;
+  if (!(pol.min_confidence >= 0.0f && pol.min_confidence <= 1.0f) || pol.verify < 1 || pol.verify > 2 ||
+      !(pol.critical_band >= 0.0))
+    return fail_msg("surrogate render: policy needs min_confidence in [0, 1], verify 1 or 2, critical_band >= 0");
+  BH_KerrScene sc = *scene;
+  sc.precision = BH_PRECISION_MIXED;  // the fallback integrator
+  BhkImageParams p;
+  BhkLaunch L;
+  if (bhh_prepare_image_launch(&sc, &p, &L) != 0) return -1;
+  const int64_t n = p.n_pix;
+  s->last_pixels = n;
+  if (n == 0) return 0;
+  if (n > s->ren_pixels) {
+    for (void *q : {static_cast<void *>(s->r_inputs), static_cast<void *>(s->r_head), static_cast<void *>(s->r_list)}) {
+      if (!q) continue;
+      auto it = std::find(s->allocs.begin(), s->allocs.end(), q);
+      if (it != s->allocs.end()) s->allocs.erase(it);
+      cudaFree(q);
+    }
+    s->r_inputs = s->r_head = nullptr;
+    s->r_list = nullptr;
+    s->ren_pixels = 0;
+    if (int rc = alloc(s, &s->r_inputs, static_cast<size_t>(n) * 4, "cudaMalloc(render inputs)")) return rc;
+    if (int rc = alloc(s, &s->r_head, static_cast<size_t>(n) * BHS_HEAD, "cudaMalloc(render head)")) return rc;
+    if (int rc = alloc(s, &s->r_list, static_cast<size_t>(n), "cudaMalloc(fallback list)")) return rc;
+    s->ren_pixels = n;
+  }
+  if (!s->r_counts) {
+    if (int rc = alloc(s, &s->r_counts, 8, "cudaMalloc(render counters)")) return rc;
+    if (int rc = alloc(s, &s->r_counter, 1, "cudaMalloc(work counter)")) return rc;
+  }
+  auto st = static_cast<cudaStream_t>(stream);
+  const double da = (sc.alpha_max - sc.alpha_min) / sc.width, db = (sc.beta_max - sc.beta_min) / sc.height;
+  if (bhs_launch_grid_inputs(sc.spin, std::cos(sc.theta_obs), sc.alpha_min, da, sc.beta_min, db, sc.width, n,
+                             s->r_inputs, st))
+    return fail_msg("surrogate render: input launch failed");
+  if (int rc = bh_surrogate_forward(s, s->r_inputs, n, s->r_head, stream)) return rc;
+  if (int rc = cuda_check(cudaMemsetAsync(s->r_counts, 0, 8 * sizeof(unsigned int), st), "cudaMemsetAsync"))
+    return rc;
+  const BhkImageOut o{out->cls,   out->steps,     out->n_cross,   out->r_hit,     out->phi_hit,
+                      out->g,     out->flux,      out->intensity, out->theta_inf, out->phi_inf};
+  if (bhk_surrogate_refine(&p, &o, s->r_head, pol.min_confidence, pol.critical_band, pol.verify, s->r_list,
+                           s->r_counts, s->r_counts + 1, stream))
+    return fail_msg("surrogate render: refine launch failed");
+  if (bhk_trace_list_mixed(&p, &o, s->r_list, s->r_counts, s->r_counter, L, stream))
+    return fail_msg("surrogate render: fallback tracer launch failed");
+  return 0;
+}
+
+int bh_surrogate_last_stats(BH_Surrogate *s, BH_SurrogateStats *out) {
+  if (!s || !out) return fail_msg("surrogate stats: NULL argument");
+  unsigned int c[8] = {};
+  if (s->r_counts) {
+    if (int rc = cuda_check(cudaDeviceSynchronize(), "cudaDeviceSynchronize")) return rc;
+    if (int rc = cuda_check(cudaMemcpy(c, s->r_counts, sizeof(c), cudaMemcpyDeviceToHost), "cudaMemcpy(stats)"))
+      return rc;
+  }
+  out->pixels = s->last_pixels;
+  out->accepted = c[1];
+  out->low_confidence = c[2];
+  out->critical_band = c[3];
+  out->solve_failed = c[4];
+  out->disagreement = c[5];
   return 0;
 }
 

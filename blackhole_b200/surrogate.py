@@ -156,6 +156,25 @@ class Surrogate:
         check(self._lib.bh_surrogate_train_step(self._h, _ptr(inputs), _ptr(targets), inputs.shape[0],
                                                 C.byref(cfg), _ptr(loss), _stream(stream)))
 
+    def trace_image(self, scene, outs: dict | None = None, min_confidence: float = 0.99, verify: int = 1,
+                    critical_band: float = 0.05, stream=None) -> dict:
+        """Render a scene through the network with exact refinement and the
+        integrator on rejected pixels (bh_surrogate_trace_image)."""
+        from .kerr import _out_struct, alloc_image_outputs
+
+        if outs is None:
+            outs = alloc_image_outputs(scene)
+        pol = _abi.SurrogatePolicy(min_confidence, verify, critical_band)
+        o = _out_struct(outs)
+        check(self._lib.bh_surrogate_trace_image(self._h, C.byref(scene), C.byref(o), C.byref(pol),
+                                                 _stream(stream)))
+        return outs
+
+    def last_stats(self) -> dict:
+        st = _abi.SurrogateStats()
+        check(self._lib.bh_surrogate_last_stats(self._h, C.byref(st)))
+        return {name: int(getattr(st, name)) for name, _ in st._fields_}
+
     def device_error(self) -> int:
         rc = self._lib.bh_surrogate_device_error(self._h)
         if rc < 0:

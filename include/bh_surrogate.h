@@ -85,6 +85,38 @@ int bh_surrogate_make_targets(const BH_KerrImageOut* outs, int64_t n, int max_cr
 /* Inputs [width * height][4] of a scene's pixel centres. */
 int bh_surrogate_grid_inputs(const BH_KerrScene* scene, float* inputs, void* stream);
 
+/* Which pixels the surrogate renderer leaves to the integrator. */
+typedef struct BH_SurrogatePolicy {
+    float min_confidence;  /* softmax class probability below this -> integrator (0.99) */
+    int32_t verify;        /* 1: check the radial kind of captured/escaped predictions;
+                              2: run the exact crossing search on every pixel */
+    double critical_band;  /* first-order image-plane distance to the critical curve, M,
+                              below which a pixel goes to the integrator (0.05) */
+} BH_SurrogatePolicy;
+
+typedef struct BH_SurrogateStats {
+    int64_t pixels;
+    int64_t accepted;        /* answered without the integrator */
+    int64_t low_confidence;
+    int64_t critical_band;
+    int64_t solve_failed;    /* radial potential not handled or no convergence */
+    int64_t disagreement;    /* exact solve contradicts the network's class */
+} BH_SurrogateStats;
+
+void bh_surrogate_policy_defaults(BH_SurrogatePolicy* policy);
+
+/* Render a scene through the surrogate: network inference on every pixel,
+ * exact Mino-time refinement of accepted disk hits (r_hit, g, flux,
+ * intensity) and of escaped pixels' theta_inf, and the mixed-precision
+ * integrator (the scene's integrator) on every pixel the policy rejects.
+ * Outputs as bh_kerr_trace_image; for accepted pixels steps = 0 and phi_hit,
+ * phi_inf are the network's. Asynchronous on `stream`; no host sync. */
+int bh_surrogate_trace_image(BH_Surrogate* s, const BH_KerrScene* scene, const BH_KerrImageOut* out,
+                             const BH_SurrogatePolicy* policy, void* stream);
+
+/* Counts of the last bh_surrogate_trace_image (synchronises the device). */
+int bh_surrogate_last_stats(BH_Surrogate* s, BH_SurrogateStats* stats);
+
 /* C = A * B^T in FP32 for BF16 A [M][K], B [N][K] (K a multiple of 8;
  * N = 16, 192 or a multiple of 256): the tensor-core GEMM the network uses. */
 int bh_bf16_gemm(const void* A, const void* B, int64_t M, int N, int K, float* C, void* stream);

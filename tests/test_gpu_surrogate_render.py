@@ -1,0 +1,91 @@
+"""GPU checks of the surrogate renderer (bh_surrogate_trace_image).
+
+* with an untrained network no pixel is confident, so every pixel goes to
+  the integrator and the image equals the mixed-precision tracer's bit for
+  bit (the fallback list traces the same per-pixel arithmetic);
+* with the confidence gate off and the full exact crossing search, every
+  pixel the exact solve decides (those where the untrained network's class
+  happens to agree) matches the FP64 oracle: class, disk radius, redshift;
+* with the trained network shipped in blackhole_b200/data, the a = 0.9
+  disk scene meets the accuracy targets against the FP64 oracle.
+"""
+from __future__ import annotations
+
+import math
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+WEIGHTS = Path(__file__).resolve().parent.parent / "blackhole_b200" / "data" / "surrogate_c4.npz"
+
+
+def c4_scene(W, **kw):
+    from blackhole_b200 import kerr
+
+    args = dict(width=W, height=W, spin=0.9, theta_obs=math.radians(60), integrator=1, max_crossings=1)
+    args.update(kw)
+    return kerr.scene(**args)
+
+
+def host(o):
+    return {k: v.cpu().numpy() for k, v in o.items()}
+
+
+def test_untrained_network_falls_back_everywhere(cuda):
+    from blackhole_b200 import kerr
+    from blackhole_b200 import surrogate as S
+
+    net = S.Surrogate(max_batch=128, seed=3)
+    s = c4_scene(96, precision=1)
+    got = host(net.trace_image(s))
+    st = net.last_stats()
+    assert st["pixels"] == 96 * 96 and st["accepted"] == 0 and st["low_confidence"] == 96 * 96
+    ref = host(kerr.trace_image(s))
+    torch.cuda.synchronize()
+    for k in ref:
+        np.testing.assert_array_equal(got[k], ref[k], err_msg=k)
+
+
+@pytest.mark.parametrize("spin,incl,form", [(0.9, 60, 0), (0.998, 85, 0), (0.3, 17, 1)])
+def test_exact_solve_matches_oracle(cuda, oracle, spin, incl, form):
+    from blackhole_b200 import surrogate as S
+
+    net = S.Surrogate(max_batch=128, seed=4)
+    s = c4_scene(80, spin=spin, theta_obs=math.radians(incl), potential_form=form, precision=1)
+    got = host(net.trace_image(s, min_confidence=0.0, verify=2, critical_band=0.05))
+    st = net.last_stats()
+    assert st["accepted"] > 0 and st["solve_failed"] < 0.01 * st["pixels"]
+    so = c4_scene(80, spin=spin, theta_obs=math.radians(incl), potential_form=form, precision=0)
+    ref = oracle.trace_pixels(so)
+    acc = got["steps"] == 0  # answered without the integrator
+    np.testing.assert_array_equal(got["cls"][acc], ref["cls"][acc])
+    assert np.mean(got["cls"] == ref["cls"]) >= 0.999
+    d = acc & (ref["n_cross"] > 0)
+    assert d.any()
+    np.testing.assert_allclose(got["r_hit"][0][d], ref["r_hit"][0][d], rtol=1e-6)
+    np.testing.assert_allclose(got["g"][0][d], ref["g"][0][d], rtol=1e-6)
+    np.testing.assert_allclose(got["flux"][d], ref["flux"][d], rtol=1e-5, atol=1e-12)
+    esc = acc & (ref["cls"] == 2)
+    assert np.abs(got["theta_inf"][esc] - ref["theta_inf"][esc]).max() < 2e-3
+
+
+@pytest.mark.skipif(not WEIGHTS.exists(), reason="trained weights not shipped")
+def test_trained_network_meets_targets(cuda, oracle):
+    from blackhole_b200 import surrogate as S
+
+    net = S.Surrogate(max_batch=128)
+    net.load(WEIGHTS)
+    s = c4_scene(256, precision=1)
+    got = host(net.trace_image(s))
+    st = net.last_stats()
+    assert st["accepted"] > 0.5 * st["pixels"], st
+    ref = oracle.trace_pixels(c4_scene(256, precision=0))
+    agree = np.mean(got["cls"] == ref["cls"])
+    assert agree >= 0.999, agree
+    d = (got["n_cross"] > 0) & (ref["n_cross"] > 0)
+    rel = np.abs(got["g"][0][d] - ref["g"][0][d]) / ref["g"][0][d]
+    assert np.median(rel) <= 1e-4 and rel.max() <= 1e-3, (np.median(rel), rel.max())
