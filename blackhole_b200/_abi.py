@@ -118,7 +118,8 @@ class AdamConfig(C.Structure):
 class SurrogatePolicy(C.Structure):
     """struct BH_SurrogatePolicy."""
 
-    _fields_ = [("min_confidence", C.c_float), ("verify", C.c_int32), ("critical_band", C.c_double)]
+    _fields_ = [("min_confidence", C.c_float), ("verify", C.c_int32), ("critical_band", C.c_double),
+                ("refine_fp64", C.c_int32), ("reserved", C.c_int32)]
 
 
 class SurrogateStats(C.Structure):

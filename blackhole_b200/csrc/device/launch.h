@@ -94,8 +94,8 @@ int bhk_trace_list_mixed(const BhkImageParams *p, const BhkImageOut *o, const in
 // and the list of pixels left to the integrator. stats[5] += pixels accepted,
 // low confidence, critical band, solve failed, disagreement.
 int bhk_surrogate_refine(const BhkImageParams *p, const BhkImageOut *o, const float *head, float min_conf,
-                         double band, int verify, int *list, unsigned int *count, unsigned int *stats,
-                         void *stream);
+                         double band, int verify, int refine_fp64, int *list, unsigned int *count,
+                         unsigned int *stats, void *stream);
 
 // Reference stepper kernels (src/physics/kerr.cpp semantics), FP64.
 typedef struct BhkStateSoA { double *r, *theta, *phi, *t, *sr, *sth; } BhkStateSoA;

@@ -1,5 +1,5 @@
 // mino_solve.cuh - exact equatorial crossings of a Kerr image-plane ray
-// without stepping (FP64, host and device).
+// without stepping (FP64; device code under nvcc, plain C++ elsewhere).
 //
 // The image tracer integrates r'' = R'(r)/2, u'' = U'(u)/2 in Mino time tau
 // with p_r^2 = R, p_u^2 = U (u = cos theta). Both motions separate, so the
@@ -29,12 +29,20 @@
 #include <cmath>
 
 #ifdef __CUDACC__
-#define BHM_HD __host__ __device__ __forceinline__
+#define BHM_HD __device__ __forceinline__
 #else
 #define BHM_HD inline
 #endif
 
 namespace bhmino {
+
+#ifdef __CUDACC__
+BHM_HD double inv_sqrt(double x) { return rsqrt(x); }
+BHM_HD float inv_sqrt(float x) { return rsqrtf(x); }
+#else
+BHM_HD double inv_sqrt(double x) { return 1.0 / std::sqrt(x); }
+BHM_HD float inv_sqrt(float x) { return 1.0f / std::sqrt(x); }
+#endif
 
 // Gauss-Legendre, 16 points on [-1, 1]: the 8 positive nodes and weights.
 struct GlNode {
@@ -49,24 +57,73 @@ __constant__
         {7.55404408355002999e-01, 1.24628971255534071e-01}, {8.65631202387831755e-01, 9.51585116824926053e-02},
         {9.44575023073232600e-01, 6.22535239386474565e-02}, {9.89400934991649939e-01, 2.71524594117541762e-02}};
 
+// Gauss-Legendre, 8 points on [-1, 1]: the 4 positive nodes and weights.
+#ifdef __CUDACC__
+__constant__
+#endif
+    static const GlNode kGl8[4] = {{1.83434642495649805e-01, 3.62683783378361983e-01},
+                                   {5.25532409916328986e-01, 3.13706645877887287e-01},
+                                   {7.96666477413626740e-01, 2.22381034453374471e-01},
+                                   {9.60289856497536232e-01, 1.01228536290376259e-01}};
+
+// The same nodes and weights in FP32 (the FP32 quadrature of the fast path).
+struct GlNodeF {
+  float x, w;
+};
+#ifdef __CUDACC__
+__constant__
+#endif
+    static const GlNodeF kGl16f[8] = {{9.50125098376374405e-02f, 1.89450610455068641e-01f},
+                                      {2.81603550779258915e-01f, 1.82603415044923639e-01f},
+                                      {4.58016777657227370e-01f, 1.69156519395002647e-01f},
+                                      {6.17876244402643771e-01f, 1.49595988816576708e-01f},
+                                      {7.55404408355002999e-01f, 1.24628971255534071e-01f},
+                                      {8.65631202387831755e-01f, 9.51585116824926053e-02f},
+                                      {9.44575023073232600e-01f, 6.22535239386474565e-02f},
+                                      {9.89400934991649939e-01f, 2.71524594117541762e-02f}};
+#ifdef __CUDACC__
+__constant__
+#endif
+    static const GlNodeF kGl8f[4] = {{1.83434642495649805e-01f, 3.62683783378361983e-01f},
+                                     {5.25532409916328986e-01f, 3.13706645877887287e-01f},
+                                     {7.96666477413626740e-01f, 2.22381034453374471e-01f},
+                                     {9.60289856497536232e-01f, 1.01228536290376259e-01f}};
+
 // Carlson's symmetric integral R_F(x, y, z) = 1/2 int_0^inf dt / sqrt((t+x)(t+y)(t+z)),
 // x, y, z >= 0 with at most one zero.
-BHM_HD double carlson_rf(double x, double y, double z) {
+template <class T>
+BHM_HD T carlson_rf(T x, T y, T z) {
+  const T tol = sizeof(T) == 4 ? T(3e-2) : T(1e-3);  // series error ~ tol^6
   for (int it = 0; it < 60; ++it) {
-    const double sx = sqrt(x), sy = sqrt(y), sz = sqrt(z);
-    const double lam = sx * sy + sy * sz + sz * sx;
-    x = 0.25 * (x + lam);
-    y = 0.25 * (y + lam);
-    z = 0.25 * (z + lam);
-    const double A = (x + y + z) * (1.0 / 3.0);
-    const double dx = 1.0 - x / A, dy = 1.0 - y / A;
-    const double dz = -(dx + dy);
-    if (fmax(fabs(dx), fmax(fabs(dy), fabs(dz))) < 1e-3) {
-      const double e2 = dx * dy - dz * dz, e3 = dx * dy * dz;
-      return (1.0 - 0.1 * e2 + e3 * (1.0 / 14.0) + e2 * e2 * (1.0 / 24.0) - e2 * e3 * (3.0 / 44.0)) / sqrt(A);
+    const T sx = sqrt(x), sy = sqrt(y), sz = sqrt(z);
+    const T lam = sx * sy + sy * sz + sz * sx;
+    x = T(0.25) * (x + lam);
+    y = T(0.25) * (y + lam);
+    z = T(0.25) * (z + lam);
+    const T A = (x + y + z) * T(1.0 / 3.0);
+    const T dx = T(1) - x / A, dy = T(1) - y / A;
+    const T dz = -(dx + dy);
+    if (fmax(fabs(dx), fmax(fabs(dy), fabs(dz))) < tol) {
+      const T e2 = dx * dy - dz * dz, e3 = dx * dy * dz;
+      return (T(1) - T(0.1) * e2 + e3 * T(1.0 / 14.0) + e2 * e2 * T(1.0 / 24.0) - e2 * e3 * T(3.0 / 44.0)) *
+             inv_sqrt(A);
     }
   }
-  return NAN;
+  return T(NAN);
+}
+
+// int_0^{pi/2} dchi / sqrt(w + m sin^2 chi) = pi / (2 AGM(sqrt(w), sqrt(w + m)))
+// (Gauss's arithmetic-geometric mean; quadratic convergence).
+template <class T>
+BHM_HD T quarter_period(T w, T m) {
+  const T eps = sizeof(T) == 4 ? T(1e-7) : T(1e-15);
+  T a = sqrt(w + m), g = sqrt(w);
+  for (int it = 0; it < 12 && fabs(a - g) > eps * a; ++it) {
+    const T an = T(0.5) * (a + g);
+    g = sqrt(a * g);
+    a = an;
+  }
+  return T(1.5707963267948966) / (T(0.5) * (a + g));
 }
 
 struct ThetaMotion {
@@ -75,7 +132,9 @@ struct ThetaMotion {
   double period;  // 2K: Mino time between crossings
 };
 
-// u0 = cos theta_obs, pu0 = du/dtau at the observer.
+// u0 = cos theta_obs, pu0 = du/dtau at the observer. T: precision of the
+// elliptic integrals (the roots z+, w are formed in FP64).
+template <class T = double>
 BHM_HD ThetaMotion theta_motion(double a2, double qTh, double lam, double u0, double pu0) {
   ThetaMotion t{false, INFINITY, INFINITY};
   const double c0 = qTh - lam * lam;  // U(0)
@@ -87,12 +146,12 @@ BHM_HD ThetaMotion theta_motion(double a2, double qTh, double lam, double u0, do
   const double m = a2 * zp;
   double s = fabs(u0) / sqrt(zp);  // sin chi_obs
   s = fmin(s, 1.0);
-  const double phi_obs = s * carlson_rf(w * (1.0 - s * s), w + m * s * s, w);
-  const double K = carlson_rf(0.0, w + m, w);
+  const T phi_obs = T(s) * carlson_rf<T>(T(w * (1.0 - s * s)), T(w + m * s * s), T(w));
+  const T K = quarter_period<T>(T(w), T(m));
   const bool toward = (pu0 * u0) < 0.0;
   t.crosses = true;
-  t.tau1 = toward ? phi_obs : 2.0 * K - phi_obs;
-  t.period = 2.0 * K;
+  t.tau1 = toward ? (double)phi_obs : 2.0 * (double)K - (double)phi_obs;
+  t.period = 2.0 * (double)K;
   return t;
 }
 
@@ -130,31 +189,69 @@ BHM_HD double integrand(const Radial& q, double v) {
   if (q.kind == 1) {
     const double x = q.x_tp - v * v;
     const double pt = ((q.q3 * x + q.q2) * x + q.q1) * x + q.q0;
-    return 2.0 / sqrt(pt);
+    return 2.0 * inv_sqrt(pt);
   }
   const double x = v;
   const double x2 = x * x;
   const double P = 1.0 + x2 * (q.p2 + x * (q.p1 + x * q.p0));
-  return 1.0 / sqrt(P);
+  return inv_sqrt(P);
+}
+
+// The same integrand with the polynomial in FP64 (it nearly cancels next to
+// the critical curve) and the reciprocal square root in FP32.
+BHM_HD float integrand_f(const Radial& q, double v) {
+  if (q.kind == 1) {
+    const double x = q.x_tp - v * v;
+    const double pt = ((q.q3 * x + q.q2) * x + q.q1) * x + q.q0;
+    return 2.0f * inv_sqrt((float)pt);
+  }
+  const double x = v;
+  const double P = 1.0 + x * x * (q.p2 + x * (q.p1 + x * q.p0));
+  return inv_sqrt((float)P);
 }
 
 BHM_HD double radius_of(const Radial& q, double v) { return q.kind == 1 ? 1.0 / (q.x_tp - v * v) : 1.0 / v; }
 
-// int_{v0}^{v1} integrand, composite Gauss-Legendre-16 with panels <= hmax.
+// int_{v0}^{v1} integrand: composite Gauss-Legendre with panels no wider
+// than hmax, 16 points per panel (ORDER 16), or 8 points on intervals
+// shorter than hmax / 4 (the Newton increments near convergence). FAST
+// takes the reciprocal square root and the panel sums in FP32; nodes, the
+// polynomial and the sum over panels stay FP64.
+template <int ORDER = 16, bool FAST = false>
 BHM_HD double integrate(const Radial& q, double v0, double v1, double hmax) {
   const double len = v1 - v0;
   if (len == 0.0) return 0.0;
+  if ((ORDER == 8 || fabs(len) <= 0.25 * hmax) && fabs(len) <= hmax) {
+    const double c = v0 + 0.5 * len, hh = 0.5 * len;
+    if (FAST) {
+      float s = 0.0f;
+      for (int k = 0; k < 4; ++k)
+        s += kGl8f[k].w * (integrand_f(q, c - hh * kGl8[k].x) + integrand_f(q, c + hh * kGl8[k].x));
+      return (double)s * hh;
+    }
+    double s = 0.0;
+    for (int k = 0; k < 4; ++k)
+      s += kGl8[k].w * (integrand(q, c - hh * kGl8[k].x) + integrand(q, c + hh * kGl8[k].x));
+    return s * hh;
+  }
   int n = (int)ceil(fabs(len) / hmax);
   n = n < 1 ? 1 : (n > 64 ? 64 : n);
   const double h = len / n;
   double sum = 0.0;
   for (int p = 0; p < n; ++p) {
     const double c = v0 + (p + 0.5) * h, hh = 0.5 * h;
-    double s = 0.0;
-    for (int k = 0; k < 8; ++k) {
-      s += kGl16[k].w * (integrand(q, c - hh * kGl16[k].x) + integrand(q, c + hh * kGl16[k].x));
+    if (FAST) {
+      float s = 0.0f;
+      for (int k = 0; k < 8; ++k)
+        s += kGl16f[k].w *
+             (integrand_f(q, c - hh * kGl16[k].x) + integrand_f(q, c + hh * kGl16[k].x));
+      sum += (double)s * hh;
+    } else {
+      double s = 0.0;
+      for (int k = 0; k < 8; ++k)
+        s += kGl16[k].w * (integrand(q, c - hh * kGl16[k].x) + integrand(q, c + hh * kGl16[k].x));
+      sum += s * hh;
     }
-    sum += s * hh;
   }
   return sum;
 }
@@ -209,33 +306,55 @@ BHM_HD Radial radial_motion(double a2, double a2_alam, double C, double r_obs, d
   return q;
 }
 
-// Solve tau(v) = T for v in [lo, hi] with tau(lo) = tlo <= T <= tau(hi) = thi.
-BHM_HD bool solve_tau(const Radial& q, double T, double lo, double tlo, double hi, double thi, double seed,
-                      double hmax, double& v_out, double& t_out) {
-  double v = (seed > lo && seed < hi) ? seed : lo + (hi - lo) * ((T - tlo) / (thi - tlo));
-  if (!(v > lo && v < hi)) v = 0.5 * (lo + hi);
-  double tv = (v - lo < hi - v) ? tlo + integrate(q, lo, v, hmax) : thi - integrate(q, v, hi, hmax);
-  for (int it = 0; it < 60; ++it) {
-    if (tv < T) {
+// Solve tau(v) = T on [lo, hi] given tau(lo) = tlo <= T, where tau is
+// increasing: Newton steps safeguarded by bisection of the bracket, each new
+// tau(v) from the last by an increment of quadrature. Returns 1 with (v, tau)
+// when found, 0 when tau(hi) < T (the ray stops before reaching T), -1 if
+// the iteration did not settle. seed: a first guess inside (lo, hi), or NaN.
+template <int ORDER = 16, bool FAST = false>
+BHM_HD int solve_tau(const Radial& q, double T, double lo, double tlo, double hi, double seed, double hmax,
+                     double& v_out, double& t_out) {
+  double v = lo, tv = tlo;
+  if (seed > lo && seed < hi) {
+    v = seed;
+    tv = tlo + integrate<ORDER, FAST>(q, lo, seed, hmax);
+  }
+  bool end_known = false;  // tau(hi) evaluated once, when Newton first aims past the end of the ray
+  for (int it = 0; it < 80; ++it) {
+    if (tv <= T) {
       lo = v;
       tlo = tv;
     } else {
       hi = v;
-      thi = tv;
+      end_known = true;
     }
-    double vn = v + (T - tv) / integrand(q, v);
+    double vn = v + (T - tv) / (FAST ? (double)integrand_f(q, v) : integrand(q, v));
+    if (!(vn < hi) && !end_known) {
+      const double t_hi = tv + integrate<ORDER, FAST>(q, v, hi, hmax);
+      if (t_hi < T) {
+        v_out = hi;
+        t_out = t_hi;
+        return 0;
+      }
+      end_known = true;
+    }
     if (!(vn > lo && vn < hi)) vn = 0.5 * (lo + hi);
     const double step = vn - v;
-    const double tn = tv + integrate(q, v, vn, hmax);
+    tv += integrate<ORDER, FAST>(q, v, vn, hmax);
     v = vn;
-    tv = tn;
-    if (fabs(step) <= 1e-14 * fmax(1e-3, fabs(v)) || hi - lo <= 1e-15) {
+    if (fabs(step) <= 1e-14 * fmax(1e-3, fabs(v))) {
+      // FP32 panel sums leave ~1e-8 of noise in tau, which can pinch the bracket.
+      if (fabs(tv - T) <= (FAST ? 1e-6 : 1e-9) * fmax(1.0, T)) {
+        v_out = v;
+        t_out = tv;
+        return 1;
+      }
       v_out = v;
       t_out = tv;
-      return true;
+      return (tv < T) ? 0 : -1;  // pinned at the end of the ray: no crossing before it stops
     }
   }
-  return false;
+  return -1;
 }
 
 struct Crossings {
@@ -243,6 +362,8 @@ struct Crossings {
   int kind;        // radial kind (1 escapes, 0 falls in)
   int n_hits;      // disk hits found (<= max_hits)
   double r[3];     // their radii
+  double v_last;   // variable and Mino time of the last solved crossing (or the observer)
+  double t_last;
   double r_min;    // largest local minimum of R above r+ (0 if none) ...
   double R_min;    // ... and R there: near zero next to the critical curve
 };
@@ -252,25 +373,23 @@ struct Crossings {
 // q_Th (theta potential) and C = q_R + (lambda - a)^2 (radial potential),
 // u0 = cos theta_obs and pu0 = du/dtau at the observer. r_seed > 0 is a guess
 // of the first hit radius that starts the Newton iterations.
-BHM_HD Crossings crossings(double a, double lam, double qTh, double C, double r_obs, double r_plus, double r_hor,
-                           double r_esc, double r_in, double r_out, double u0, double pu0, double r_seed,
-                           int max_hits, double hmax) {
+template <int ORDER = 16, bool FAST = false>
+BHM_HD Crossings crossings(const Radial& q, double a2, double lam, double qTh, double r_in, double r_out,
+                           double u0, double pu0, double r_seed, int max_hits, double hmax) {
   Crossings c{};
   c.status = 0;
   c.n_hits = 0;
-  const double a2 = a * a;
-  const double a2_alam = a2 - a * lam;
-  const Radial q = radial_motion(a2, a2_alam, C, r_obs, r_plus, r_hor, r_esc);
   c.kind = q.kind;
   c.r_min = q.r_min;
   c.R_min = q.R_min;
+  c.v_last = q.v_obs;
+  c.t_last = 0.0;
   if (q.kind < 0) {
     c.status = -1;
     return c;
   }
-  const ThetaMotion th = theta_motion(a2, qTh, lam, u0, pu0);
+  const ThetaMotion th = FAST ? theta_motion<float>(a2, qTh, lam, u0, pu0) : theta_motion<double>(a2, qTh, lam, u0, pu0);
   if (!th.crosses) return c;
-  const double t_end = integrate(q, q.v_obs, q.v_end, hmax);
   double seed_v[2] = {NAN, NAN};
   if (r_seed > 0.0) {
     if (q.kind == 1) {
@@ -284,24 +403,27 @@ BHM_HD Crossings crossings(double a, double lam, double qTh, double C, double r_
   double lo = q.v_obs, tlo = 0.0;
   for (int n = 0; n < 64; ++n) {
     const double T = th.tau1 + n * th.period;
-    if (!(T < t_end)) break;
     double seed = NAN;
     if (seed_v[0] > lo && seed_v[0] < q.v_end)
       seed = seed_v[0];
     else if (seed_v[1] > lo && seed_v[1] < q.v_end)
       seed = seed_v[1];
     double v, tv;
-    if (!solve_tau(q, T, lo, tlo, q.v_end, t_end, seed, hmax, v, tv)) {
+    const int rc = solve_tau<ORDER, FAST>(q, T, lo, tlo, q.v_end, seed, hmax, v, tv);
+    if (rc < 0) {
       c.status = -2;
       return c;
     }
+    if (rc == 0) break;  // the ray stops before this crossing
     const double r = radius_of(q, v);
+    lo = v;
+    tlo = tv;
+    c.v_last = v;
+    c.t_last = tv;
     if (r >= r_in && r <= r_out) {
       c.r[c.n_hits++] = r;
       if (c.n_hits >= max_hits) break;
     }
-    lo = v;
-    tlo = tv;
   }
   return c;
 }
@@ -316,7 +438,7 @@ BHM_HD double u_at(double a2, double qTh, double lam, double u0, double pu0, dou
   const double zp = (b2 > 0.0) ? (b2 + sq) / (2.0 * a2) : 2.0 * c0 / (sq - b2);
   const double w = c0 / zp, m = a2 * zp, rz = sqrt(zp);
   const double s0 = fmax(-1.0, fmin(1.0, u0 / rz));
-  const double K = carlson_rf(0.0, w + m, w);
+  const double K = quarter_period<double>(w, m);
   const double phi_x = s0 * carlson_rf(w * (1.0 - s0 * s0), w + m * s0 * s0, w);  // odd in s0
   const double phi_start = (pu0 >= 0.0) ? phi_x : 2.0 * K - phi_x;
   double total = phi_start + tau;
@@ -341,8 +463,12 @@ BHM_HD double u_at(double a2, double qTh, double lam, double u0, double pu0, dou
   return sgn * rz * sin(chi);
 }
 
-// Mino time at which the tracer stops (escape or horizon radius).
-BHM_HD double tau_end(const Radial& q, double hmax) { return integrate(q, q.v_obs, q.v_end, hmax); }
+// Mino time at which the tracer stops (escape or horizon radius), from a
+// point (v, tau(v)) of the ray.
+template <int ORDER = 16, bool FAST = false>
+BHM_HD double tau_end(const Radial& q, double v, double tv, double hmax) {
+  return tv + integrate<ORDER, FAST>(q, v, q.v_end, hmax);
+}
 
 // First-order image-plane distance (M) from pixel (alpha, beta) to the
 // critical curve: |R(r_min)| over the (alpha, beta) gradient of R at fixed

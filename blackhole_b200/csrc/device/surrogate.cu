@@ -13,6 +13,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <mutex>
 
@@ -39,10 +40,21 @@ struct GemmCfg {
   static_assert(BN % 16 == 0 && BN >= 16 && BN <= 256, "UMMA N for M = 128");
 };
 
-__device__ __forceinline__ float silu(float y) { return __fdividef(y, 1.0f + __expf(fminf(-y, 80.0f))); }
+__device__ __forceinline__ float tanh_approx(float x) {
+  float r;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+// SiLU(y) = y sigmoid(y) with sigmoid(y) = (1 + tanh(y/2)) / 2: one MUFU
+// operation per element (training and inference use the same form).
+__device__ __forceinline__ float silu(float y) {
+  const float h = 0.5f * y;
+  return fmaf(h, tanh_approx(h), h);
+}
 
 __device__ __forceinline__ float silu_grad(float y) {
-  const float s = __fdividef(1.0f, 1.0f + __expf(fminf(-y, 80.0f)));
+  const float s = fmaf(0.5f, tanh_approx(0.5f * y), 0.5f);
   return s * (1.0f + y * (1.0f - s));
 }
 
@@ -274,33 +286,60 @@ __constant__ float c_freq[BHS_FOURIER] = {1.0f,
                      25.398416831491190f,
                      32.0f};
 
-__global__ void k_features(const float* __restrict__ in, int64_t n, __nv_bfloat16* __restrict__ F,
-              __nv_bfloat16* __restrict__ FT, int64_t ldt) {
-  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= n) return;
-  const float4 q = reinterpret_cast<const float4*>(in)[r];
-  const float al = q.x, be = q.y, spin = q.z, ct = q.w;
-  float x[4] = {al * (1.0f / 15.0f), be * (1.0f / 15.0f), 2.0f * spin - 1.0f, 2.0f * ct - 1.0f};
-  const float st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct));
-  const float lam = -al * st;
-  const float eta = be * be + (al * al - spin * spin) * ct * ct;
-  float f[BHS_FEATURES_USED];
-  f[0] = x[0];
-  f[1] = x[1];
-  f[2] = x[2];
-  f[3] = x[3];
-  f[4] = lam * (1.0f / 15.0f);
-  f[5] = eta * (1.0f / 225.0f);
+// Fourier features of one input x: (sin, cos)(pi 2^(k/3) x), k = 0..15,
+// interleaved. Frequencies k = 0, 1, 2 come from sincospif; every further
+// one doubles the angle of the one three below (sin 2t = 2 s c,
+// cos 2t = (c - s)(c + s)), which keeps the absolute error near 1e-6.
+__device__ __forceinline__ void fourier_pairs(float x, float (&v)[2 * BHS_FOURIER]) {
+#pragma unroll
+  for (int k = 0; k < 3; ++k) sincospif(c_freq[k] * x, &v[2 * k], &v[2 * k + 1]);
+#pragma unroll
+  for (int k = 3; k < BHS_FOURIER; ++k) {
+    const float sn = v[2 * (k - 3)], cs = v[2 * (k - 3) + 1];
+    v[2 * k] = 2.0f * sn * cs;
+    v[2 * k + 1] = (cs - sn) * (cs + sn);
+  }
+}
+
+// The network's scaled inputs: x = (alpha/15, beta/15, 2a - 1, 2 cos theta - 1)
+// and the constants of motion lambda/15, eta/225.
+__device__ __forceinline__ void scaled_inputs(float4 q, float (&x)[4], float& lam, float& eta) {
+  x[0] = q.x * (1.0f / 15.0f);
+  x[1] = q.y * (1.0f / 15.0f);
+  x[2] = 2.0f * q.z - 1.0f;
+  x[3] = 2.0f * q.w - 1.0f;
+  const float st = sqrtf(fmaxf(0.0f, 1.0f - q.w * q.w));
+  lam = -q.x * st * (1.0f / 15.0f);
+  eta = (q.y * q.y + (q.x * q.x - q.z * q.z) * q.w * q.w) * (1.0f / 225.0f);
+}
+
+// The network's input features of one ray: columns 32 d + 2k, 32 d + 2k + 1
+// = Fourier pair k of input d (d = 0..3), columns 128..133 = the scaled
+// inputs and constants of motion, 134..191 zero.
+__device__ __forceinline__ void ray_features(float4 q, float (&f)[BHS_FEATURES_USED]) {
+  float x[4], lam, eta;
+  scaled_inputs(q, x, lam, eta);
 #pragma unroll
   for (int d = 0; d < 4; ++d) {
+    float v[2 * BHS_FOURIER];
+    fourier_pairs(x[d], v);
 #pragma unroll
-    for (int k = 0; k < BHS_FOURIER; ++k) {
-      float s, c;
-      sincospif(c_freq[k] * x[d], &s, &c);
-      f[6 + d * 2 * BHS_FOURIER + 2 * k] = s;
-      f[6 + d * 2 * BHS_FOURIER + 2 * k + 1] = c;
-    }
+    for (int j = 0; j < 2 * BHS_FOURIER; ++j) f[2 * BHS_FOURIER * d + j] = v[j];
   }
+  f[128] = x[0];
+  f[129] = x[1];
+  f[130] = x[2];
+  f[131] = x[3];
+  f[132] = lam;
+  f[133] = eta;
+}
+
+__global__ void k_features(const float* __restrict__ in, int64_t n, __nv_bfloat16* __restrict__ F,
+                           __nv_bfloat16* __restrict__ FT, int64_t ldt) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  float f[BHS_FEATURES_USED];
+  ray_features(reinterpret_cast<const float4*>(in)[r], f);
   uint4* row = reinterpret_cast<uint4*>(F + r * BHS_FEATURES);
 #pragma unroll
   for (int u = 0; u < BHS_FEATURES / 8; ++u) {
@@ -379,6 +418,226 @@ __global__ void k_loss(const float* __restrict__ out, const float* __restrict__ 
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if ((threadIdx.x & 31) == 0 && v != 0.0f) atomicAdd(loss + c, v);
   }
+}
+
+// ---- fused inference -----------------------------------------------------------
+//
+// One persistent CTA per SM runs the whole network on pairs of 128-row tiles.
+// Warp 0 streams weight K-chunks by TMA through a 3-stage ring (each chunk
+// is loaded once per tile), warp 1 issues the tcgen05 MMAs, warps 2-5 and
+// 6-9 are the epilogues of tile slots 0 and 1. The activations of a slot
+// stay in shared memory, in the 128-byte-swizzled K-major layout the MMA
+// reads; its FP32 accumulator is one half of the CTA's 512 TMEM columns.
+// While one slot's epilogue (bias, SiLU, BF16, store to shared) runs, the
+// tensor core works on the other slot.
+
+constexpr int kInfThreads = 320;
+constexpr int kInfRing = 3;
+constexpr int kActChunk = kBM * kBK * 2;       // 16 KB: one 64-column chunk of a tile
+constexpr int kActBytes = 4 * kActChunk;        // 64 KB: 256 columns
+constexpr int kWChunk = BHS_HIDDEN * kBK * 2;   // 32 KB: [256 x 64] weights
+constexpr int kInfSmem = 2 * kActBytes + kInfRing * kWChunk + 1024 + 256;
+
+// Biases travel in kernel parameter space: every lane of a warp reads the
+// same column, so the loads are constant-bank broadcasts, not global loads.
+constexpr int kBiasCount = 4 * BHS_HIDDEN + BHS_HEAD;
+
+struct InferArgs {
+  const float* in;
+  float* out;
+  int64_t n;
+  int64_t pairs;
+  int* err;
+  float bias[kBiasCount];  // layers 0..3 (256 each), then the head (16)
+};
+
+__device__ __forceinline__ int layer_chunks(int l) { return (l == 0 ? BHS_FEATURES : BHS_HIDDEN) / kBK; }
+
+// One 16-byte unit (8 BF16, unit j of 8 in a 64-column chunk) of row r of a
+// K-major 128-byte-swizzled tile chunk at shared address cb.
+__device__ __forceinline__ void st_unit(uint32_t cb, int r, int j, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+  const uint32_t addr = cb + (uint32_t)r * 128u + ((uint32_t)(j ^ (r & 7)) << 4);
+  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(a), "r"(b), "r"(c), "r"(d) : "memory");
+}
+
+__global__ void __launch_bounds__(kInfThreads, 1)
+    k_mlp_infer(const __grid_constant__ CUtensorMap w0, const __grid_constant__ CUtensorMap w1,
+                const __grid_constant__ CUtensorMap w2, const __grid_constant__ CUtensorMap w3,
+                const __grid_constant__ CUtensorMap w4, InferArgs A) {
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = umma::smem_u32(smem_raw);
+  const uint32_t pad = (1024u - (raw & 1023u)) & 1023u;
+  const uint32_t act0 = raw + pad;
+  const uint32_t ring0 = act0 + 2u * kActBytes;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + pad + 2 * kActBytes + kInfRing * kWChunk);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kInfRing + 4);
+  const uint32_t b0 = umma::smem_u32(bars);
+  auto full = [&](int i) { return b0 + 8u * i; };
+  auto empty = [&](int i) { return b0 + 8u * (kInfRing + i); };
+  auto act_ready = [&](int s) { return b0 + 8u * (2 * kInfRing + s); };
+  auto acc_full = [&](int s) { return b0 + 8u * (2 * kInfRing + 2 + s); };
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kInfRing; ++i) {
+      umma::mbar_init(full(i), 1);
+      umma::mbar_init(empty(i), 1);
+    }
+    for (int s = 0; s < 2; ++s) {
+      umma::mbar_init(act_ready(s), 128);
+      umma::mbar_init(acc_full(s), 1);
+    }
+    umma::fence_mbar_init();
+    umma::tma_prefetch_desc(&w0);
+    umma::tma_prefetch_desc(&w1);
+    umma::tma_prefetch_desc(&w2);
+    umma::tma_prefetch_desc(&w3);
+    umma::tma_prefetch_desc(&w4);
+  }
+  if (warp == 0) {
+    umma::tmem_alloc(umma::smem_u32(tmem_slot), 512);
+    umma::tmem_relinquish();
+  }
+  umma::tc_fence_before();
+  __syncthreads();
+  umma::tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {  // weight producer
+      const CUtensorMap* maps[BHS_LAYERS] = {&w0, &w1, &w2, &w3, &w4};
+      uint32_t it = 0;
+      bool ok = true;
+      for (int64_t p = blockIdx.x; ok && p < A.pairs; p += gridDim.x)
+        for (int l = 0; ok && l < BHS_LAYERS; ++l) {
+          const uint32_t bytes = (uint32_t)((l == BHS_LAYERS - 1 ? BHS_HEAD : BHS_HIDDEN) * kBK * 2);
+          for (int s = 0; ok && s < 2; ++s)
+            for (int c = 0; c < layer_chunks(l); ++c, ++it) {
+              const int st = (int)(it % kInfRing);
+              if (it >= (uint32_t)kInfRing && !umma::mbar_wait(empty(st), ((it / kInfRing) - 1) & 1, kWaitNs)) {
+                atomicExch(A.err, kErrProducer);
+                ok = false;
+                break;
+              }
+              umma::mbar_arrive_expect_tx(full(st), bytes);
+              umma::tma_load_2d(ring0 + (uint32_t)st * kWChunk, maps[l], full(st), c * kBK, 0);
+            }
+        }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {  // MMA issuer
+      uint32_t it = 0, ph[2] = {0u, 0u};
+      bool ok = true;
+      for (int64_t p = blockIdx.x; ok && p < A.pairs; p += gridDim.x)
+        for (int l = 0; ok && l < BHS_LAYERS; ++l)
+          for (int s = 0; ok && s < 2; ++s) {
+            if (!umma::mbar_wait(act_ready(s), ph[s], kWaitNs)) {
+              atomicExch(A.err, kErrMma);
+              ok = false;
+              break;
+            }
+            ph[s] ^= 1u;
+            umma::tc_fence_after();
+            const uint32_t idesc = umma::idesc_bf16_f32(kBM, l == BHS_LAYERS - 1 ? BHS_HEAD : BHS_HIDDEN);
+            const uint32_t d = tmem + (uint32_t)s * 256u;
+            for (int c = 0; c < layer_chunks(l); ++c, ++it) {
+              const int st = (int)(it % kInfRing);
+              if (!umma::mbar_wait(full(st), (it / kInfRing) & 1, kWaitNs)) {
+                atomicExch(A.err, kErrMma);
+                ok = false;
+                break;
+              }
+              umma::tc_fence_after();
+              const uint64_t ad = umma::sw128_desc(act0 + (uint32_t)s * kActBytes + (uint32_t)c * kActChunk);
+              const uint64_t bd = umma::sw128_desc(ring0 + (uint32_t)st * kWChunk);
+#pragma unroll
+              for (int k = 0; k < kBK / 16; ++k)
+                umma::mma_bf16(d, ad + 2u * k, bd + 2u * k, idesc, (c > 0 || k > 0) ? 1u : 0u);
+              umma::mma_commit(empty(st));
+            }
+            umma::mma_commit(acc_full(s));
+          }
+    }
+  } else {  // epilogue of slot s, TMEM lane quarter q
+    const int s = (warp - 2) >> 2;
+    const int q = warp & 3;
+    const int r = q * 32 + lane;
+    const uint32_t act = act0 + (uint32_t)s * kActBytes;
+    const uint32_t tacc = tmem + (uint32_t)s * 256u + ((uint32_t)(q * 32) << 16);
+    uint32_t ph = 0;
+    for (int64_t p = blockIdx.x; p < A.pairs; p += gridDim.x) {
+      const int64_t row = (2 * p + s) * kBM + r;
+      const bool valid = row < A.n;
+      {
+        const float4 in = valid ? reinterpret_cast<const float4*>(A.in)[row] : make_float4(0.f, 0.f, 0.f, 0.5f);
+        float x[4], lam, eta;
+        scaled_inputs(in, x, lam, eta);
+        const float z = valid ? 1.0f : 0.0f;
+#pragma unroll 1
+        for (int d = 0; d < 4; ++d) {  // columns 32 d .. 32 d + 31: units 4 d .. 4 d + 3
+          float v[2 * BHS_FOURIER];
+          fourier_pairs(x[d], v);
+#pragma unroll
+          for (int uu = 0; uu < 4; ++uu) {
+            const int u = 4 * d + uu;
+            st_unit(act + (uint32_t)(u >> 3) * kActChunk, r, u & 7, pack_bf16(z * v[8 * uu], z * v[8 * uu + 1]),
+                    pack_bf16(z * v[8 * uu + 2], z * v[8 * uu + 3]), pack_bf16(z * v[8 * uu + 4], z * v[8 * uu + 5]),
+                    pack_bf16(z * v[8 * uu + 6], z * v[8 * uu + 7]));
+          }
+        }
+        // unit 16: columns 128..135 (scaled inputs, lambda, eta, two zeros); units 17..23: zero
+        st_unit(act + 2u * kActChunk, r, 0, pack_bf16(z * x[0], z * x[1]), pack_bf16(z * x[2], z * x[3]),
+                pack_bf16(z * lam, z * eta), 0u);
+#pragma unroll
+        for (int u = 17; u < BHS_FEATURES / 8; ++u) st_unit(act + 2u * kActChunk, r, u & 7, 0u, 0u, 0u, 0u);
+      }
+      umma::fence_async_smem();
+      umma::mbar_arrive(act_ready(s));
+      bool ok = true;
+      for (int l = 0; l < BHS_LAYERS - 1; ++l) {
+        ok = __all_sync(0xffffffffu, umma::mbar_wait(acc_full(s), ph, kWaitNs));
+        ph ^= 1u;
+        if (!ok) break;
+        umma::tc_fence_after();
+        const float* b = A.bias + l * BHS_HIDDEN;
+#pragma unroll 1
+        for (int j = 0; j < BHS_HIDDEN / 32; ++j) {
+          float v[32];
+          umma::tmem_ld32(tacc + 32u * j, v);
+          uint32_t pk[16];
+#pragma unroll
+          for (int i = 0; i < 16; ++i)
+            pk[i] = pack_bf16(silu(v[2 * i] + b[32 * j + 2 * i]), silu(v[2 * i + 1] + b[32 * j + 2 * i + 1]));
+          const uint32_t cb = act + (uint32_t)(j >> 1) * kActChunk;
+#pragma unroll
+          for (int uu = 0; uu < 4; ++uu)
+            st_unit(cb, r, (j & 1) * 4 + uu, pk[4 * uu], pk[4 * uu + 1], pk[4 * uu + 2], pk[4 * uu + 3]);
+        }
+        umma::fence_async_smem();
+        umma::tc_fence_before();
+        umma::mbar_arrive(act_ready(s));
+      }
+      if (ok) ok = __all_sync(0xffffffffu, umma::mbar_wait(acc_full(s), ph, kWaitNs));
+      ph ^= 1u;
+      if (!ok) {
+        if (lane == 0) atomicExch(A.err, kErrDone);
+        break;
+      }
+      umma::tc_fence_after();
+      float v[16];
+      tmem_ld16(tacc, v);
+      if (valid) {
+        const float* b = A.bias + 4 * BHS_HIDDEN;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) v[i] += b[i];
+        store_f32x16(A.out + row * BHS_HEAD, v);
+      }
+      umma::tc_fence_before();
+    }
+  }
+  umma::tc_fence_before();
+  __syncthreads();
+  if (warp == 0) umma::tmem_dealloc(tmem, 512);
 }
 
 // ---- gradients and optimiser -------------------------------------------------
@@ -613,6 +872,37 @@ int launch_bn(const BhsGemm* g, int* err, cudaStream_t st) {
 int blocks_for(int64_t n, int threads) { return (int)((n + threads - 1) / threads); }
 
 }  // namespace
+
+extern "C" int bhs_launch_infer(const __nv_bfloat16* const* wb, const float* host_bias, const float* inputs,
+                                int64_t n, float* head, int* d_err, cudaStream_t stream) {
+  if (n <= 0) return 0;
+  CUtensorMap m[BHS_LAYERS];
+  for (int l = 0; l < BHS_LAYERS; ++l)
+    if (!make_map(&m[l], wb[l], bhs_layer_n(l), bhs_layer_k(l), bhs_layer_k(l), bhs_layer_n(l))) {
+      std::fprintf(stderr, "blackhole_b200: tensor map encoding failed\n");
+      return -1;
+    }
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+      return -1;
+    if (cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kInfSmem) != cudaSuccess)
+      return -1;
+  }
+  InferArgs a{};
+  a.in = inputs;
+  a.out = head;
+  a.n = n;
+  const int64_t tiles = (n + kBM - 1) / kBM;
+  a.pairs = (tiles + 1) / 2;
+  for (int i = 0; i < kBiasCount; ++i) a.bias[i] = host_bias[i];
+  a.err = d_err;
+  const int grid = (int)std::min<int64_t>(sms, a.pairs);
+  k_mlp_infer<<<grid, kInfThreads, kInfSmem, stream>>>(m[0], m[1], m[2], m[3], m[4], a);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
 
 extern "C" int bhs_launch_gemm(const BhsGemm* g, int* d_err, cudaStream_t stream) {
   if (g->M <= 0) return 0;

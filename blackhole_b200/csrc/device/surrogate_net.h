@@ -3,8 +3,9 @@
 // ray's termination class, disk crossings, redshift and escape direction.
 //
 //   input   (alpha, beta, spin, cos theta_obs) -> 192 features (BF16):
-//           4 scaled inputs, lambda and eta (the ray's constants of motion),
-//           16 Fourier frequencies x 4 inputs x (sin, cos), zero padding
+//           16 Fourier frequencies x 4 inputs x (sin, cos) in columns 0..127,
+//           the 4 scaled inputs and lambda, eta (the ray's constants of
+//           motion) in 128..133, zero padding
 //   hidden  4 layers x 256, SiLU, BF16 weights, FP32 accumulation
 //   head    16 outputs (FP32): 3 class logits (captured, disk, escaped),
 //           ln r1 - 2, cos phi1, sin phi1, ln r2 - 2, cos phi2, sin phi2,
@@ -69,6 +70,13 @@ typedef struct BhsGemm {
 } BhsGemm;
 
 int bhs_launch_gemm(const BhsGemm* g, int* d_err, cudaStream_t stream);
+
+// Fused inference of n rows (features, 4 hidden layers, head) in one
+// persistent launch: head [n][16] = network(inputs [n][4]). host_bias: the
+// 4 x 256 hidden biases then the 16 head biases (host memory, copied into
+// the launch's parameters).
+int bhs_launch_infer(const __nv_bfloat16* const* wb, const float* host_bias, const float* inputs, int64_t n,
+                     float* head, int* d_err, cudaStream_t stream);
 
 // Features of n rays from inputs [n][4] = (alpha, beta, spin, cos theta_obs).
 int bhs_launch_features(const float* inputs, int64_t n, __nv_bfloat16* F, __nv_bfloat16* FT, int64_t ld_t,

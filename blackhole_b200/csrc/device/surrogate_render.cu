@@ -12,7 +12,8 @@
 //   4. the exact solve disagrees with the network's
 //      class                                          -> integrator
 // Accepted disk pixels get r_hit from the Mino-time solve seeded with the
-// network's radius, and g, flux and intensity from r_hit exactly as the
+// network's radius (FP32 reciprocal square roots in the quadrature by
+// default, all FP64 on request), and g, flux and intensity from r_hit exactly as the
 // tracer computes them; escaped pixels get theta_inf from the exact polar
 // motion at the escape radius; phi_hit and phi_inf are the network's.
 #include <cuda_runtime.h>
@@ -24,13 +25,14 @@
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr double kPanel = 0.125;  // Gauss-Legendre panel width of the Mino-time quadrature
+constexpr double kPanel = 0.125;  // Gauss-Legendre-16 panel width of the Mino-time quadrature
 
 __device__ __forceinline__ void warp_count(unsigned *stats, int slot, bool pred) {
   const unsigned m = __ballot_sync(kFull, pred);
   if ((threadIdx.x & 31u) == 0 && m) atomicAdd(stats + slot, (unsigned)__popc(m));
 }
 
+template <bool FAST>
 __global__ void __launch_bounds__(128) k_surrogate_refine(const __grid_constant__ BhkImageParams p,
                                                           const __grid_constant__ BhkImageOut o,
                                                           const float *__restrict__ head, float min_conf,
@@ -74,11 +76,13 @@ __global__ void __launch_bounds__(128) k_surrogate_refine(const __grid_constant_
         int nhit = 0;
         double rh[3] = {0.0, 0.0, 0.0};
         bool solved = true;
+        bhmino::Crossings c{};
+        c.v_last = q.v_obs;
+        c.t_last = 0.0;
         if (nn_cls == 1 || verify >= 2) {
           const double r_seed = exp((double)h[3] + 2.0);
-          const bhmino::Crossings c =
-              bhmino::crossings(a, lam, qTh, C, p.r_obs, p.r_plus, p.r_hor, p.r_esc, p.r_in, p.r_out, p.cos_o, pu0,
-                                r_seed, p.max_cross, kPanel);
+          c = bhmino::crossings<16, FAST>(q, p.a2, lam, qTh, p.r_in, p.r_out, p.cos_o, pu0, r_seed, p.max_cross,
+                                          kPanel);
           solved = c.status == 0;
           nhit = c.n_hits;
           for (int k = 0; k < 3; ++k) rh[k] = c.r[k];
@@ -96,7 +100,7 @@ __global__ void __launch_bounds__(128) k_surrogate_refine(const __grid_constant_
           if (cls == 2) {
             const bhmino::ThetaMotion tm = bhmino::theta_motion(p.a2, qTh, lam, p.cos_o, pu0);
             if (tm.crosses) {
-              const double te = bhmino::tau_end(q, kPanel);
+              const double te = bhmino::tau_end<16, FAST>(q, c.v_last, c.t_last, kPanel);
               const double u = bhmino::u_at(p.a2, qTh, lam, p.cos_o, pu0, te);
               th_inf = acos(fmin(1.0, fmax(-1.0, u)));
             } else {
@@ -144,11 +148,14 @@ __global__ void __launch_bounds__(128) k_surrogate_refine(const __grid_constant_
 }  // namespace
 
 extern "C" int bhk_surrogate_refine(const BhkImageParams *p, const BhkImageOut *o, const float *head, float min_conf,
-                                    double band, int verify, int *list, unsigned int *count, unsigned int *stats,
-                                    void *stream) {
+                                    double band, int verify, int refine_fp64, int *list, unsigned int *count,
+                                    unsigned int *stats, void *stream) {
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (p->n_pix <= 0) return 0;
   const long long blocks = (p->n_pix + 127) / 128;
-  k_surrogate_refine<<<(unsigned)blocks, 128, 0, s>>>(*p, *o, head, min_conf, band, verify, list, count, stats);
+  if (refine_fp64)
+    k_surrogate_refine<false><<<(unsigned)blocks, 128, 0, s>>>(*p, *o, head, min_conf, band, verify, list, count, stats);
+  else
+    k_surrogate_refine<true><<<(unsigned)blocks, 128, 0, s>>>(*p, *o, head, min_conf, band, verify, list, count, stats);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

@@ -39,9 +39,6 @@ struct BH_Surrogate {
   float *part[BHS_LAYERS] = {};
   float *loss = nullptr;
   int *err = nullptr;
-  // inference chunk buffers (grow-only)
-  int64_t inf_rows = 0;
-  bf16 *iF = nullptr, *iA = nullptr, *iB = nullptr;
   // renderer buffers (grow-only)
   int64_t ren_pixels = 0;
   float *r_inputs = nullptr, *r_head = nullptr;
@@ -49,12 +46,14 @@ struct BH_Surrogate {
   unsigned int *r_counts = nullptr;  // [0] list length, [1..5] stats
   unsigned long long *r_counter = nullptr;
   int64_t last_pixels = 0;
+  // host copy of the biases for the fused inference launch
+  std::vector<float> host_bias;
+  bool bias_stale = true;
 };
 
 namespace {
 
 constexpr int kDwChunks = 8;  // 64-row K chunks per split of the batch reduction
-constexpr int64_t kInferChunk = 131072;
 
 int fail_msg(const char *fmt, ...) __attribute__((format(printf, 1, 2)));
 int fail_msg(const char *fmt, ...) {
@@ -206,25 +205,6 @@ int forward_backward(BH_Surrogate *s, const float *inputs, const float *targets,
   return 0;
 }
 
-int grow_inference(BH_Surrogate *s, int64_t rows) {
-  if (rows <= s->inf_rows) return 0;
-  for (void *p : {static_cast<void *>(s->iF), static_cast<void *>(s->iA), static_cast<void *>(s->iB)}) {
-    if (!p) continue;
-    auto it = std::find(s->allocs.begin(), s->allocs.end(), p);
-    if (it != s->allocs.end()) s->allocs.erase(it);
-    cudaFree(p);
-  }
-  s->iF = s->iA = s->iB = nullptr;
-  s->inf_rows = 0;
-  if (int rc = alloc(s, &s->iF, static_cast<size_t>(rows) * BHS_FEATURES, "cudaMalloc(inference features)")) return rc;
-  if (int rc = alloc(s, &s->iA, static_cast<size_t>(rows) * BHS_HIDDEN, "cudaMalloc(inference activations)"))
-    return rc;
-  if (int rc = alloc(s, &s->iB, static_cast<size_t>(rows) * BHS_HIDDEN, "cudaMalloc(inference activations)"))
-    return rc;
-  s->inf_rows = rows;
-  return 0;
-}
-
 }  // namespace
 
 extern "C" {
@@ -310,6 +290,7 @@ int bh_surrogate_set_params(BH_Surrogate *s, const float *host, int64_t n) {
                           "cudaMemcpy(params)"))
     return rc;
   if (int rc = refresh(s, nullptr)) return rc;
+  s->bias_stale = true;
   s->step = 0;
   if (int rc = cuda_check(cudaMemset(s->m, 0, static_cast<size_t>(n) * sizeof(float)), "cudaMemset")) return rc;
   if (int rc = cuda_check(cudaMemset(s->v, 0, static_cast<size_t>(n) * sizeof(float)), "cudaMemset")) return rc;
@@ -326,28 +307,17 @@ int bh_surrogate_features(const float *inputs, int64_t n, void *features, void *
 int bh_surrogate_forward(BH_Surrogate *s, const float *inputs, int64_t n, float *head, void *stream) {
   if (!s || n < 0 || (n > 0 && (!inputs || !head))) return fail_msg("surrogate: bad forward arguments");
   if (n == 0) return 0;
-  const int64_t chunk = std::min<int64_t>(n, kInferChunk);
-  if (int rc = grow_inference(s, chunk)) return rc;
-  auto st = static_cast<cudaStream_t>(stream);
-  for (int64_t r0 = 0; r0 < n; r0 += chunk) {
-    const int64_t rows = std::min(chunk, n - r0);
-    if (bhs_launch_features(inputs + 4 * r0, rows, s->iF, nullptr, 0, st))
-      return fail_msg("surrogate: feature launch failed");
-    const bf16 *X = s->iF;
-    bf16 *bufs[2] = {s->iA, s->iB};
-    for (int l = 0; l < 4; ++l) {
-      const int K = bhs_layer_k(l);
-      BhsGemm g = make_gemm(X, K, s->wb[l], K, rows, BHS_HIDDEN, K, BHS_EPI_HIDDEN);
-      g.bias = s->w + bhs_bias_offset(l);
-      g.out = bufs[l & 1];
-      if (int rc = gemm(s, g, st, "inference")) return rc;
-      X = bufs[l & 1];
-    }
-    BhsGemm g = make_gemm(X, BHS_HIDDEN, s->wb[4], BHS_HIDDEN, rows, BHS_HEAD, BHS_HIDDEN, BHS_EPI_HEAD);
-    g.bias = s->w + bhs_bias_offset(4);
-    g.out = head + BHS_HEAD * r0;
-    if (int rc = gemm(s, g, st, "inference head")) return rc;
+  if (s->bias_stale) {  // after training steps: fetch the biases once (synchronous)
+    s->host_bias.resize(4 * BHS_HIDDEN + BHS_HEAD);
+    for (int l = 0; l < BHS_LAYERS; ++l)
+      if (int rc = cuda_check(cudaMemcpy(s->host_bias.data() + l * BHS_HIDDEN, s->w + bhs_bias_offset(l),
+                                         static_cast<size_t>(bhs_layer_n(l)) * sizeof(float), cudaMemcpyDeviceToHost),
+                              "cudaMemcpy(biases)"))
+        return rc;
+    s->bias_stale = false;
   }
+  if (bhs_launch_infer(s->wb, s->host_bias.data(), inputs, n, head, s->err, static_cast<cudaStream_t>(stream)) != 0)
+    return fail_msg("surrogate: fused inference launch failed");
   return 0;
 }
 
@@ -376,6 +346,7 @@ int bh_surrogate_train_step(BH_Surrogate *s, const float *inputs, const float *t
   if (bhs_launch_adam(s->w, s->grad, s->m, s->v, s->n_params, lr_t, adam->beta1, adam->beta2, adam->eps, s->wb, s->wt,
                       st) != 0)
     return fail_msg("surrogate: Adam launch failed");
+  s->bias_stale = true;
   return 0;
 }
 
@@ -420,6 +391,8 @@ void bh_surrogate_policy_defaults(BH_SurrogatePolicy *p) {
   p->min_confidence = 0.99f;
   p->verify = 1;
   p->critical_band = 0.05;
+  p->refine_fp64 = 0;
+  p->reserved = 0;
 }
 
 int bh_surrogate_trace_image(BH_Surrogate *s, const BH_KerrScene *scene, const BH_KerrImageOut *out,
@@ -468,8 +441,8 @@ int bh_surrogate_trace_image(BH_Surrogate *s, const BH_KerrScene *scene, const B
     return rc;
   const BhkImageOut o{out->cls,   out->steps,     out->n_cross,   out->r_hit,     out->phi_hit,
                       out->g,     out->flux,      out->intensity, out->theta_inf, out->phi_inf};
-  if (bhk_surrogate_refine(&p, &o, s->r_head, pol.min_confidence, pol.critical_band, pol.verify, s->r_list,
-                           s->r_counts, s->r_counts + 1, stream))
+  if (bhk_surrogate_refine(&p, &o, s->r_head, pol.min_confidence, pol.critical_band, pol.verify, pol.refine_fp64,
+                           s->r_list, s->r_counts, s->r_counts + 1, stream))
     return fail_msg("surrogate render: refine launch failed");
   if (bhk_trace_list_mixed(&p, &o, s->r_list, s->r_counts, s->r_counter, L, stream))
     return fail_msg("surrogate render: fallback tracer launch failed");

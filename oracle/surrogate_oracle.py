@@ -31,7 +31,9 @@ def bf16(x) -> np.ndarray:
 
 
 def features(inputs: np.ndarray) -> np.ndarray:
-    """[n][192] float64 features (before BF16 rounding) of [n][4] inputs."""
+    """[n][192] float64 features (before BF16 rounding) of [n][4] inputs:
+    columns 32 d + 2 k, 32 d + 2 k + 1 = (sin, cos)(pi 2^(k/3) x_d), columns
+    128..133 = the scaled inputs and lambda / 15, eta / 225, the rest zero."""
     x = np.asarray(inputs, np.float64)
     al, be, a, ct = x[:, 0], x[:, 1], x[:, 2], x[:, 3]
     xs = np.stack([al / 15.0, be / 15.0, 2.0 * a - 1.0, 2.0 * ct - 1.0], 1)
@@ -39,14 +41,14 @@ def features(inputs: np.ndarray) -> np.ndarray:
     lam = -al * st
     eta = be * be + (al * al - a * a) * ct * ct
     F = np.zeros((x.shape[0], 192))
-    F[:, 0:4] = xs
-    F[:, 4] = lam / 15.0
-    F[:, 5] = eta / 225.0
     for d in range(4):
         for k in range(16):
             arg = np.pi * FREQ[k].astype(np.float64) * xs[:, d]
-            F[:, 6 + d * 32 + 2 * k] = np.sin(arg)
-            F[:, 6 + d * 32 + 2 * k + 1] = np.cos(arg)
+            F[:, 32 * d + 2 * k] = np.sin(arg)
+            F[:, 32 * d + 2 * k + 1] = np.cos(arg)
+    F[:, 128:132] = xs
+    F[:, 132] = lam / 15.0
+    F[:, 133] = eta / 225.0
     return F
 
 

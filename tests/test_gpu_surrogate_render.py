@@ -50,13 +50,15 @@ def test_untrained_network_falls_back_everywhere(cuda):
         np.testing.assert_array_equal(got[k], ref[k], err_msg=k)
 
 
+@pytest.mark.parametrize("fp64", [True, False])
 @pytest.mark.parametrize("spin,incl,form", [(0.9, 60, 0), (0.998, 85, 0), (0.3, 17, 1)])
-def test_exact_solve_matches_oracle(cuda, oracle, spin, incl, form):
+def test_exact_solve_matches_oracle(cuda, oracle, spin, incl, form, fp64):
     from blackhole_b200 import surrogate as S
 
     net = S.Surrogate(max_batch=128, seed=4)
     s = c4_scene(80, spin=spin, theta_obs=math.radians(incl), potential_form=form, precision=1)
-    got = host(net.trace_image(s, min_confidence=0.0, verify=2, critical_band=0.05))
+    got = host(net.trace_image(s, min_confidence=0.0, verify=2, critical_band=0.05, refine_fp64=fp64))
+    tol = 1e-6 if fp64 else 1e-5
     st = net.last_stats()
     assert st["accepted"] > 0 and st["solve_failed"] < 0.01 * st["pixels"]
     so = c4_scene(80, spin=spin, theta_obs=math.radians(incl), potential_form=form, precision=0)
@@ -66,9 +68,10 @@ def test_exact_solve_matches_oracle(cuda, oracle, spin, incl, form):
     assert np.mean(got["cls"] == ref["cls"]) >= 0.999
     d = acc & (ref["n_cross"] > 0)
     assert d.any()
-    np.testing.assert_allclose(got["r_hit"][0][d], ref["r_hit"][0][d], rtol=1e-6)
-    np.testing.assert_allclose(got["g"][0][d], ref["g"][0][d], rtol=1e-6)
-    np.testing.assert_allclose(got["flux"][d], ref["flux"][d], rtol=1e-5, atol=1e-12)
+    np.testing.assert_allclose(got["r_hit"][0][d], ref["r_hit"][0][d], rtol=tol)
+    np.testing.assert_allclose(got["g"][0][d], ref["g"][0][d], rtol=tol)
+    # NT flux ~ (1 - sqrt(r_isco / r)) / r^3 amplifies a radius error next to the ISCO
+    np.testing.assert_allclose(got["flux"][d], ref["flux"][d], rtol=10 * tol, atol=1e-6)
     esc = acc & (ref["cls"] == 2)
     assert np.abs(got["theta_inf"][esc] - ref["theta_inf"][esc]).max() < 2e-3
 

@@ -47,7 +47,8 @@ def test_features_shape_and_padding():
     F = so.features(x)
     assert F.shape == (50, 192)
     assert np.all(F[:, 134:] == 0.0)
-    np.testing.assert_allclose(F[:, 6] ** 2 + F[:, 7] ** 2, 1.0, rtol=1e-12)
+    np.testing.assert_allclose(F[:, 0] ** 2 + F[:, 1] ** 2, 1.0, rtol=1e-12)
+    np.testing.assert_allclose(F[:, 128], x[:, 0] / 15.0)
 
 
 def test_oracle_backward_matches_finite_differences():
