@@ -1,10 +1,18 @@
 """Benchmark: Kerr rays/s on one B200 (or N independent replicas).
 
-Workload (default ``disk16``): the adaptive Dormand-Prince disk scene, 16
-frames of 1024x1024 pixels, spin a in {0, 0.5, 0.9, 0.998} crossed with
-inclination in {17, 45, 75, 85} deg, observer at r = 1000 M, image plane
-alpha, beta in [-12, 12] M, rtol 1e-8, atol 1e-10, up to 3 crossings of a
-transparent thin disk r_isco..30 M. One step = one render of all 16 frames.
+Default workload ``c4_2048``: the a = 0.9 thin-disk scene (observer at
+r = 1000 M, 60 deg, alpha, beta in [-12, 12] M, opaque disk r_isco..30 M)
+at 2048 x 2048 pixels rendered by mixed precision plus the learned
+surrogate (bh_surrogate_trace_image: network inference on every pixel,
+exact Mino-time refinement, the mixed DP45 integrator on rejected pixels),
+beside the plain FP64 integrators on the same scene: FP64 DP45 (rtol 1e-8)
+at 2048^2 and FP64 RK4 with h = 0.02 min(r, 20) (the plain method of the
+256^2 scene) timed on its 256^2 frame. One step = one render of the frame.
+
+Other workloads (``--workload``): ``disk16`` (16 frames of 1024^2, spins
+{0, 0.5, 0.9, 0.998} x inclinations {17, 45, 75, 85} deg, DP45, 3 crossings,
+one persistent launch), ``batch4096`` (4096 uneven frames in one launch),
+single frames ``c0_256``, ``disk1_512``, ``disk1_1024``, ``disk_2048``.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -51,7 +59,11 @@ WORKLOADS = {
     "disk1_1024": dict(width=1024, height=1024, integrator=1, max_crossings=3, frames=[(0.9, 45.0)]),
     "disk_2048": dict(width=2048, height=2048, integrator=0, max_crossings=1, frames=[(0.9, 60.0)]),
     "batch4096": dict(integrator=1, max_crossings=1, generator=lambda: batch_frames()),
+    "c4_2048": dict(width=2048, height=2048, integrator=1, max_crossings=1, frames=[(0.9, 60.0)], surrogate=True),
 }
+SURROGATE_WEIGHTS = ROOT / "blackhole_b200" / "data" / "surrogate_c4.npz"
+# MACs per ray of the network (192x256 + 3 x 256x256 + 256x16), 2 FLOPs each.
+SURROGATE_FLOPS_PER_RAY = 2.0 * (192 * 256 + 3 * 256 * 256 + 256 * 16)
 OUT_FIELDS_USED = ("cls", "steps", "n_cross", "r_hit", "phi_hit", "g", "intensity", "theta_inf", "phi_inf")
 
 
@@ -311,6 +323,149 @@ def run_ours(args, rank: int, world: int, dist):
                 launches=len(runs) * args.steps, extra=extra)
 
 
+
+def _timed_launches(fn, stream, steps: int, warmup: int):
+    """CUDA-event times (ms) of ``steps`` calls of fn on ``stream`` after ``warmup``."""
+    import torch
+
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    out = []
+    for _ in range(steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        out.append((a, b))
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in out]
+
+
+def run_surrogate(args, rank: int, world: int, dist):
+    """The learned-surrogate workload: one step = one bh_surrogate_trace_image
+    render of the 2048^2 a = 0.9 disk frame."""
+    import torch
+
+    from blackhole_b200 import _abi, kerr
+    from blackhole_b200 import surrogate as S
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    lib = _abi.load_library()
+    if not SURROGATE_WEIGHTS.exists():
+        raise RuntimeError(f"{SURROGATE_WEIGHTS} missing: python -m blackhole_b200.train_surrogate")
+    net = S.Surrogate(max_batch=128)
+    net.load(SURROGATE_WEIGHTS)
+    stream = torch.cuda.Stream(device=dev)
+    smx = scenes_for(args.workload, 1)[0]
+    s64 = scenes_for(args.workload, 0)[0]
+    n = smx.width * smx.height
+    outs = kerr.alloc_image_outputs(smx, device=dev, fields=list(OUT_FIELDS_USED))
+
+    def render():
+        net.trace_image(smx, outs, stream=stream)
+
+    sampler = ClockSampler(dev.index if "CUDA_VISIBLE_DEVICES" not in os.environ else 0)
+    sampler.start()
+    sampler.wait_first_sample()
+    for _ in range(args.warmup):
+        render()
+    torch.cuda.synchronize(dev)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    sampler.lines.clear()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    steps_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    t0.record(stream)
+    for a, b in steps_ev:
+        a.record(stream)
+        render()
+        b.record(stream)
+    t1.record(stream)
+    torch.cuda.synchronize(dev)
+    clocks = sampler.stop()
+    if dist is not None:
+        dist.barrier()
+    elapsed_ms = t0.elapsed_time(t1)
+    if dist is not None:
+        t = torch.tensor([elapsed_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    render_ms = [a.elapsed_time(b) for a, b in steps_ev]
+    stats = net.last_stats()
+    value = n * args.steps * world / (elapsed_ms * 1e-3)
+
+    # ---- the plain integrators on the same scene (same run, same box) ----
+    o64 = kerr.alloc_image_outputs(s64, device=dev, fields=list(OUT_FIELDS_USED))
+    omx = kerr.alloc_image_outputs(smx, device=dev, fields=list(OUT_FIELDS_USED))
+    ms64 = _timed_launches(lambda: kerr.trace_image(s64, o64, stream=stream), stream, 2, 1)
+    msmx = _timed_launches(lambda: kerr.trace_image(smx, omx, stream=stream), stream, 2, 1)
+    from blackhole_b200._abi import default_scene
+
+    c0 = default_scene(width=256, height=256, spin=0.9, theta_obs=math.radians(60.0), integrator=0,
+                       max_crossings=1, precision=0)
+    oc0 = kerr.alloc_image_outputs(c0, device=dev, fields=["cls", "steps"])
+    msc0 = _timed_launches(lambda: kerr.trace_image(c0, oc0, stream=stream), stream, 2, 1)
+    fp64_dp45 = n / (statistics.mean(ms64) * 1e-3)
+    fp64_rk4 = 256 * 256 / (statistics.mean(msc0) * 1e-3)
+    extra = {
+        "fp64_plain": {"value": fp64_dp45, "unit": UNIT, "ms_per_step": statistics.mean(ms64),
+                       "method": "FP64 DP45 rtol 1e-8 on the same 2048^2 frame",
+                       "steps_per_ray": float(o64["steps"].double().mean().item())},
+        "fp64_plain_rk4": {"value": fp64_rk4, "unit": UNIT, "ms_per_step": statistics.mean(msc0),
+                           "method": "FP64 RK4 h = 0.02 min(r, 20), the plain method of the 256^2 frame of this "
+                                     "scene (rays/s measured on that frame)",
+                           "steps_per_ray": float(oc0["steps"].double().mean().item())},
+        "mixed_integrator": {"value": n / (statistics.mean(msmx) * 1e-3), "unit": UNIT,
+                             "ms_per_step": statistics.mean(msmx), "method": "mixed-precision DP45, every pixel"},
+        "speedup_vs_fp64_plain": value / fp64_dp45,
+        "speedup_vs_fp64_rk4": value / fp64_rk4,
+        "surrogate_stats": stats,
+        "accuracy_vs_fp64": accuracy([o64], [outs]),
+        "render_ms": {"mean": statistics.mean(render_ms), "min": min(render_ms), "max": max(render_ms)},
+    }
+    # ---- network inference alone: the tensor-core kernel's roofline ----
+    inp = S.grid_inputs(smx, device=dev, stream=stream)
+    head = torch.empty(n, 16, dtype=torch.float32, device=dev)
+    fwd_ms = _timed_launches(lambda: net.forward(inp, head, stream=stream), stream, 5, 2)
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = peaks.get("bf16_tflops")
+    achieved = SURROGATE_FLOPS_PER_RAY * n / (statistics.mean(fwd_ms) * 1e-3) / 1e12
+    roofline = {"bound": "tensor", "achieved": achieved, "peak": peak or 1590.0, "unit": "TFLOP/s",
+                "frac": achieved / (peak or 1590.0), "traffic": None,
+                "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst, of measured)" if peak else "fallback 1.59 PF",
+                "kernel": "k_mlp_infer", "flops_per_ray": SURROGATE_FLOPS_PER_RAY, "rays_per_launch": n,
+                "launch_ms_mean": statistics.mean(fwd_ms),
+                "note": "network inference timed alone on the frame's inputs; a render also runs the refinement "
+                        "kernel (FP64 set-up, FP32 quadrature) concurrently and the integrator on rejected pixels"}
+    extra["stage_ms"] = {"network_inference": statistics.mean(fwd_ms),
+                         "render_total": statistics.mean(render_ms)}
+
+    # ---- end to end through the host-buffer C entry point (pinned host memory) ----
+    e2e = None
+    if rank == 0:
+        fields = ("cls", "n_cross", "r_hit", "g", "flux", "intensity")
+        pinned = {f: torch.empty(n, dtype=torch.int32 if f in _abi.INT_FIELDS else torch.float64).pin_memory()
+                  for f in fields}
+        o = _abi.KerrImageOut()
+        for f, t in pinned.items():
+            setattr(o, f, t.data_ptr())
+        pol = _abi.SurrogatePolicy(0.99, 1, 0.05, 0, 0)
+        _abi.check(lib.bh_surrogate_trace_image_host(net._h, C.byref(smx), C.byref(o), C.byref(pol)))
+        k = max(1, min(args.steps, 3))
+        w0 = time.perf_counter()
+        for _ in range(k):
+            _abi.check(lib.bh_surrogate_trace_image_host(net._h, C.byref(smx), C.byref(o), C.byref(pol)))
+        w1 = time.perf_counter()
+        e2e = {"value": n * k / (w1 - w0), "unit": UNIT, "h2d_bytes_per_step": C.sizeof(_abi.KerrScene),
+               "d2h_bytes_per_step": sum(t.numel() * t.element_size() for t in pinned.values()),
+               "api": "bh_surrogate_trace_image_host", "fields": list(fields)}
+    launches = (1 + 2 * 8 + 1) * args.steps  # inputs, 8 x (inference, refinement), fallback tracer
+    return dict(value=value, ms_per_step=elapsed_ms / args.steps, e2e=e2e, roofline=roofline, clocks=clocks,
+                total_steps=int(outs["steps"].sum().item()), rays_per_step=n, launches=launches, extra=extra)
+
 # ---------------------------------------------------------------------------
 # reference arm: the reference's compiled CPU code on the host cores
 # ---------------------------------------------------------------------------
@@ -344,7 +499,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--workload", choices=tuple(WORKLOADS), default="disk16")
+    ap.add_argument("--workload", choices=tuple(WORKLOADS), default="c4_2048")
     ap.add_argument("--precision", choices=("fp64", "mixed"), default="mixed")
     ap.add_argument("--compare", action=argparse.BooleanOptionalAction, default=True,
                     help="also time the FP64 plain path and report the accuracy against it")
@@ -367,6 +522,13 @@ def main():
                   "max_crossings": wl["max_crossings"], "r_obs": 1000.0, "image_plane_M": [-12, 12]}
     config.update({"parallelism": f"replicas{world}", "launch": "one persistent launch per step (CUDA graph)",
                    "l2": "no inputs; outputs written once per step, larger than L2"})
+    if wl.get("surrogate"):
+        config.update({"spin": 0.9, "theta_obs_deg": 60.0, "method": "mixed precision + learned surrogate",
+                       "network": "192 features -> 4 x 256 SiLU -> 16, BF16 weights, FP32 accumulation",
+                       "weights": "blackhole_b200/data/surrogate_c4.npz (trained on 2^26 integrator rays)",
+                       "policy": {"min_confidence": 0.99, "critical_band_M": 0.05, "verify": "radial kind"},
+                       "launch": "18 launches per render on two streams (inference || refinement)",
+                       "l2": "outputs (4 Mi pixels x 9 fields) written once per step, larger than L2"})
 
     if args.impl == "reference":
         if rank != 0:
@@ -386,12 +548,13 @@ def main():
 
         dist_mod.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
         dist = dist_mod
-    res = run_ours(args, rank, world, dist)
+    res = run_surrogate(args, rank, world, dist) if wl.get("surrogate") else run_ours(args, rank, world, dist)
     if rank == 0:
         cb = cpu_reference(args.workload, args.cpu_budget) if (world == 1 and args.cpu_budget > 0) else None
         line = {"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "bf16+f32+f64" if wl.get("surrogate") else ("f64" if args.precision == "fp64" else "f32+f64"),
                 "data": "synthetic", "config": config, "precision": args.precision,
                 "steps_per_s": res["total_steps"] * args.steps * world / (res["ms_per_step"] * args.steps * 1e-3),
                 **res["extra"],

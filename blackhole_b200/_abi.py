@@ -261,6 +261,9 @@ def _declare(lib: C.CDLL) -> None:
     lib.bh_surrogate_trace_image.restype = C.c_int
     lib.bh_surrogate_trace_image.argtypes = [vp, C.POINTER(KerrScene), C.POINTER(KerrImageOut),
                                              C.POINTER(SurrogatePolicy), vp]
+    lib.bh_surrogate_trace_image_host.restype = C.c_int
+    lib.bh_surrogate_trace_image_host.argtypes = [vp, C.POINTER(KerrScene), C.POINTER(KerrImageOut),
+                                                  C.POINTER(SurrogatePolicy)]
     lib.bh_surrogate_last_stats.restype = C.c_int
     lib.bh_surrogate_last_stats.argtypes = [vp, C.POINTER(SurrogateStats)]
     lib.bh_bf16_gemm.restype = C.c_int

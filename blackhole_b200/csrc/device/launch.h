@@ -90,12 +90,12 @@ int bhk_trace_list_mixed(const BhkImageParams *p, const BhkImageOut *o, const in
                          unsigned long long *work_counter, BhkLaunch L, void *stream);
 
 // Surrogate renderer (surrogate_render.cu): per-pixel acceptance of the
-// network's head outputs [n_pix][16], exact refinement of accepted disk hits,
-// and the list of pixels left to the integrator. stats[5] += pixels accepted,
+// network's head outputs [n_pix][16] for pixels [p0, p1), exact refinement of
+// accepted disk hits, and the list of pixels left to the integrator. stats[5] += pixels accepted,
 // low confidence, critical band, solve failed, disagreement.
 int bhk_surrogate_refine(const BhkImageParams *p, const BhkImageOut *o, const float *head, float min_conf,
-                         double band, int verify, int refine_fp64, int *list, unsigned int *count,
-                         unsigned int *stats, void *stream);
+                         double band, int verify, int refine_fp64, long long p0, long long p1, int *list,
+                         unsigned int *count, unsigned int *stats, void *stream);
 
 // Reference stepper kernels (src/physics/kerr.cpp semantics), FP64.
 typedef struct BhkStateSoA { double *r, *theta, *phi, *t, *sr, *sth; } BhkStateSoA;

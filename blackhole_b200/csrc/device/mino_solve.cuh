@@ -173,16 +173,26 @@ BHM_HD double poly_R(const Radial& q, double r) {
 
 // Largest real root of R'(r) / 4 = r^3 + (p2/2) r + p1/4.
 BHM_HD double largest_dR_root(double p2, double p1) {
+  // FP32 closed form (trigonometric or Cardano), then two FP64 Newton steps.
   const double p = 0.5 * p2, qq = 0.25 * p1;
   const double disc = qq * qq * 0.25 + p * p * p * (1.0 / 27.0);
+  float t;
   if (disc < 0.0) {  // three real roots (p < 0)
-    const double rr = sqrt(-p * (1.0 / 3.0));
-    double c = (-0.5 * qq) / (rr * rr * rr);
-    c = fmax(-1.0, fmin(1.0, c));
-    return 2.0 * rr * cos(acos(c) * (1.0 / 3.0));
+    const float rr = sqrtf((float)(-p * (1.0 / 3.0)));
+    float c = (float)(-0.5 * qq) / (rr * rr * rr);
+    c = fmaxf(-1.0f, fminf(1.0f, c));
+    t = 2.0f * rr * cosf(acosf(c) * (1.0f / 3.0f));
+  } else {
+    const float sd = sqrtf((float)disc);
+    t = cbrtf((float)(-0.5 * qq) + sd) + cbrtf((float)(-0.5 * qq) - sd);
   }
-  const double sd = sqrt(disc);
-  return cbrt(-0.5 * qq + sd) + cbrt(-0.5 * qq - sd);
+  double r = (double)t;
+  for (int it = 0; it < 2; ++it) {
+    const double g = (r * r + p) * r + qq;
+    const double dg = 3.0 * r * r + p;
+    if (dg != 0.0) r -= g / dg;
+  }
+  return r;
 }
 
 BHM_HD double integrand(const Radial& q, double v) {

@@ -38,9 +38,10 @@ __global__ void __launch_bounds__(128) k_surrogate_refine(const __grid_constant_
                                                           const float *__restrict__ head, float min_conf,
                                                           double band, int verify, int *__restrict__ list,
                                                           unsigned int *__restrict__ count,
-                                                          unsigned int *__restrict__ stats) {
-  const long long pix = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool live = pix < p.n_pix;
+                                                          unsigned int *__restrict__ stats, long long p0,
+                                                          long long p1) {
+  const long long pix = p0 + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = pix < p1;
   int reason = 0;  // 0 accepted, 1 confidence, 2 critical band, 3 solve, 4 disagreement
   if (live) {
     const long long i = pix % p.width, j = pix / p.width;
@@ -80,7 +81,7 @@ __global__ void __launch_bounds__(128) k_surrogate_refine(const __grid_constant_
         c.v_last = q.v_obs;
         c.t_last = 0.0;
         if (nn_cls == 1 || verify >= 2) {
-          const double r_seed = exp((double)h[3] + 2.0);
+          const double r_seed = (double)__expf(h[3] + 2.0f);
           c = bhmino::crossings<16, FAST>(q, p.a2, lam, qTh, p.r_in, p.r_out, p.cos_o, pu0, r_seed, p.max_cross,
                                           kPanel);
           solved = c.status == 0;
@@ -106,7 +107,7 @@ __global__ void __launch_bounds__(128) k_surrogate_refine(const __grid_constant_
             } else {
               th_inf = acos(fmin(1.0, fmax(-1.0, (double)h[10])));
             }
-            ph_inf = atan2((double)h[12], (double)h[11]);
+            ph_inf = (double)atan2f(h[12], h[11]);
           }
           double inten = 0.0;
           for (int k = 0; k < p.max_cross; ++k) {
@@ -117,7 +118,7 @@ __global__ void __launch_bounds__(128) k_surrogate_refine(const __grid_constant_
               g = bhk::disk_g(r, a, lam);
               const double qq = p.r_in / r;
               inten += g * g * g * g * qq * qq * qq;
-              ph = (k == 0) ? atan2((double)h[5], (double)h[4]) : ((k == 1) ? atan2((double)h[8], (double)h[7]) : 0.0);
+              ph = (double)((k == 0) ? atan2f(h[5], h[4]) : ((k == 1) ? atan2f(h[8], h[7]) : 0.0f));
             }
             if (o.r_hit) o.r_hit[off] = r;
             if (o.g) o.g[off] = g;
@@ -148,14 +149,17 @@ __global__ void __launch_bounds__(128) k_surrogate_refine(const __grid_constant_
 }  // namespace
 
 extern "C" int bhk_surrogate_refine(const BhkImageParams *p, const BhkImageOut *o, const float *head, float min_conf,
-                                    double band, int verify, int refine_fp64, int *list, unsigned int *count,
-                                    unsigned int *stats, void *stream) {
+                                    double band, int verify, int refine_fp64, long long p0, long long p1, int *list,
+                                    unsigned int *count, unsigned int *stats, void *stream) {
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (p->n_pix <= 0) return 0;
-  const long long blocks = (p->n_pix + 127) / 128;
+  p1 = p1 < p->n_pix ? p1 : p->n_pix;
+  if (p1 <= p0) return 0;
+  const long long blocks = (p1 - p0 + 127) / 128;
   if (refine_fp64)
-    k_surrogate_refine<false><<<(unsigned)blocks, 128, 0, s>>>(*p, *o, head, min_conf, band, verify, list, count, stats);
+    k_surrogate_refine<false>
+        <<<(unsigned)blocks, 128, 0, s>>>(*p, *o, head, min_conf, band, verify, list, count, stats, p0, p1);
   else
-    k_surrogate_refine<true><<<(unsigned)blocks, 128, 0, s>>>(*p, *o, head, min_conf, band, verify, list, count, stats);
+    k_surrogate_refine<true>
+        <<<(unsigned)blocks, 128, 0, s>>>(*p, *o, head, min_conf, band, verify, list, count, stats, p0, p1);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

@@ -21,6 +21,8 @@
 
 using bf16 = __nv_bfloat16;
 
+constexpr int kRenderChunks = 8;
+
 struct BH_Surrogate {
   int device = -1;
   int64_t max_batch = 0;
@@ -46,6 +48,13 @@ struct BH_Surrogate {
   unsigned int *r_counts = nullptr;  // [0] list length, [1..5] stats
   unsigned long long *r_counter = nullptr;
   int64_t last_pixels = 0;
+  // renderer concurrency: refine of chunk k on `side` while chunk k+1 is inferred
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev[kRenderChunks + 2] = {};
+  // device outputs and stream of the host-buffer entry point (grow-only)
+  char *host_out = nullptr;
+  size_t host_out_bytes = 0;
+  cudaStream_t host_stream = nullptr;
   // host copy of the biases for the fused inference launch
   std::vector<float> host_bias;
   bool bias_stale = true;
@@ -217,6 +226,10 @@ void bh_surrogate_destroy(BH_Surrogate *s) {
   cudaGetDevice(&cur);
   if (s->device >= 0) cudaSetDevice(s->device);
   for (void *p : s->allocs) cudaFree(p);
+  for (cudaEvent_t e : s->ev)
+    if (e) cudaEventDestroy(e);
+  if (s->side) cudaStreamDestroy(s->side);
+  if (s->host_stream) cudaStreamDestroy(s->host_stream);
   if (cur >= 0) cudaSetDevice(cur);
   delete s;
 }
@@ -436,17 +449,80 @@ int bh_surrogate_trace_image(BH_Surrogate *s, const BH_KerrScene *scene, const B
   if (bhs_launch_grid_inputs(sc.spin, std::cos(sc.theta_obs), sc.alpha_min, da, sc.beta_min, db, sc.width, n,
                              s->r_inputs, st))
     return fail_msg("surrogate render: input launch failed");
-  if (int rc = bh_surrogate_forward(s, s->r_inputs, n, s->r_head, stream)) return rc;
   if (int rc = cuda_check(cudaMemsetAsync(s->r_counts, 0, 8 * sizeof(unsigned int), st), "cudaMemsetAsync"))
     return rc;
   const BhkImageOut o{out->cls,   out->steps,     out->n_cross,   out->r_hit,     out->phi_hit,
                       out->g,     out->flux,      out->intensity, out->theta_inf, out->phi_inf};
-  if (bhk_surrogate_refine(&p, &o, s->r_head, pol.min_confidence, pol.critical_band, pol.verify, pol.refine_fp64,
-                           s->r_list, s->r_counts, s->r_counts + 1, stream))
-    return fail_msg("surrogate render: refine launch failed");
-  if (bhk_trace_list_mixed(&p, &o, s->r_list, s->r_counts, s->r_counter, L, stream))
+  if (!s->side) {
+    if (int rc = cuda_check(cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking), "cudaStreamCreate")) return rc;
+    for (cudaEvent_t &e : s->ev)
+      if (int rc = cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate")) return rc;
+  }
+  // Chunks of whole tile pairs (256 rows): the network infers chunk k on the
+  // caller's stream while `side` refines chunk k - 1; then the integrator
+  // traces the rejected pixels on `side`, which the caller's stream joins.
+  const int64_t chunk = ((n + kRenderChunks - 1) / kRenderChunks + 255) / 256 * 256;
+  if (int rc = cuda_check(cudaEventRecord(s->ev[kRenderChunks], st), "cudaEventRecord")) return rc;
+  if (int rc = cuda_check(cudaStreamWaitEvent(s->side, s->ev[kRenderChunks], 0), "cudaStreamWaitEvent")) return rc;
+  for (int k = 0; k < kRenderChunks; ++k) {
+    const int64_t p0 = k * chunk, p1 = std::min<int64_t>(n, p0 + chunk);
+    if (p1 <= p0) break;
+    if (int rc = bh_surrogate_forward(s, s->r_inputs + 4 * p0, p1 - p0, s->r_head + BHS_HEAD * p0, stream)) return rc;
+    if (int rc = cuda_check(cudaEventRecord(s->ev[k], st), "cudaEventRecord")) return rc;
+    if (int rc = cuda_check(cudaStreamWaitEvent(s->side, s->ev[k], 0), "cudaStreamWaitEvent")) return rc;
+    if (bhk_surrogate_refine(&p, &o, s->r_head, pol.min_confidence, pol.critical_band, pol.verify, pol.refine_fp64,
+                             p0, p1, s->r_list, s->r_counts, s->r_counts + 1, s->side))
+      return fail_msg("surrogate render: refine launch failed");
+  }
+  if (bhk_trace_list_mixed(&p, &o, s->r_list, s->r_counts, s->r_counter, L, s->side))
     return fail_msg("surrogate render: fallback tracer launch failed");
-  return 0;
+  if (int rc = cuda_check(cudaEventRecord(s->ev[kRenderChunks + 1], s->side), "cudaEventRecord")) return rc;
+  return cuda_check(cudaStreamWaitEvent(st, s->ev[kRenderChunks + 1], 0), "cudaStreamWaitEvent");
+}
+
+int bh_surrogate_trace_image_host(BH_Surrogate *s, const BH_KerrScene *scene, const BH_KerrImageOut *h,
+                                  const BH_SurrogatePolicy *policy) {
+  if (!s || !scene || !h) return fail_msg("surrogate render: NULL argument");
+  if (bh_kerr_scene_validate(scene) != 0) return -1;
+  const size_t n = size_t(scene->width) * size_t(scene->height);
+  if (n == 0) return 0;
+  const size_t mc = size_t(scene->max_crossings);
+  void *const host[10] = {h->cls, h->steps, h->n_cross, h->r_hit, h->phi_hit,
+                          h->g,   h->flux,  h->intensity, h->theta_inf, h->phi_inf};
+  const size_t bytes[10] = {4 * n, 4 * n, 4 * n, 8 * n * mc, 8 * n * mc, 8 * n * mc, 8 * n, 8 * n, 8 * n, 8 * n};
+  size_t total = 0, off[10];
+  for (int i = 0; i < 10; ++i) {
+    off[i] = total;
+    if (host[i]) total += (bytes[i] + 255) & ~size_t(255);
+  }
+  if (total == 0) return 0;
+  if (total > s->host_out_bytes) {
+    if (s->host_out) {
+      auto it = std::find(s->allocs.begin(), s->allocs.end(), s->host_out);
+      if (it != s->allocs.end()) s->allocs.erase(it);
+      cudaFree(s->host_out);
+      s->host_out = nullptr;
+      s->host_out_bytes = 0;
+    }
+    if (int rc = alloc(s, &s->host_out, total, "cudaMalloc(render outputs)")) return rc;
+    s->host_out_bytes = total;
+  }
+  if (!s->host_stream)
+    if (int rc = cuda_check(cudaStreamCreateWithFlags(&s->host_stream, cudaStreamNonBlocking), "cudaStreamCreate"))
+      return rc;
+  void *d[10];
+  for (int i = 0; i < 10; ++i) d[i] = host[i] ? s->host_out + off[i] : nullptr;
+  const BH_KerrImageOut dev{static_cast<int32_t *>(d[0]), static_cast<int32_t *>(d[1]), static_cast<int32_t *>(d[2]),
+                            static_cast<double *>(d[3]),  static_cast<double *>(d[4]),  static_cast<double *>(d[5]),
+                            static_cast<double *>(d[6]),  static_cast<double *>(d[7]),  static_cast<double *>(d[8]),
+                            static_cast<double *>(d[9])};
+  if (int rc = bh_surrogate_trace_image(s, scene, &dev, policy, s->host_stream)) return rc;
+  for (int i = 0; i < 10; ++i)
+    if (host[i])
+      if (int rc = cuda_check(cudaMemcpyAsync(host[i], d[i], bytes[i], cudaMemcpyDeviceToHost, s->host_stream),
+                              "cudaMemcpyAsync(D2H)"))
+        return rc;
+  return cuda_check(cudaStreamSynchronize(s->host_stream), "bh_surrogate_trace_image_host");
 }
 
 int bh_surrogate_last_stats(BH_Surrogate *s, BH_SurrogateStats *out) {

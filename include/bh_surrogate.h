@@ -117,6 +117,12 @@ void bh_surrogate_policy_defaults(BH_SurrogatePolicy* policy);
 int bh_surrogate_trace_image(BH_Surrogate* s, const BH_KerrScene* scene, const BH_KerrImageOut* out,
                              const BH_SurrogatePolicy* policy, void* stream);
 
+/* The same with HOST output buffers (BH_KerrImageOut of host pointers, NULL =
+ * not wanted): grow-only device buffers owned by the network, one
+ * device-to-host copy per requested field, returns when the copies are done. */
+int bh_surrogate_trace_image_host(BH_Surrogate* s, const BH_KerrScene* scene, const BH_KerrImageOut* out_host,
+                                  const BH_SurrogatePolicy* policy);
+
 /* Counts of the last bh_surrogate_trace_image (synchronises the device). */
 int bh_surrogate_last_stats(BH_Surrogate* s, BH_SurrogateStats* stats);
 
