@@ -52,7 +52,7 @@ FLOPS_PER_STEP = {"dp45": 506.0, "rk4": 213.0}
 
 WORKLOADS = {
     # name: (frames, width, integrator, max_crossings)
-    "disk16": dict(width=1024, height=1024, integrator=1, max_crossings=3,
+    "disk16": dict(width=1024, height=1024, integrator=1, max_crossings=3, sky=True,
                    frames=[(a, i) for a in (0.0, 0.5, 0.9, 0.998) for i in (17.0, 45.0, 75.0, 85.0)]),
     "c0_256": dict(width=256, height=256, integrator=0, max_crossings=1, frames=[(0.9, 60.0)]),
     "disk1_512": dict(width=512, height=512, integrator=1, max_crossings=3, frames=[(0.9, 45.0)]),
@@ -62,6 +62,9 @@ WORKLOADS = {
     "c4_2048": dict(width=2048, height=2048, integrator=1, max_crossings=1, frames=[(0.9, 60.0)], surrogate=True),
 }
 SURROGATE_WEIGHTS = ROOT / "blackhole_b200" / "data" / "surrogate_c4.npz"
+# The sky of escaping rays in the disk16 workload: 6 x 512 x 512 FP16 cubemap,
+# seeded uniform noise plus 10^4 point stars (bh_sky_generate).
+SKY_SIZE, SKY_STARS, SKY_SEED = 512, 10_000, 20261203
 # MACs per ray of the network (192x256 + 3 x 256x256 + 256x16), 2 FLOPs each.
 SURROGATE_FLOPS_PER_RAY = 2.0 * (192 * 256 + 3 * 256 * 256 + 256 * 16)
 OUT_FIELDS_USED = ("cls", "steps", "n_cross", "r_hit", "phi_hit", "g", "intensity", "theta_inf", "phi_inf")
@@ -99,61 +102,68 @@ def scenes_for(workload: str, precision: int):
 # clocks sampled during the timed region
 # ---------------------------------------------------------------------------
 class ClockSampler:
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock, its maximum, power and the throttle reasons of one GPU,
+    polled through NVML every 5 ms from a thread (reads only)."""
+
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40, "sw_power_cap": 0x4}
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
-        self.proc = None
-        self.lines: list[str] = []
+        self.samples: list[tuple] = []
+        self._stop = threading.Event()
+        self._on = threading.Event()
+        self._t = None
+        self.nvml = None
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self._t = threading.Thread(target=self._read, daemon=True)
-            self._t.start()
-        except FileNotFoundError:
-            self.proc = None
+            import pynvml
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+            self.sm_max = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nvml = None
+            return
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
 
-    def wait_first_sample(self, timeout_s: float = 20.0) -> None:
-        """Block until nvidia-smi has printed a sample, so that its start-up
-        (NVML initialisation) is over before the timed region begins."""
-        t0 = time.perf_counter()
-        while self.proc is not None and not self.lines and time.perf_counter() - t0 < timeout_s:
-            time.sleep(0.05)
-        self.lines.clear()
+    def _run(self):
+        p = self.nvml
+        while not self._stop.is_set():
+            if self._on.is_set():
+                try:
+                    sm = p.nvmlDeviceGetClockInfo(self.h, p.NVML_CLOCK_SM)
+                    reasons = p.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                    power = p.nvmlDeviceGetPowerUsage(self.h) / 1000.0
+                    self.samples.append((sm, reasons, power))
+                except Exception:
+                    pass
+            time.sleep(0.005)
+
+    def wait_first_sample(self, timeout_s: float = 5.0) -> None:
+        """Arm the sampler (call just before the timed region)."""
+        self.samples.clear()
+        self._on.set()
+
+    @property
+    def lines(self):
+        return self.samples
 
     def stop(self) -> dict:
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        sm, smax, reasons = [], [], set()
-        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        if self.nvml is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["NVML unavailable"]}
+        time.sleep(0.012)  # at least one more sample after the timed region
+        self._on.clear()
+        self._stop.set()
+        if self._t is not None:
+            self._t.join(timeout=1.0)
+        sm = [s[0] for s in self.samples]
+        reasons = sorted(name for name, bit in self.REASONS.items() if any(s[1] & bit for s in self.samples))
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.sm_max, "reasons": reasons,
+                "samples": len(sm), "power_w_max": max((s[2] for s in self.samples), default=None),
+                "source": "NVML, 5 ms polling during the timed region"}
 
 
 # ---------------------------------------------------------------------------
@@ -169,6 +179,8 @@ def time_precision(args, precision: str, dev, stream, dist):
     # All frames of a step go out as one persistent launch, replayed from a
     # CUDA graph; the per-step events bracket that one launch.
     batch = kerr.TraceBatch(scenes, device=dev, fields=list(OUT_FIELDS_USED))
+    if WORKLOADS[args.workload].get("sky"):
+        batch.set_sky(kerr.sky_generate(SKY_SIZE, SKY_STARS, SKY_SEED, device=dev))
     outs = batch.outs
     tuned = batch.autotune(stream=stream) if args.autotune else batch.launch()
 
@@ -522,6 +534,9 @@ def main():
                   "max_crossings": wl["max_crossings"], "r_obs": 1000.0, "image_plane_M": [-12, 12]}
     config.update({"parallelism": f"replicas{world}", "launch": "one persistent launch per step (CUDA graph)",
                    "l2": "no inputs; outputs written once per step, larger than L2"})
+    if wl.get("sky"):
+        config["sky"] = {"cubemap": f"6x{SKY_SIZE}x{SKY_SIZE} FP16", "stars": SKY_STARS, "seed": SKY_SEED,
+                         "lookup": "nearest texel at the escape direction, added to the intensity"}
     if wl.get("surrogate"):
         config.update({"spin": 0.9, "theta_obs_deg": 60.0, "method": "mixed precision + learned surrogate",
                        "network": "192 features -> 4 x 256 SiLU -> 16, BF16 weights, FP32 accumulation",

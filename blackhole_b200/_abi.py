@@ -109,6 +109,12 @@ class KerrLaunchConfig(C.Structure):
                 ("reserved", C.c_int32)]
 
 
+class SkyCubemap(C.Structure):
+    """struct BH_SkyCubemap (device FP16 texels [6][size][size])."""
+
+    _fields_ = [("texels", C.c_void_p), ("size", C.c_int32), ("reserved", C.c_int32)]
+
+
 class AdamConfig(C.Structure):
     """struct BH_AdamConfig."""
 
@@ -119,7 +125,7 @@ class SurrogatePolicy(C.Structure):
     """struct BH_SurrogatePolicy."""
 
     _fields_ = [("min_confidence", C.c_float), ("verify", C.c_int32), ("critical_band", C.c_double),
-                ("refine_fp64", C.c_int32), ("reserved", C.c_int32)]
+                ("refine_fp64", C.c_int32), ("chunks", C.c_int32)]
 
 
 class SurrogateStats(C.Structure):
@@ -230,6 +236,12 @@ def _declare(lib: C.CDLL) -> None:
     lib.bh_kerr_batch_pixels.argtypes = [vp]
     lib.bh_kerr_batch_destroy.restype = None
     lib.bh_kerr_batch_destroy.argtypes = [vp]
+    lib.bh_sky_generate.restype = C.c_int
+    lib.bh_sky_generate.argtypes = [vp, i32, i32, C.c_uint64, vp]
+    lib.bh_kerr_trace_image_sky.restype = C.c_int
+    lib.bh_kerr_trace_image_sky.argtypes = [C.POINTER(KerrScene), C.POINTER(KerrImageOut), C.POINTER(SkyCubemap), vp]
+    lib.bh_kerr_batch_set_sky.restype = C.c_int
+    lib.bh_kerr_batch_set_sky.argtypes = [vp, C.POINTER(SkyCubemap)]
     lib.bh_measure_fma_peak.restype = C.c_int
     lib.bh_measure_fma_peak.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
     # include/bh_surrogate.h

@@ -32,6 +32,9 @@ typedef struct BhkImageParams {
   int32_t form;            // 0 reference, 1 Carter
   int32_t integrator;      // 0 RK4, 1 DP45
   int32_t precision;       // 0 FP64, 1 mixed
+  const uint16_t *sky;     // FP16 cubemap [6][sky_size][sky_size] added to escaped rays' intensity, or NULL
+  int32_t sky_size;
+  int32_t sky_pad;
 } BhkImageParams;
 
 typedef struct BhkImageOut {
@@ -119,6 +122,13 @@ int bhh_make_params(const struct BH_KerrScene *scene, BhkImageParams *p);
 int bhh_launch_image(const BhkImageParams *p, const BhkImageOut *o, unsigned long long *counter, BhkLaunch L,
                      void *stream);
 int bhh_fail(const char *msg);
+// The current device's persistent-kernel work counter (allocated once).
+int bhh_work_counter(unsigned long long **counter);
+
+// Sky cubemap (sky.cu): noise texels for every texel, then the star texels
+// (index, FP32 value) from the host list.
+int bhk_sky_fill(uint16_t *tex, int size, uint64_t seed, const long long *star_idx, const float *star_val,
+                 int n_stars, void *stream);
 
 // FMA-throughput probe (probe.cu).
 int bhk_fma_probe(int fp64, int iters, int repeats, double *tflops);

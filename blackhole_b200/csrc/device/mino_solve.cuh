@@ -207,38 +207,39 @@ BHM_HD double integrand(const Radial& q, double v) {
   return inv_sqrt(P);
 }
 
-// The same integrand with the polynomial in FP64 (it nearly cancels next to
-// the critical curve) and the reciprocal square root in FP32.
-BHM_HD float integrand_f(const Radial& q, double v) {
-  if (q.kind == 1) {
-    const double x = q.x_tp - v * v;
-    const double pt = ((q.q3 * x + q.q2) * x + q.q1) * x + q.q0;
-    return 2.0f * inv_sqrt((float)pt);
+// The same integrand entirely in FP32 (coefficients rounded once per ray).
+struct RadialF {
+  float x_tp, q3, q2, q1, q0;  // turning-point form
+  float p2, p1, p0;            // direct form
+};
+
+BHM_HD RadialF to_f32(const Radial& q) {
+  return RadialF{(float)q.x_tp, (float)q.q3, (float)q.q2, (float)q.q1, (float)q.q0,
+                 (float)q.p2,   (float)q.p1, (float)q.p0};
+}
+
+template <int KIND>
+BHM_HD float integrand_f(const RadialF& q, float v) {
+  if (KIND == 1) {
+    const float x = q.x_tp - v * v;
+    const float pt = ((q.q3 * x + q.q2) * x + q.q1) * x + q.q0;
+    return 2.0f * inv_sqrt(pt);
   }
-  const double x = v;
-  const double P = 1.0 + x * x * (q.p2 + x * (q.p1 + x * q.p0));
-  return inv_sqrt((float)P);
+  const float P = 1.0f + v * v * (q.p2 + v * (q.p1 + v * q.p0));
+  return inv_sqrt(P);
 }
 
 BHM_HD double radius_of(const Radial& q, double v) { return q.kind == 1 ? 1.0 / (q.x_tp - v * v) : 1.0 / v; }
 
 // int_{v0}^{v1} integrand: composite Gauss-Legendre with panels no wider
 // than hmax, 16 points per panel (ORDER 16), or 8 points on intervals
-// shorter than hmax / 4 (the Newton increments near convergence). FAST
-// takes the reciprocal square root and the panel sums in FP32; nodes, the
-// polynomial and the sum over panels stay FP64.
-template <int ORDER = 16, bool FAST = false>
+// shorter than hmax / 4 (the Newton increments near convergence).
+template <int ORDER = 16>
 BHM_HD double integrate(const Radial& q, double v0, double v1, double hmax) {
   const double len = v1 - v0;
   if (len == 0.0) return 0.0;
   if ((ORDER == 8 || fabs(len) <= 0.25 * hmax) && fabs(len) <= hmax) {
     const double c = v0 + 0.5 * len, hh = 0.5 * len;
-    if (FAST) {
-      float s = 0.0f;
-      for (int k = 0; k < 4; ++k)
-        s += kGl8f[k].w * (integrand_f(q, c - hh * kGl8[k].x) + integrand_f(q, c + hh * kGl8[k].x));
-      return (double)s * hh;
-    }
     double s = 0.0;
     for (int k = 0; k < 4; ++k)
       s += kGl8[k].w * (integrand(q, c - hh * kGl8[k].x) + integrand(q, c + hh * kGl8[k].x));
@@ -250,18 +251,39 @@ BHM_HD double integrate(const Radial& q, double v0, double v1, double hmax) {
   double sum = 0.0;
   for (int p = 0; p < n; ++p) {
     const double c = v0 + (p + 0.5) * h, hh = 0.5 * h;
-    if (FAST) {
-      float s = 0.0f;
-      for (int k = 0; k < 8; ++k)
-        s += kGl16f[k].w *
-             (integrand_f(q, c - hh * kGl16[k].x) + integrand_f(q, c + hh * kGl16[k].x));
-      sum += (double)s * hh;
-    } else {
-      double s = 0.0;
-      for (int k = 0; k < 8; ++k)
-        s += kGl16[k].w * (integrand(q, c - hh * kGl16[k].x) + integrand(q, c + hh * kGl16[k].x));
-      sum += s * hh;
-    }
+    double s = 0.0;
+    for (int k = 0; k < 8; ++k)
+      s += kGl16[k].w * (integrand(q, c - hh * kGl16[k].x) + integrand(q, c + hh * kGl16[k].x));
+    sum += s * hh;
+  }
+  return sum;
+}
+
+// The FP32 version for radial kind KIND: nodes, integrand and panel sums in
+// FP32; the sum over panels and the interval ends stay FP64.
+template <int KIND>
+BHM_HD double integrate_f(const RadialF& q, double v0, double v1, double hmax) {
+  const double len = v1 - v0;
+  if (len == 0.0) return 0.0;
+  if (fabs(len) <= 0.25 * hmax) {
+    const float c = (float)(v0 + 0.5 * len), hh = (float)(0.5 * len);
+    float s = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      s += kGl8f[k].w * (integrand_f<KIND>(q, c - hh * kGl8f[k].x) + integrand_f<KIND>(q, c + hh * kGl8f[k].x));
+    return (double)s * (0.5 * len);
+  }
+  int n = (int)ceil(fabs(len) / hmax);
+  n = n < 1 ? 1 : (n > 64 ? 64 : n);
+  const double h = len / n;
+  double sum = 0.0;
+  for (int p = 0; p < n; ++p) {
+    const float c = (float)(v0 + (p + 0.5) * h), hh = (float)(0.5 * h);
+    float s = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      s += kGl16f[k].w * (integrand_f<KIND>(q, c - hh * kGl16f[k].x) + integrand_f<KIND>(q, c + hh * kGl16f[k].x));
+    sum += (double)s * (0.5 * h);
   }
   return sum;
 }
@@ -321,13 +343,25 @@ BHM_HD Radial radial_motion(double a2, double a2_alam, double C, double r_obs, d
 // tau(v) from the last by an increment of quadrature. Returns 1 with (v, tau)
 // when found, 0 when tau(hi) < T (the ray stops before reaching T), -1 if
 // the iteration did not settle. seed: a first guess inside (lo, hi), or NaN.
-template <int ORDER = 16, bool FAST = false>
-BHM_HD int solve_tau(const Radial& q, double T, double lo, double tlo, double hi, double seed, double hmax,
+// FAST: FP32 quadrature (radial kind KIND), whose ~1e-8 noise in tau sets
+// the acceptance tolerance.
+template <bool FAST, int KIND>
+struct Quad {
+  const Radial& q;
+  RadialF f;
+  BHM_HD double integ(double a, double b, double hmax) const {
+    return FAST ? integrate_f<KIND>(f, a, b, hmax) : integrate<16>(q, a, b, hmax);
+  }
+  BHM_HD double at(double v) const { return FAST ? (double)integrand_f<KIND>(f, (float)v) : integrand(q, v); }
+};
+
+template <bool FAST, int KIND>
+BHM_HD int solve_tau(const Quad<FAST, KIND>& Q, double T, double lo, double tlo, double hi, double seed, double hmax,
                      double& v_out, double& t_out) {
   double v = lo, tv = tlo;
   if (seed > lo && seed < hi) {
     v = seed;
-    tv = tlo + integrate<ORDER, FAST>(q, lo, seed, hmax);
+    tv = tlo + Q.integ(lo, seed, hmax);
   }
   bool end_known = false;  // tau(hi) evaluated once, when Newton first aims past the end of the ray
   for (int it = 0; it < 80; ++it) {
@@ -338,9 +372,9 @@ BHM_HD int solve_tau(const Radial& q, double T, double lo, double tlo, double hi
       hi = v;
       end_known = true;
     }
-    double vn = v + (T - tv) / (FAST ? (double)integrand_f(q, v) : integrand(q, v));
+    double vn = v + (T - tv) / Q.at(v);
     if (!(vn < hi) && !end_known) {
-      const double t_hi = tv + integrate<ORDER, FAST>(q, v, hi, hmax);
+      const double t_hi = tv + Q.integ(v, hi, hmax);
       if (t_hi < T) {
         v_out = hi;
         t_out = t_hi;
@@ -350,10 +384,10 @@ BHM_HD int solve_tau(const Radial& q, double T, double lo, double tlo, double hi
     }
     if (!(vn > lo && vn < hi)) vn = 0.5 * (lo + hi);
     const double step = vn - v;
-    tv += integrate<ORDER, FAST>(q, v, vn, hmax);
+    tv += Q.integ(v, vn, hmax);
     v = vn;
-    if (fabs(step) <= 1e-14 * fmax(1e-3, fabs(v))) {
-      // FP32 panel sums leave ~1e-8 of noise in tau, which can pinch the bracket.
+    const double tol_v = FAST ? 1e-9 : 1e-14;
+    if (fabs(step) <= tol_v * fmax(1e-3, fabs(v))) {
       if (fabs(tv - T) <= (FAST ? 1e-6 : 1e-9) * fmax(1.0, T)) {
         v_out = v;
         t_out = tv;
@@ -383,6 +417,53 @@ struct Crossings {
 // q_Th (theta potential) and C = q_R + (lambda - a)^2 (radial potential),
 // u0 = cos theta_obs and pu0 = du/dtau at the observer. r_seed > 0 is a guess
 // of the first hit radius that starts the Newton iterations.
+template <bool FAST, int KIND>
+BHM_HD void crossing_loop(const Radial& q, const ThetaMotion& th, double r_in, double r_out, double r_seed,
+                          int max_hits, double hmax, Crossings& c) {
+  const Quad<FAST, KIND> Q{q, to_f32(q)};
+  double seed_v[2] = {NAN, NAN};
+  if (r_seed > 0.0) {
+    if (KIND == 1) {
+      const double s = sqrt(fmax(0.0, q.x_tp - 1.0 / r_seed));
+      seed_v[0] = -s;
+      seed_v[1] = s;
+    } else {
+      seed_v[0] = 1.0 / r_seed;
+    }
+  }
+  double lo = q.v_obs, tlo = 0.0;
+  for (int n = 0; n < 64; ++n) {
+    const double T = th.tau1 + n * th.period;
+    double seed = NAN;
+    if (seed_v[0] > lo && seed_v[0] < q.v_end)
+      seed = seed_v[0];
+    else if (seed_v[1] > lo && seed_v[1] < q.v_end)
+      seed = seed_v[1];
+    double v, tv;
+    const int rc = solve_tau<FAST, KIND>(Q, T, lo, tlo, q.v_end, seed, hmax, v, tv);
+    if (rc < 0) {
+      c.status = -2;
+      return;
+    }
+    if (rc == 0) return;  // the ray stops before this crossing
+    const double r = radius_of(q, v);
+    lo = v;
+    tlo = tv;
+    c.v_last = v;
+    c.t_last = tv;
+    if (r >= r_in && r <= r_out) {
+      c.r[c.n_hits++] = r;
+      if (c.n_hits >= max_hits) return;
+    }
+  }
+}
+
+// Disk crossings (r_in <= r <= r_out) of a ray in the order the tracer finds
+// them, up to max_hits (<= 3), from the ray's constants: spin a, lambda,
+// q_Th (theta potential) and C = q_R + (lambda - a)^2 (radial potential),
+// u0 = cos theta_obs and pu0 = du/dtau at the observer. r_seed > 0 is a guess
+// of the first hit radius that starts the Newton iterations. FAST: FP32
+// quadrature and FP32 elliptic integrals (r to ~4e-6 instead of ~1e-8).
 template <int ORDER = 16, bool FAST = false>
 BHM_HD Crossings crossings(const Radial& q, double a2, double lam, double qTh, double r_in, double r_out,
                            double u0, double pu0, double r_seed, int max_hits, double hmax) {
@@ -400,41 +481,10 @@ BHM_HD Crossings crossings(const Radial& q, double a2, double lam, double qTh, d
   }
   const ThetaMotion th = FAST ? theta_motion<float>(a2, qTh, lam, u0, pu0) : theta_motion<double>(a2, qTh, lam, u0, pu0);
   if (!th.crosses) return c;
-  double seed_v[2] = {NAN, NAN};
-  if (r_seed > 0.0) {
-    if (q.kind == 1) {
-      const double s = sqrt(fmax(0.0, q.x_tp - 1.0 / r_seed));
-      seed_v[0] = -s;
-      seed_v[1] = s;
-    } else {
-      seed_v[0] = 1.0 / r_seed;
-    }
-  }
-  double lo = q.v_obs, tlo = 0.0;
-  for (int n = 0; n < 64; ++n) {
-    const double T = th.tau1 + n * th.period;
-    double seed = NAN;
-    if (seed_v[0] > lo && seed_v[0] < q.v_end)
-      seed = seed_v[0];
-    else if (seed_v[1] > lo && seed_v[1] < q.v_end)
-      seed = seed_v[1];
-    double v, tv;
-    const int rc = solve_tau<ORDER, FAST>(q, T, lo, tlo, q.v_end, seed, hmax, v, tv);
-    if (rc < 0) {
-      c.status = -2;
-      return c;
-    }
-    if (rc == 0) break;  // the ray stops before this crossing
-    const double r = radius_of(q, v);
-    lo = v;
-    tlo = tv;
-    c.v_last = v;
-    c.t_last = tv;
-    if (r >= r_in && r <= r_out) {
-      c.r[c.n_hits++] = r;
-      if (c.n_hits >= max_hits) break;
-    }
-  }
+  if (q.kind == 1)
+    crossing_loop<FAST, 1>(q, th, r_in, r_out, r_seed, max_hits, hmax, c);
+  else
+    crossing_loop<FAST, 0>(q, th, r_in, r_out, r_seed, max_hits, hmax, c);
   return c;
 }
 
@@ -477,7 +527,11 @@ BHM_HD double u_at(double a2, double qTh, double lam, double u0, double pu0, dou
 // point (v, tau(v)) of the ray.
 template <int ORDER = 16, bool FAST = false>
 BHM_HD double tau_end(const Radial& q, double v, double tv, double hmax) {
-  return tv + integrate<ORDER, FAST>(q, v, q.v_end, hmax);
+  if (FAST) {
+    const RadialF f = to_f32(q);
+    return tv + (q.kind == 1 ? integrate_f<1>(f, v, q.v_end, hmax) : integrate_f<0>(f, v, q.v_end, hmax));
+  }
+  return tv + integrate<ORDER>(q, v, q.v_end, hmax);
 }
 
 // First-order image-plane distance (M) from pixel (alpha, beta) to the

@@ -424,14 +424,16 @@ __global__ void k_loss(const float* __restrict__ out, const float* __restrict__ 
 //
 // One persistent CTA per SM runs the whole network on pairs of 128-row tiles.
 // Warp 0 streams weight K-chunks by TMA through a 3-stage ring (each chunk
-// is loaded once per tile), warp 1 issues the tcgen05 MMAs, warps 2-5 and
-// 6-9 are the epilogues of tile slots 0 and 1. The activations of a slot
+// is loaded once per tile), warp 1 issues the tcgen05 MMAs, warps 2-9 and
+// 10-17 are the epilogues of tile slots 0 and 1 (two warps per TMEM lane
+// quarter, 128 columns each). The activations of a slot
 // stay in shared memory, in the 128-byte-swizzled K-major layout the MMA
 // reads; its FP32 accumulator is one half of the CTA's 512 TMEM columns.
 // While one slot's epilogue (bias, SiLU, BF16, store to shared) runs, the
 // tensor core works on the other slot.
 
-constexpr int kInfThreads = 320;
+constexpr int kInfThreads = 576;  // 2 control warps + 2 slots x 8 epilogue warps
+constexpr int kEpiThreads = 256;  // epilogue threads per slot
 constexpr int kInfRing = 3;
 constexpr int kActChunk = kBM * kBK * 2;       // 16 KB: one 64-column chunk of a tile
 constexpr int kActBytes = 4 * kActChunk;        // 64 KB: 256 columns
@@ -484,7 +486,7 @@ __global__ void __launch_bounds__(kInfThreads, 1)
       umma::mbar_init(empty(i), 1);
     }
     for (int s = 0; s < 2; ++s) {
-      umma::mbar_init(act_ready(s), 128);
+      umma::mbar_init(act_ready(s), kEpiThreads);
       umma::mbar_init(acc_full(s), 1);
     }
     umma::fence_mbar_init();
@@ -558,8 +560,10 @@ __global__ void __launch_bounds__(kInfThreads, 1)
             umma::mma_commit(acc_full(s));
           }
     }
-  } else {  // epilogue of slot s, TMEM lane quarter q
-    const int s = (warp - 2) >> 2;
+  } else {  // epilogue of slot s: TMEM lane quarter q (warp % 4), column half hf
+    const int e = warp - 2;
+    const int s = e >> 3;
+    const int hf = (e & 7) >> 2;
     const int q = warp & 3;
     const int r = q * 32 + lane;
     const uint32_t act = act0 + (uint32_t)s * kActBytes;
@@ -568,13 +572,13 @@ __global__ void __launch_bounds__(kInfThreads, 1)
     for (int64_t p = blockIdx.x; p < A.pairs; p += gridDim.x) {
       const int64_t row = (2 * p + s) * kBM + r;
       const bool valid = row < A.n;
-      {
+      {  // features: half 0 writes inputs 0, 1 (units 0..7), half 1 inputs 2, 3 and the rest (units 8..23)
         const float4 in = valid ? reinterpret_cast<const float4*>(A.in)[row] : make_float4(0.f, 0.f, 0.f, 0.5f);
         float x[4], lam, eta;
         scaled_inputs(in, x, lam, eta);
         const float z = valid ? 1.0f : 0.0f;
 #pragma unroll 1
-        for (int d = 0; d < 4; ++d) {  // columns 32 d .. 32 d + 31: units 4 d .. 4 d + 3
+        for (int d = 2 * hf; d < 2 * hf + 2; ++d) {  // columns 32 d .. 32 d + 31: units 4 d .. 4 d + 3
           float v[2 * BHS_FOURIER];
           fourier_pairs(x[d], v);
 #pragma unroll
@@ -585,11 +589,13 @@ __global__ void __launch_bounds__(kInfThreads, 1)
                     pack_bf16(z * v[8 * uu + 6], z * v[8 * uu + 7]));
           }
         }
-        // unit 16: columns 128..135 (scaled inputs, lambda, eta, two zeros); units 17..23: zero
-        st_unit(act + 2u * kActChunk, r, 0, pack_bf16(z * x[0], z * x[1]), pack_bf16(z * x[2], z * x[3]),
-                pack_bf16(z * lam, z * eta), 0u);
+        if (hf == 1) {
+          // unit 16: columns 128..135 (scaled inputs, lambda, eta, two zeros); units 17..23: zero
+          st_unit(act + 2u * kActChunk, r, 0, pack_bf16(z * x[0], z * x[1]), pack_bf16(z * x[2], z * x[3]),
+                  pack_bf16(z * lam, z * eta), 0u);
 #pragma unroll
-        for (int u = 17; u < BHS_FEATURES / 8; ++u) st_unit(act + 2u * kActChunk, r, u & 7, 0u, 0u, 0u, 0u);
+          for (int u = 17; u < BHS_FEATURES / 8; ++u) st_unit(act + 2u * kActChunk, r, u & 7, 0u, 0u, 0u, 0u);
+        }
       }
       umma::fence_async_smem();
       umma::mbar_arrive(act_ready(s));
@@ -601,17 +607,25 @@ __global__ void __launch_bounds__(kInfThreads, 1)
         umma::tc_fence_after();
         const float* b = A.bias + l * BHS_HIDDEN;
 #pragma unroll 1
-        for (int j = 0; j < BHS_HIDDEN / 32; ++j) {
-          float v[32];
-          umma::tmem_ld32(tacc + 32u * j, v);
-          uint32_t pk[16];
+        for (int jj = 0; jj < 2; ++jj) {  // 64 columns per TMEM wait: two loads in flight
+          const int j0 = 4 * hf + 2 * jj;
+          float v[64];
+          umma::tmem_ld32_nowait(tacc + 32u * j0, v);
+          umma::tmem_ld32_nowait(tacc + 32u * (j0 + 1), v + 32);
+          umma::tmem_wait_ld();
 #pragma unroll
-          for (int i = 0; i < 16; ++i)
-            pk[i] = pack_bf16(silu(v[2 * i] + b[32 * j + 2 * i]), silu(v[2 * i + 1] + b[32 * j + 2 * i + 1]));
-          const uint32_t cb = act + (uint32_t)(j >> 1) * kActChunk;
+          for (int h = 0; h < 2; ++h) {
+            const int j = j0 + h;
+            uint32_t pk[16];
 #pragma unroll
-          for (int uu = 0; uu < 4; ++uu)
-            st_unit(cb, r, (j & 1) * 4 + uu, pk[4 * uu], pk[4 * uu + 1], pk[4 * uu + 2], pk[4 * uu + 3]);
+            for (int i = 0; i < 16; ++i)
+              pk[i] = pack_bf16(silu(v[32 * h + 2 * i] + b[32 * j + 2 * i]),
+                                silu(v[32 * h + 2 * i + 1] + b[32 * j + 2 * i + 1]));
+            const uint32_t cb = act + (uint32_t)(j >> 1) * kActChunk;
+#pragma unroll
+            for (int uu = 0; uu < 4; ++uu)
+              st_unit(cb, r, (j & 1) * 4 + uu, pk[4 * uu], pk[4 * uu + 1], pk[4 * uu + 2], pk[4 * uu + 3]);
+          }
         }
         umma::fence_async_smem();
         umma::tc_fence_before();
@@ -624,13 +638,15 @@ __global__ void __launch_bounds__(kInfThreads, 1)
         break;
       }
       umma::tc_fence_after();
-      float v[16];
-      tmem_ld16(tacc, v);
-      if (valid) {
-        const float* b = A.bias + 4 * BHS_HIDDEN;
+      if (hf == 0) {
+        float v[16];
+        tmem_ld16(tacc, v);
+        if (valid) {
+          const float* b = A.bias + 4 * BHS_HIDDEN;
 #pragma unroll
-        for (int i = 0; i < 16; ++i) v[i] += b[i];
-        store_f32x16(A.out + row * BHS_HEAD, v);
+          for (int i = 0; i < 16; ++i) v[i] += b[i];
+          store_f32x16(A.out + row * BHS_HEAD, v);
+        }
       }
       umma::tc_fence_before();
     }

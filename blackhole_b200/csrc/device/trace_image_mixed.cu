@@ -22,6 +22,7 @@
 #include <cstdio>
 
 #include "frame_source.cuh"
+#include "sky.cuh"
 #include "hermite.cuh"
 #include "image_mixed.cuh"
 #include "launch.h"
@@ -141,7 +142,6 @@ __device__ __forceinline__ void finish(const BhkImageParams &p, const BhkImageOu
   if (o.cls) o.cls[pix] = cls;
   if (o.steps) o.steps[pix] = R.steps;
   if (o.n_cross) o.n_cross[pix] = R.ncross;
-  if (o.intensity) o.intensity[pix] = R.inten;
   if (R.ncross == 0 && o.flux) o.flux[pix] = 0.0;
   for (int k = R.ncross; k < p.max_cross; ++k) {
     const long long off = (long long)k * p.n_pix + pix;
@@ -149,12 +149,14 @@ __device__ __forceinline__ void finish(const BhkImageParams &p, const BhkImageOu
     if (o.phi_hit) o.phi_hit[off] = 0.0;
     if (o.g) o.g[off] = 0.0;
   }
-  double th = 0.0, ph = 0.0;
+  double th = 0.0, ph = 0.0, inten = R.inten;
   if (cls == 2) {
     const double u = to_f64(R.y.u, R.lo.u);
     th = acos(fmin(1.0, fmax(-1.0, u)));
     ph = phi_of_psi(to_f64(R.y.phi, R.lo.phi), to_f64(R.y.r, R.lo.r), p);
+    if (p.sky) inten += bhsky::radiance(p.sky, p.sky_size, u, ph);
   }
+  if (o.intensity) o.intensity[pix] = inten;
   if (o.theta_inf) o.theta_inf[pix] = th;
   if (o.phi_inf) o.phi_inf[pix] = ph;
 }

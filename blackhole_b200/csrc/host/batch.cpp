@@ -226,6 +226,19 @@ int bh_kerr_batch_set_launch(BH_KerrBatch *b, const BH_KerrLaunchConfig *cfg) {
   return 0;
 }
 
+int bh_kerr_batch_set_sky(BH_KerrBatch *b, const BH_SkyCubemap *sky) {
+  if (!b) return bhh_fail("batch is NULL");
+  if (sky && (!sky->texels || sky->size < 1)) return bhh_fail("sky cubemap needs texels and size >= 1");
+  for (BhkFrame &f : b->frames) {
+    f.p.sky = sky ? static_cast<const uint16_t *>(sky->texels) : nullptr;
+    f.p.sky_size = sky ? sky->size : 0;
+  }
+  // The kernel reads the frame table at run time: a captured graph stays valid.
+  return cuda_check(cudaMemcpy(const_cast<BhkFrame *>(b->d.frames), b->frames.data(), sizeof(BhkFrame) * b->frames.size(),
+                               cudaMemcpyHostToDevice),
+                    "frame table");
+}
+
 int bh_kerr_batch_get_launch(const BH_KerrBatch *b, BH_KerrLaunchConfig *cfg) {
   if (!b || !cfg) return bhh_fail("batch or config is NULL");
   *cfg = b->cfg;

@@ -208,6 +208,14 @@ int bhh_prepare_image_launch(const BH_KerrScene *scene, BhkImageParams *p, BhkLa
 // Records an error message from the device layer (noalloc.cu).
 int bhh_fail(const char *msg) { return fail("%s", msg); }
 
+// The current device's persistent-kernel work counter.
+int bhh_work_counter(unsigned long long **counter) {
+  DeviceScratch *ds = nullptr;
+  if (device_scratch(&ds) != 0) return -1;
+  *counter = ds->counter;
+  return 0;
+}
+
 int bhh_launch_image(const BhkImageParams *p, const BhkImageOut *o, unsigned long long *counter, BhkLaunch L,
                      void *stream) {
   if (p->precision == BH_PRECISION_MIXED) {

@@ -21,7 +21,8 @@
 
 using bf16 = __nv_bfloat16;
 
-constexpr int kRenderChunks = 8;
+constexpr int kRenderChunks = 8;   // most chunks a render splits into
+constexpr int kDefaultChunks = 2;
 
 struct BH_Surrogate {
   int device = -1;
@@ -405,7 +406,7 @@ void bh_surrogate_policy_defaults(BH_SurrogatePolicy *p) {
   p->verify = 1;
   p->critical_band = 0.05;
   p->refine_fp64 = 0;
-  p->reserved = 0;
+  p->chunks = 0;
 }
 
 int bh_surrogate_trace_image(BH_Surrogate *s, const BH_KerrScene *scene, const BH_KerrImageOut *out,
@@ -415,8 +416,10 @@ int bh_surrogate_trace_image(BH_Surrogate *s, const BH_KerrScene *scene, const B
   bh_surrogate_policy_defaults(&pol);
   if (policy) pol = *policy;
   if (!(pol.min_confidence >= 0.0f && pol.min_confidence <= 1.0f) || pol.verify < 1 || pol.verify > 2 ||
-      !(pol.critical_band >= 0.0))
-    return fail_msg("surrogate render: policy needs min_confidence in [0, 1], verify 1 or 2, critical_band >= 0");
+      !(pol.critical_band >= 0.0) || pol.chunks < 0 || pol.chunks > kRenderChunks)
+    return fail_msg("surrogate render: policy needs min_confidence in [0, 1], verify 1 or 2, critical_band >= 0, "
+                    "chunks in [0, %d]", kRenderChunks);
+  const int n_chunks = pol.chunks > 0 ? pol.chunks : kDefaultChunks;
   BH_KerrScene sc = *scene;
   sc.precision = BH_PRECISION_MIXED;  // the fallback integrator
   BhkImageParams p;
@@ -461,10 +464,10 @@ int bh_surrogate_trace_image(BH_Surrogate *s, const BH_KerrScene *scene, const B
   // Chunks of whole tile pairs (256 rows): the network infers chunk k on the
   // caller's stream while `side` refines chunk k - 1; then the integrator
   // traces the rejected pixels on `side`, which the caller's stream joins.
-  const int64_t chunk = ((n + kRenderChunks - 1) / kRenderChunks + 255) / 256 * 256;
+  const int64_t chunk = ((n + n_chunks - 1) / n_chunks + 255) / 256 * 256;
   if (int rc = cuda_check(cudaEventRecord(s->ev[kRenderChunks], st), "cudaEventRecord")) return rc;
   if (int rc = cuda_check(cudaStreamWaitEvent(s->side, s->ev[kRenderChunks], 0), "cudaStreamWaitEvent")) return rc;
-  for (int k = 0; k < kRenderChunks; ++k) {
+  for (int k = 0; k < n_chunks; ++k) {
     const int64_t p0 = k * chunk, p1 = std::min<int64_t>(n, p0 + chunk);
     if (p1 <= p0) break;
     if (int rc = bh_surrogate_forward(s, s->r_inputs + 4 * p0, p1 - p0, s->r_head + BHS_HEAD * p0, stream)) return rc;

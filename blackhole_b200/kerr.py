@@ -77,11 +77,29 @@ def _out_struct(outs: dict) -> KerrImageOut:
     return o
 
 
-def trace_image(s: KerrScene, outs: dict[str, torch.Tensor] | None = None, stream=None) -> dict[str, torch.Tensor]:
+def sky_generate(size: int = 512, n_stars: int = 10_000, seed: int = 1, device="cuda", stream=None) -> torch.Tensor:
+    """The seeded background sky (bh_sky_generate): FP16 cubemap [6][size][size]."""
+    tex = torch.empty(6, size, size, dtype=torch.float16, device=device)
+    check(_abi.load_library().bh_sky_generate(tex.data_ptr(), size, n_stars, seed, _stream_ptr(stream)))
+    return tex
+
+
+def _sky_struct(sky: torch.Tensor | None):
+    if sky is None:
+        return None
+    if sky.dtype != torch.float16 or not sky.is_cuda or sky.dim() != 3 or sky.shape[0] != 6:
+        raise TypeError("sky must be a CUDA float16 tensor [6][N][N]")
+    return _abi.SkyCubemap(sky.data_ptr(), sky.shape[1], 0)
+
+
+def trace_image(s: KerrScene, outs: dict[str, torch.Tensor] | None = None, stream=None,
+                sky: torch.Tensor | None = None) -> dict[str, torch.Tensor]:
     """Trace every pixel of ``s`` on the current CUDA device (asynchronous).
 
     ``outs`` maps BH_KerrImageOut field names to device tensors; missing
     fields are not written. Allocates all fields when ``outs`` is None.
+    ``sky``: a cubemap (sky_generate) whose radiance escaped rays add to
+    their intensity.
     """
     if outs is None:
         outs = alloc_image_outputs(s)
@@ -91,7 +109,11 @@ def trace_image(s: KerrScene, outs: dict[str, torch.Tensor] | None = None, strea
         if not v.is_cuda or not v.is_contiguous():
             raise TypeError(f"output {k} must be a contiguous CUDA tensor")
     o = _out_struct(outs)
-    check(_abi.load_library().bh_kerr_trace_image(C.byref(s), C.byref(o), _stream_ptr(stream)))
+    if sky is not None:
+        check(_abi.load_library().bh_kerr_trace_image_sky(C.byref(s), C.byref(o), C.byref(_sky_struct(sky)),
+                                                          _stream_ptr(stream)))
+    else:
+        check(_abi.load_library().bh_kerr_trace_image(C.byref(s), C.byref(o), _stream_ptr(stream)))
     return outs
 
 
@@ -173,6 +195,12 @@ class TraceBatch:
         """Trace through a captured CUDA graph (captured on first use)."""
         check(self._lib.bh_kerr_batch_trace_graph(self._h, _stream_ptr(stream)))
         return self.outs
+
+    def set_sky(self, sky: torch.Tensor | None):
+        """Attach a sky cubemap to every frame (None detaches)."""
+        self._sky = sky  # keep the texels alive
+        st = _sky_struct(sky)
+        check(self._lib.bh_kerr_batch_set_sky(self._h, C.byref(st) if st is not None else None))
 
     def set_launch(self, block_threads=0, ctas_per_sm=0, refill_steps=1):
         cfg = _abi.KerrLaunchConfig(block_threads, ctas_per_sm, refill_steps, 0)

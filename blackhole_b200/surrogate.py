@@ -157,14 +157,14 @@ class Surrogate:
                                                 C.byref(cfg), _ptr(loss), _stream(stream)))
 
     def trace_image(self, scene, outs: dict | None = None, min_confidence: float = 0.99, verify: int = 1,
-                    critical_band: float = 0.05, refine_fp64: bool = False, stream=None) -> dict:
+                    critical_band: float = 0.05, refine_fp64: bool = False, chunks: int = 0, stream=None) -> dict:
         """Render a scene through the network with exact refinement and the
         integrator on rejected pixels (bh_surrogate_trace_image)."""
         from .kerr import _out_struct, alloc_image_outputs
 
         if outs is None:
             outs = alloc_image_outputs(scene)
-        pol = _abi.SurrogatePolicy(min_confidence, verify, critical_band, int(refine_fp64), 0)
+        pol = _abi.SurrogatePolicy(min_confidence, verify, critical_band, int(refine_fp64), int(chunks))
         o = _out_struct(outs)
         check(self._lib.bh_surrogate_trace_image(self._h, C.byref(scene), C.byref(o), C.byref(pol),
                                                  _stream(stream)))

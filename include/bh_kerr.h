@@ -333,6 +333,40 @@ int64_t bh_kerr_batch_pixels(const BH_KerrBatch *batch);
 /** Free the batch (NULL is allowed). */
 void bh_kerr_batch_destroy(BH_KerrBatch *batch);
 
+/* ------------------------------------------------------------------------ */
+/* Part 4: background sky of escaping rays                                   */
+/* ------------------------------------------------------------------------ */
+
+/**
+ * A cubemap of FP16 texels on the device: [6][size][size], faces +X, -X, +Y,
+ * -Y, +Z, -Z with the OpenGL cube-map addressing; an escaped ray samples the
+ * nearest texel in its direction (theta_inf, phi_inf) at the escape radius.
+ * The reference renders its sky from textures bound to its GL/CUDA kernels
+ * (src/cuda/device_physics.cuh, background sampling of d_shade_hit); this is
+ * its headless counterpart.
+ */
+typedef struct BH_SkyCubemap {
+    const void *texels;
+    int32_t size;
+    int32_t reserved;
+} BH_SkyCubemap;
+
+/**
+ * Fill `texels` (device, 6 * size^2 FP16) with the seeded sky: uniform noise
+ * in [0, 1) plus n_stars point stars of brightness in [2, 20) added to single
+ * texels (stars on the same texel add up). Deterministic in (size, n_stars,
+ * seed); synchronises with the device when n_stars > 0.
+ */
+int bh_sky_generate(void *texels, int32_t size, int32_t n_stars, uint64_t seed, void *stream);
+
+/** bh_kerr_trace_image plus the sky: escaped rays add the radiance of their
+ *  texel to `intensity` (sky NULL: same as bh_kerr_trace_image). */
+int bh_kerr_trace_image_sky(const BH_KerrScene *scene, const BH_KerrImageOut *out, const BH_SkyCubemap *sky,
+                            void *stream);
+
+/** Attach a sky to every frame of a batch (NULL detaches). */
+int bh_kerr_batch_set_sky(BH_KerrBatch *batch, const BH_SkyCubemap *sky);
+
 /**
  * Measured FMA-pipe peak of the current device in TFLOP/s (fp64 != 0: FP64,
  * else FP32): best of `repeats` launches of independent FMA chains covering

@@ -92,9 +92,9 @@ typedef struct BH_SurrogatePolicy {
                               2: run the exact crossing search on every pixel */
     double critical_band;  /* first-order image-plane distance to the critical curve, M,
                               below which a pixel goes to the integrator (0.05) */
-    int32_t refine_fp64;   /* 0: Mino-time quadrature with FP32 reciprocal square roots and
-                              panel sums (r_hit to ~4e-6); 1: all FP64 (~1e-8) */
-    int32_t reserved;
+    int32_t refine_fp64;   /* 0: Mino-time quadrature in FP32 (r_hit to ~4e-6); 1: all FP64 (~1e-8) */
+    int32_t chunks;        /* pixel chunks whose refinement (second stream) overlaps the next
+                              chunk's inference; 0 = default (1..8) */
 } BH_SurrogatePolicy;
 
 typedef struct BH_SurrogateStats {

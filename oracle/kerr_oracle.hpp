@@ -519,6 +519,7 @@ template <class T> struct PixelResult {
   int32_t cls, steps, n_cross;
   T r_hit[3], phi_hit[3], g[3];
   T flux, intensity, theta_inf, phi_inf;
+  T u_inf;  // cos(theta_inf) before the arc cosine (sky lookups)
 };
 
 // Derived per-scene constants.
@@ -689,7 +690,8 @@ inline PixelResult<T> trace_pixel(const Scene &s, const SceneDerived<T> &d, T al
   const int maxc = std::max(1, std::min(3, int(s.max_crossings)));
   auto in_disk = [&](T r) { return r >= d.r_in && r <= d.r_out; };
   auto finish_escape = [&](const Y<T> &yy) {
-    out.theta_inf = s_acos(s_clamp(yy.u, T(-1), T(1)));
+    out.u_inf = s_clamp(yy.u, T(-1), T(1));
+    out.theta_inf = s_acos(out.u_inf);
     out.phi_inf = phi_of_psi(yy.phi, yy.r, T(s.r_obs), d.a, d.r_plus, d.r_minus);
   };
 

@@ -6,6 +6,7 @@
 // the FLOP count per step with the counting scalar, and a __float128 run of
 // the stepper.
 #include <atomic>
+#include <bit>
 #include <cstring>
 #include <thread>
 #include <vector>
@@ -110,6 +111,68 @@ int bho_trace_alpha_beta(const BH_KerrScene *scene, int64_t n, const double *alp
     const auto p = bho::trace_pixel<double>(s, d, alpha[i], beta[i]);
     store(out, i, n, maxc, p);
   });
+  return 0;
+}
+
+// ---- background sky (restated from the OpenGL cube-map convention) ----
+//
+// Face of the largest |component| (ties: x, then y) in the order +X, -X, +Y,
+// -Y, +Z, -Z; face coordinates +X (-z,-y), -X (z,-y), +Y (x,z), -Y (x,-z),
+// +Z (x,-y), -Z (-x,-y); nearest texel of u = (s/ma + 1)/2, v = (t/ma + 1)/2.
+static int64_t sky_texel(double x, double y, double z, int N) {
+  const double ax = std::fabs(x), ay = std::fabs(y), az = std::fabs(z);
+  int face;
+  double sc, tc, ma;
+  if (ax >= ay && ax >= az) {
+    ma = ax;
+    face = x >= 0.0 ? 0 : 1;
+    sc = x >= 0.0 ? -z : z;
+    tc = -y;
+  } else if (ay >= az) {
+    ma = ay;
+    face = y >= 0.0 ? 2 : 3;
+    sc = x;
+    tc = y >= 0.0 ? z : -z;
+  } else {
+    ma = az;
+    face = z >= 0.0 ? 4 : 5;
+    sc = z >= 0.0 ? x : -x;
+    tc = -y;
+  }
+  const double u = 0.5 * (sc / ma + 1.0), v = 0.5 * (tc / ma + 1.0);
+  int i = int(u * double(N)), j = int(v * double(N));
+  i = std::min(std::max(i, 0), N - 1);
+  j = std::min(std::max(j, 0), N - 1);
+  return (int64_t(face) * N + j) * N + i;
+}
+
+static double sky_radiance(const uint16_t *tex, int N, double u, double phi) {
+  const double st = std::sqrt((1.0 - u) * (1.0 + u));
+  const double x = st * std::cos(phi), y = st * std::sin(phi), z = u;
+  const _Float16 h = std::bit_cast<_Float16>(tex[sky_texel(x, y, z, N)]);
+  return double(float(h));
+}
+
+// bho_trace_pixels with the sky added to escaped rays' intensity.
+int bho_trace_pixels_sky(const BH_KerrScene *scene, int64_t n, const int64_t *pix_index, const BH_KerrImageOut *out,
+                         int threads, const uint16_t *sky, int sky_size) {
+  const bho::Scene s = to_scene(scene);
+  const auto d = bho::derive<double>(s);
+  const int maxc = std::max(1, std::min(3, int(s.max_crossings)));
+  parallel_for(n, threads, [&](int64_t i) {
+    const int64_t pix = pix_index ? pix_index[i] : i;
+    double alpha, beta;
+    bho::pixel_alpha_beta(s, pix, alpha, beta);
+    auto p = bho::trace_pixel<double>(s, d, alpha, beta);
+    if (sky && p.cls == 2) p.intensity = p.intensity + sky_radiance(sky, sky_size, p.u_inf, p.phi_inf);
+    store(out, i, n, maxc, p);
+  });
+  return 0;
+}
+
+// Texel indices of directions (tests of the addressing).
+int bho_sky_texels(int64_t n, const double *x, const double *y, const double *z, int N, int64_t *out) {
+  for (int64_t i = 0; i < n; ++i) out[i] = sky_texel(x[i], y[i], z[i], N);
   return 0;
 }
 

@@ -86,6 +86,9 @@ class Oracle(_Base):
         L = self.lib
         L.bho_trace_pixels.argtypes = [C.POINTER(KerrScene), _i64, _vp, C.POINTER(KerrImageOut), C.c_int]
         L.bho_trace_alpha_beta.argtypes = [C.POINTER(KerrScene), _i64, _vp, _vp, C.POINTER(KerrImageOut), C.c_int]
+        L.bho_trace_pixels_sky.argtypes = [C.POINTER(KerrScene), _i64, _vp, C.POINTER(KerrImageOut), C.c_int, _vp,
+                                           C.c_int]
+        L.bho_sky_texels.argtypes = [_i64, _vp, _vp, _vp, C.c_int, _vp]
         L.bho_trace_alpha_beta_ld.argtypes = L.bho_trace_alpha_beta.argtypes
         L.bho_count_ops.argtypes = [C.POINTER(KerrScene), _f64, _f64, _vp, _vp]
         L.bho_count_step_ops.argtypes = [_f64, _f64, _f64, _vp]
@@ -106,6 +109,21 @@ class Oracle(_Base):
     def trace_pixels(self, scene: KerrScene, pix: np.ndarray | None = None, threads: int | None = None):
         n = scene.width * scene.height if pix is None else len(pix)
         return self._trace(self.lib.bho_trace_pixels, scene, pix, n, threads or default_threads())
+
+    def trace_pixels_sky(self, scene: KerrScene, sky: np.ndarray, pix: np.ndarray | None = None,
+                         threads: int | None = None):
+        """trace_pixels plus the cubemap sky (uint16 FP16 bits [6][N][N]) on escaped rays."""
+        sky = np.ascontiguousarray(sky).view(np.uint16)
+        size = int(round((sky.size / 6) ** 0.5))
+        fn = lambda sc, n, idx, o, th: self.lib.bho_trace_pixels_sky(sc, n, idx, o, th, _ptr(sky), size)  # noqa: E731
+        n = scene.width * scene.height if pix is None else len(pix)
+        return self._trace(fn, scene, pix, n, threads or default_threads())
+
+    def sky_texels(self, x, y, z, size: int) -> np.ndarray:
+        x, y, z = (np.ascontiguousarray(v, np.float64) for v in (x, y, z))
+        out = np.zeros(len(x), np.int64)
+        self.lib.bho_sky_texels(len(x), _ptr(x), _ptr(y), _ptr(z), size, _ptr(out))
+        return out
 
     def trace_alpha_beta(self, scene: KerrScene, alpha, beta, threads: int | None = None, long_double=False):
         alpha = np.ascontiguousarray(alpha, np.float64)
