@@ -60,6 +60,7 @@ WORKLOADS = {
     "disk_2048": dict(width=2048, height=2048, integrator=0, max_crossings=1, frames=[(0.9, 60.0)]),
     "batch4096": dict(integrator=1, max_crossings=1, generator=lambda: batch_frames()),
     "c4_2048": dict(width=2048, height=2048, integrator=1, max_crossings=1, frames=[(0.9, 60.0)], surrogate=True),
+    "c2_512": dict(width=512, height=512, integrator=1, max_crossings=1, frames=[(0.94, 17.0)], rt=True),
 }
 SURROGATE_WEIGHTS = ROOT / "blackhole_b200" / "data" / "surrogate_c4.npz"
 # The sky of escaping rays in the disk16 workload: 6 x 512 x 512 FP16 cubemap,
@@ -478,6 +479,53 @@ def run_surrogate(args, rank: int, world: int, dist):
     return dict(value=value, ms_per_step=elapsed_ms / args.steps, e2e=e2e, roofline=roofline, clocks=clocks,
                 total_steps=int(outs["steps"].sum().item()), rays_per_step=n, launches=launches, extra=extra)
 
+
+def run_rt(args, rank: int, world: int, dist):
+    """The volumetric workload: one step = one 512^2 render of I_nu through the
+    synthetic 128 x 64 x 64 torus (FP64 DP45 rays, <= 2000 steps)."""
+    import torch
+
+    from blackhole_b200 import kerr
+    from blackhole_b200 import rt
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(device=dev)
+    med = rt.Medium(device=dev)
+    lut = rt.Lut(device=dev)
+    prm = rt.rt_defaults()
+    s = kerr.scene(width=512, height=512, spin=0.94, theta_obs=math.radians(17.0), integrator=1, precision=0,
+                   max_crossings=1, max_steps=2000, alpha_min=-20, alpha_max=20, beta_min=-20, beta_max=20)
+    n = s.width * s.height
+    outs = None
+
+    def render():
+        nonlocal outs
+        outs = rt.trace(s, med, lut, prm, outs=outs, stream=stream)
+
+    sampler = ClockSampler(dev.index if "CUDA_VISIBLE_DEVICES" not in os.environ else 0)
+    sampler.start()
+    sampler.wait_first_sample()
+    ms = _timed_launches(render, stream, args.steps, args.warmup)
+    clocks = sampler.stop()
+    elapsed_ms = sum(ms)
+    if dist is not None:
+        t = torch.tensor([elapsed_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    value = n * args.steps * world / (elapsed_ms * 1e-3)
+    steps = int(outs["steps"].sum().item())
+    cls = outs["cls"].cpu().numpy()
+    extra = {"rt": {"steps_per_ray": steps / n, "classes": {str(c): int((cls == c).sum()) for c in np.unique(cls)},
+                    "lit_fraction": float((outs["i_nu"] > 0).double().mean().item()),
+                    "tau_median": float(outs["tau"].median().item()), "nu_hz": prm.nu_hz,
+                    "ds_max_M": prm.ds_max}}
+    roofline = {"bound": "fp64", "achieved": None, "peak": None, "unit": "TFLOP/s", "frac": None, "traffic": None,
+                "kernel": "k_trace_rt_fp64", "launch_ms_mean": statistics.mean(ms),
+                "note": "geodesic + grid/LUT sampling; no FLOP count frozen for the transfer samples yet"}
+    return dict(value=value, ms_per_step=elapsed_ms / args.steps, e2e=None, roofline=roofline, clocks=clocks,
+                total_steps=steps, rays_per_step=n, launches=args.steps, extra=extra)
+
 # ---------------------------------------------------------------------------
 # reference arm: the reference's compiled CPU code on the host cores
 # ---------------------------------------------------------------------------
@@ -537,6 +585,13 @@ def main():
     if wl.get("sky"):
         config["sky"] = {"cubemap": f"6x{SKY_SIZE}x{SKY_SIZE} FP16", "stars": SKY_STARS, "seed": SKY_SEED,
                          "lookup": "nearest texel at the escape direction, added to the intensity"}
+    if wl.get("rt"):
+        config.update({"spin": 0.94, "theta_obs_deg": 17.0, "image_plane_M": [-20, 20], "max_steps": 2000,
+                       "medium": "128x64x64 (log r 2..50 M, theta, phi) FP32 grid: Gaussian torus r_in 6, r_peak 12 "
+                                 "x exp(GRF sigma 0.5, correlation 2 M)",
+                       "emission": "thermal synchrotron, 256x256 FP32 table over (log Theta_e, log nu/nu_s), "
+                                   "Kirchhoff absorption", "precision": "fp64",
+                       "launch": "one persistent launch per step"})
     if wl.get("surrogate"):
         config.update({"spin": 0.9, "theta_obs_deg": 60.0, "method": "mixed precision + learned surrogate",
                        "network": "192 features -> 4 x 256 SiLU -> 16, BF16 weights, FP32 accumulation",
@@ -563,13 +618,18 @@ def main():
 
         dist_mod.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
         dist = dist_mod
-    res = run_surrogate(args, rank, world, dist) if wl.get("surrogate") else run_ours(args, rank, world, dist)
+    if wl.get("surrogate"):
+        res = run_surrogate(args, rank, world, dist)
+    elif wl.get("rt"):
+        res = run_rt(args, rank, world, dist)
+    else:
+        res = run_ours(args, rank, world, dist)
     if rank == 0:
         cb = cpu_reference(args.workload, args.cpu_budget) if (world == 1 and args.cpu_budget > 0) else None
         line = {"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None,
-                "dtype": "bf16+f32+f64" if wl.get("surrogate") else ("f64" if args.precision == "fp64" else "f32+f64"),
+                "dtype": "bf16+f32+f64" if wl.get("surrogate") else ("f64" if (args.precision == "fp64" or wl.get("rt")) else "f32+f64"),
                 "data": "synthetic", "config": config, "precision": args.precision,
                 "steps_per_s": res["total_steps"] * args.steps * world / (res["ms_per_step"] * args.steps * 1e-3),
                 **res["extra"],

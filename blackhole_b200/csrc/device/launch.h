@@ -125,6 +125,25 @@ int bhh_fail(const char *msg);
 // The current device's persistent-kernel work counter (allocated once).
 int bhh_work_counter(unsigned long long **counter);
 
+// Along-ray radiative transfer (rt.cuh, trace_image_fp64.cu).
+typedef struct BhkRtParams {
+  const float *cells;   // float4 (n_e, Theta_e, |B|, 0) [n_r][n_th][n_ph]
+  int32_t n_r, n_th, n_ph, pad0;
+  double r_min, r_max, inv_log_range;  // 1 / log(r_max / r_min)
+  const float *lut;     // [n_lt][n_lx] ln(j_nu / (n_e nu_B))
+  int32_t n_lt, n_lx;
+  double lt0, lt1, lx0, lx1;           // log Theta_e and log x ranges
+  double nu, length_cm, ds_max, min_transmit;
+} BhkRtParams;
+
+int bhk_trace_rt_fp64(const BhkImageParams *p, const BhkRtParams *q, double *i_nu, double *tau, int32_t *cls,
+                      int32_t *steps, unsigned long long *work_counter, int grid, int block, void *stream);
+
+// Synthetic torus grid (grmhd.cu): modes [n_modes] of (kx, ky, kz, phase).
+int bhk_grmhd_fill(float *cells, int n_r, int n_th, int n_ph, double r_min, double r_max, double r_in, double r_peak,
+                   double width, double n0, double theta0, double b0, double amp, const double *modes, int n_modes,
+                   void *stream);
+
 // Sky cubemap (sky.cu): noise texels for every texel, then the star texels
 // (index, FP32 value) from the host list.
 int bhk_sky_fill(uint16_t *tex, int size, uint64_t seed, const long long *star_idx, const float *star_val,

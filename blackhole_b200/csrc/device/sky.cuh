@@ -7,7 +7,7 @@
 //   +X (-z, -y)   -X (z, -y)   +Y (x, z)   -Y (x, -z)   +Z (x, -y)   -Z (-x, -y),
 // u = (s / ma + 1) / 2, v = (t / ma + 1) / 2, texel (floor(u N), floor(v N))
 // clamped to [0, N-1]; the texel index is (face N + row) N + column. The
-// lookup is nearest-texel.
+// lookup is nearest-texel, in the escaping ray's direction of motion.
 //
 // The generated sky (bh_sky_generate) is seeded uniform noise in [0, 1):
 // texel k gets the top 24 bits of splitmix64(seed * 0x100000001B3 + k)
@@ -86,20 +86,28 @@ BHSKY_HD long long texel_of(double x, double y, double z, int N) {
   return ((long long)face * N + j) * N + i;
 }
 
-// Direction of an escaped ray from u = cos(theta) and the azimuth phi.
-BHSKY_HD void direction(double u, double phi, double& x, double& y, double& z) {
+// Cartesian direction of motion of a ray at (r, u = cos theta, phi) moving
+// with dr = p_r, du = p_u, dphi (derivatives in any common parameter): the
+// sky point it comes from. Unlike the position angles, it changes only at
+// O(M b / r^3) along an escaping ray, so where the integrator stopped past
+// the escape radius does not matter.
+BHSKY_HD void direction_of_motion(double r, double u, double phi, double pr, double pu, double dphi, double& x,
+                                  double& y, double& z) {
   const double uc = u < -1.0 ? -1.0 : (u > 1.0 ? 1.0 : u);
   const double st = sqrt((1.0 - uc) * (1.0 + uc));
-  x = st * cos(phi);
-  y = st * sin(phi);
-  z = uc;
+  const double cp = cos(phi), sp = sin(phi);
+  const double dst = st > 1e-300 ? -uc * pu / st : 0.0;  // d(sin theta)
+  x = (pr * st + r * dst) * cp - (r * st * dphi) * sp;
+  y = (pr * st + r * dst) * sp + (r * st * dphi) * cp;
+  z = pr * uc + r * pu;
 }
 
 #ifdef __CUDACC__
-// Radiance of the nearest texel in direction (u = cos theta, phi).
-__device__ __forceinline__ double radiance(const uint16_t* tex, int N, double u, double phi) {
+// Radiance of the nearest texel in the direction of motion (see above).
+__device__ __forceinline__ double radiance(const uint16_t* tex, int N, double r, double u, double phi, double pr,
+                                           double pu, double dphi) {
   double x, y, z;
-  direction(u, phi, x, y, z);
+  direction_of_motion(r, u, phi, pr, pu, dphi, x, y, z);
   const unsigned short bits = tex[texel_of(x, y, z, N)];
   return (double)__half2float(__ushort_as_half(bits));
 }

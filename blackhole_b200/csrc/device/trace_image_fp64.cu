@@ -16,6 +16,7 @@
 #include <cstdio>
 
 #include "frame_source.cuh"
+#include "rt.cuh"
 #include "sky.cuh"
 #include "hermite.cuh"
 #include "image_fp64.cuh"
@@ -115,7 +116,12 @@ __device__ __forceinline__ void finish(const BhkImageParams &p, const BhkImageOu
     const double u = R.y.u;
     th = acos((u < -1.0) ? -1.0 : ((1.0 < u) ? 1.0 : u));
     ph = phi_of_psi(R.y.phi, R.y.r, p);
-    if (p.sky) inten = inten + bhsky::radiance(p.sky, p.sky_size, u, ph);
+    if (p.sky) {  // dphi/dtau = dpsi/dtau + a p_r / Delta  (phi = psi + a G(r), G' = 1 / Delta)
+      const Yd k = rhs(R.y, R.c);
+      const double delta = ((R.y.r * R.y.r) - (2.0 * R.y.r)) + p.a2;
+      const double dphi = k.phi + (p.a * R.y.pr) / delta;
+      inten = inten + bhsky::radiance(p.sky, p.sky_size, R.y.r, u, ph, R.y.pr, R.y.pu, dphi);
+    }
   }
   if (o.intensity) o.intensity[pix] = inten;
   if (o.theta_inf) o.theta_inf[pix] = th;
@@ -234,6 +240,103 @@ __global__ void __launch_bounds__(128, 4) k_trace_batch_fp64(const __grid_consta
   trace_loop<INTEG>(bhsrc::BatchSrc{b}, counter, refill);
 }
 
+// ---- along-ray radiative transfer -------------------------------------------
+
+// Transfer over one accepted step y0 -> y1 (derivatives k0, k1 at its ends):
+// samples at most ds_max apart in affine length, positions by cubic Hermite
+// interpolation in Mino time.
+__device__ __forceinline__ void rt_segment(const BhkImageParams &p, const BhkRtParams &q, const RayC &c,
+                                           const Yd &y0, const Yd &k0, const Yd &y1, const Yd &k1, double h,
+                                           double &I, double &T, double &tau) {
+  const double rm = 0.5 * (y0.r + y1.r) + 0.125 * h * (k0.r - k1.r);
+  const double um = 0.5 * (y0.u + y1.u) + 0.125 * h * (k0.u - k1.u);
+  const double sig_m = rm * rm + p.a2 * um * um;
+  double ns = ceil((sig_m * h) / q.ds_max);
+  ns = ns < 1.0 ? 1.0 : (ns > 64.0 ? 64.0 : ns);
+  const int nsub = (int)ns;
+  const double dt = h / ns;
+  for (int m = 0; m < nsub; ++m) {
+    const double t = ((double)m + 0.5) / ns;
+    const double t2 = t * t, t3 = t2 * t;
+    const double h00 = 2.0 * t3 - 3.0 * t2 + 1.0, h10 = t3 - 2.0 * t2 + t;
+    const double h01 = -2.0 * t3 + 3.0 * t2, h11 = t3 - t2;
+    const double r = h00 * y0.r + h10 * h * k0.r + h01 * y1.r + h11 * h * k1.r;
+    const double u = h00 * y0.u + h10 * h * k0.u + h01 * y1.u + h11 * h * k1.u;
+    const double psi = h00 * y0.phi + h10 * h * k0.phi + h01 * y1.phi + h11 * h * k1.phi;
+    const double dl = (r * r + p.a2 * u * u) * dt;  // affine length of the sample, M
+    double n, th, b;
+    if (!bhrt::sample(q, r, u, phi_of_psi(psi, r, p), n, th, b)) continue;
+    const double g = bhrt::redshift(p.a, r, u, c.lam);
+    if (!(g > 0.0)) continue;
+    double j, al;
+    bhrt::synchrotron(q, n, th, b, q.nu / g, j, al);
+    const double jo = g * g * j, ao = al / g;
+    const double ds = dl * q.length_cm;
+    const double ts = ao * ds;
+    const double om = (ts < 1.0e-4) ? ts * (1.0 - 0.5 * ts) : -expm1(-ts);
+    I = (ao > 0.0) ? I + T * ((jo / ao) * om) : I + T * (jo * ds);
+    T = T * (1.0 - om);
+    tau = tau + ts;
+  }
+}
+
+__global__ void __launch_bounds__(128) k_trace_rt_fp64(const __grid_constant__ BhkImageParams p,
+                                                       const __grid_constant__ BhkRtParams q,
+                                                       double *__restrict__ i_nu, double *__restrict__ tau_out,
+                                                       int *__restrict__ cls_out, int *__restrict__ steps_out,
+                                                       unsigned long long *__restrict__ counter) {
+  const unsigned lane = threadIdx.x & 31u;
+  for (;;) {
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(counter, 32ull);
+    base = __shfl_sync(kFull, base, 0);
+    if (base >= (unsigned long long)p.n_pix) break;
+    const long long pix = (long long)base + lane;
+    if (pix >= p.n_pix) continue;
+    RayFp64 R;
+    init_ray(p, pix, R);
+    double I = 0.0, T = 1.0, tau = 0.0;
+    int cls = 3;
+    const long long max_attempts = 4LL * p.max_steps + 64;
+    for (;;) {
+      if (R.steps >= p.max_steps || R.attempts >= max_attempts) {
+        cls = 3;
+        break;
+      }
+      if (R.y.r <= p.r_hor) {
+        cls = 0;
+        break;
+      }
+      if (R.y.r >= p.r_esc) {
+        cls = 2;
+        break;
+      }
+      ++R.attempts;
+      const DPRes d = dp45(R.y, R.h, R.c, R.k1, p.rtol, p.atol, true);
+      if (d.err <= 1.0) {
+        ++R.steps;
+        rt_segment(p, q, R.c, R.y, R.k1, d.y5, d.k7, R.h, I, T, tau);
+        R.y = d.y5;
+        R.k1 = d.k7;
+        project(R.y, R.c);
+        R.k1.r = R.y.pr;
+        R.k1.u = R.y.pu;
+        R.h = R.h * step_factor(d.err, true);
+        if (T < q.min_transmit) {
+          cls = 4;
+          break;
+        }
+      } else {
+        R.h = R.h * step_factor(d.err, false);
+      }
+    }
+    if (i_nu) i_nu[pix] = I;
+    if (tau_out) tau_out[pix] = tau;
+    if (cls_out) cls_out[pix] = cls;
+    if (steps_out) steps_out[pix] = R.steps;
+  }
+}
+
 }  // namespace bhk
 
 namespace {
@@ -291,5 +394,17 @@ extern "C" int bhk_trace_batch_fp64_occupancy(int integrator, int block, int *bl
                       : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhk::k_trace_batch_fp64<1>,
                                                                       block, 0);
   if (e != cudaSuccess) return set_err(e, "occupancy query");
+  return 0;
+}
+
+extern "C" int bhk_trace_rt_fp64(const BhkImageParams *p, const BhkRtParams *q, double *i_nu, double *tau,
+                                 int32_t *cls, int32_t *steps, unsigned long long *counter, int grid, int block,
+                                 void *stream) {
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return set_err(e, "work-counter reset");
+  bhk::k_trace_rt_fp64<<<grid, block, 0, s>>>(*p, *q, i_nu, tau, cls, steps, counter);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(e, "k_trace_rt_fp64 launch");
   return 0;
 }

@@ -154,7 +154,13 @@ __device__ __forceinline__ void finish(const BhkImageParams &p, const BhkImageOu
     const double u = to_f64(R.y.u, R.lo.u);
     th = acos(fmin(1.0, fmax(-1.0, u)));
     ph = phi_of_psi(to_f64(R.y.phi, R.lo.phi), to_f64(R.y.r, R.lo.r), p);
-    if (p.sky) inten += bhsky::radiance(p.sky, p.sky_size, u, ph);
+    if (p.sky) {  // dphi/dtau = dpsi/dtau + a p_r / Delta  (phi = psi + a G(r), G' = 1 / Delta)
+      const Yf k = rhs(R.y, R.c);
+      const double r = to_f64(R.y.r, R.lo.r);
+      const double delta = r * r - 2.0 * r + p.a2;
+      const double dphi = (double)k.phi + p.a * (double)R.y.pr / delta;
+      inten += bhsky::radiance(p.sky, p.sky_size, r, u, ph, (double)R.y.pr, (double)R.y.pu, dphi);
+    }
   }
   if (o.intensity) o.intensity[pix] = inten;
   if (o.theta_inf) o.theta_inf[pix] = th;

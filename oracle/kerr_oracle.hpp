@@ -520,6 +520,7 @@ template <class T> struct PixelResult {
   T r_hit[3], phi_hit[3], g[3];
   T flux, intensity, theta_inf, phi_inf;
   T u_inf;  // cos(theta_inf) before the arc cosine (sky lookups)
+  T r_end, pr_end, pu_end, dphi_end;  // escape point: radius, momenta, d(phi)/d(Mino time)
 };
 
 // Derived per-scene constants.
@@ -691,6 +692,14 @@ inline PixelResult<T> trace_pixel(const Scene &s, const SceneDerived<T> &d, T al
   auto in_disk = [&](T r) { return r >= d.r_in && r <= d.r_out; };
   auto finish_escape = [&](const Y<T> &yy) {
     out.u_inf = s_clamp(yy.u, T(-1), T(1));
+    {  // direction of motion for the sky: dphi = dpsi + a p_r / Delta
+      const Y<T> k = img_rhs(yy, c);
+      const T delta = ((yy.r * yy.r) - (T(2) * yy.r)) + d.a * d.a;
+      out.r_end = yy.r;
+      out.pr_end = yy.pr;
+      out.pu_end = yy.pu;
+      out.dphi_end = k.phi + (d.a * yy.pr) / delta;
+    }
     out.theta_inf = s_acos(out.u_inf);
     out.phi_inf = phi_of_psi(yy.phi, yy.r, T(s.r_obs), d.a, d.r_plus, d.r_minus);
   };

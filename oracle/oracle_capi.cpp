@@ -13,6 +13,7 @@
 
 #include "../include/bh_kerr.h"
 #include "kerr_oracle.hpp"
+#include "rt_oracle.hpp"
 
 namespace {
 
@@ -146,9 +147,17 @@ static int64_t sky_texel(double x, double y, double z, int N) {
   return (int64_t(face) * N + j) * N + i;
 }
 
-static double sky_radiance(const uint16_t *tex, int N, double u, double phi) {
+// Direction of motion of the ray at its escape point (the sky point it comes
+// from): the Cartesian velocity of (r, theta, phi) with dr = p_r,
+// du = p_u (u = cos theta) and dphi.
+static double sky_radiance(const uint16_t *tex, int N, double r, double u, double phi, double pr, double pu,
+                           double dphi) {
   const double st = std::sqrt((1.0 - u) * (1.0 + u));
-  const double x = st * std::cos(phi), y = st * std::sin(phi), z = u;
+  const double cp = std::cos(phi), sp = std::sin(phi);
+  const double dst = st > 1e-300 ? -u * pu / st : 0.0;
+  const double x = (pr * st + r * dst) * cp - (r * st * dphi) * sp;
+  const double y = (pr * st + r * dst) * sp + (r * st * dphi) * cp;
+  const double z = pr * u + r * pu;
   const _Float16 h = std::bit_cast<_Float16>(tex[sky_texel(x, y, z, N)]);
   return double(float(h));
 }
@@ -164,7 +173,9 @@ int bho_trace_pixels_sky(const BH_KerrScene *scene, int64_t n, const int64_t *pi
     double alpha, beta;
     bho::pixel_alpha_beta(s, pix, alpha, beta);
     auto p = bho::trace_pixel<double>(s, d, alpha, beta);
-    if (sky && p.cls == 2) p.intensity = p.intensity + sky_radiance(sky, sky_size, p.u_inf, p.phi_inf);
+    if (sky && p.cls == 2)
+      p.intensity = p.intensity + sky_radiance(sky, sky_size, p.r_end, p.u_inf, p.phi_inf, p.pr_end, p.pu_end,
+                                               p.dphi_end);
     store(out, i, n, maxc, p);
   });
   return 0;
@@ -174,6 +185,35 @@ int bho_trace_pixels_sky(const BH_KerrScene *scene, int64_t n, const int64_t *pi
 int bho_sky_texels(int64_t n, const double *x, const double *y, const double *z, int N, int64_t *out) {
   for (int64_t i = 0; i < n; ++i) out[i] = sky_texel(x[i], y[i], z[i], N);
   return 0;
+}
+
+// ---- along-ray radiative transfer (rt_oracle.hpp) ----
+int bho_trace_rt(const BH_KerrScene *scene, int64_t n, const int64_t *pix_index, const float *cells, int n_r,
+                 int n_th, int n_ph, double r_min, double r_max, const float *lut, int n_lt, int n_lx, double lt0,
+                 double lt1, double lx0, double lx1, double nu, double length_cm, double ds_max, double min_transmit,
+                 double *i_nu, double *tau, int32_t *cls, int32_t *steps, int threads) {
+  const bho::Scene s = to_scene(scene);
+  const auto d = bho::derive<double>(s);
+  const bho_rt::Medium q{cells, n_r, n_th, n_ph, r_min, r_max, 1.0 / std::log(r_max / r_min), lut, n_lt, n_lx,
+                         lt0, lt1, lx0, lx1, nu, length_cm, ds_max, min_transmit};
+  parallel_for(n, threads, [&](int64_t i) {
+    const int64_t pix = pix_index ? pix_index[i] : i;
+    double alpha, beta;
+    bho::pixel_alpha_beta(s, pix, alpha, beta);
+    const bho_rt::Result r = bho_rt::trace_pixel_rt(s, d, alpha, beta, q);
+    i_nu[i] = r.I;
+    tau[i] = r.tau;
+    cls[i] = r.cls;
+    steps[i] = r.steps;
+  });
+  return 0;
+}
+
+// Front-to-back formal solution over segments given near to far.
+double bho_rt_path(int64_t n, const double *j, const double *alpha, const double *ds) {
+  double I = 0.0, T = 1.0, tau = 0.0;
+  for (int64_t i = 0; i < n; ++i) bho_rt::segment(j[i], alpha[i], ds[i], I, T, tau);
+  return I;
 }
 
 // Same in long double (x87 80-bit) for rounding checks.

@@ -89,6 +89,10 @@ class Oracle(_Base):
         L.bho_trace_pixels_sky.argtypes = [C.POINTER(KerrScene), _i64, _vp, C.POINTER(KerrImageOut), C.c_int, _vp,
                                            C.c_int]
         L.bho_sky_texels.argtypes = [_i64, _vp, _vp, _vp, C.c_int, _vp]
+        L.bho_trace_rt.argtypes = ([C.POINTER(KerrScene), _i64, _vp, _vp, C.c_int, C.c_int, C.c_int, _f64, _f64, _vp,
+                                    C.c_int, C.c_int] + [_f64] * 8 + [_vp] * 4 + [C.c_int])
+        L.bho_rt_path.restype = _f64
+        L.bho_rt_path.argtypes = [_i64, _vp, _vp, _vp]
         L.bho_trace_alpha_beta_ld.argtypes = L.bho_trace_alpha_beta.argtypes
         L.bho_count_ops.argtypes = [C.POINTER(KerrScene), _f64, _f64, _vp, _vp]
         L.bho_count_step_ops.argtypes = [_f64, _f64, _f64, _vp]
@@ -118,6 +122,25 @@ class Oracle(_Base):
         fn = lambda sc, n, idx, o, th: self.lib.bho_trace_pixels_sky(sc, n, idx, o, th, _ptr(sky), size)  # noqa: E731
         n = scene.width * scene.height if pix is None else len(pix)
         return self._trace(fn, scene, pix, n, threads or default_threads())
+
+    def trace_rt(self, scene: KerrScene, cells: np.ndarray, r_range, lut: np.ndarray, log_theta, log_x, nu,
+                 length_cm, ds_max, min_transmit, pix: np.ndarray | None = None, threads: int | None = None):
+        """Along-ray transfer through the grid cells [n_r][n_th][n_ph][4] with table lut [n_lt][n_lx]."""
+        cells = np.ascontiguousarray(cells, np.float32)
+        lut = np.ascontiguousarray(lut, np.float32)
+        n = scene.width * scene.height if pix is None else len(pix)
+        idx = None if pix is None else np.ascontiguousarray(pix, np.int64)
+        out = {"i_nu": np.zeros(n), "tau": np.zeros(n), "cls": np.zeros(n, np.int32), "steps": np.zeros(n, np.int32)}
+        self.lib.bho_trace_rt(C.byref(scene), n, _ptr(idx), _ptr(cells), cells.shape[0], cells.shape[1],
+                              cells.shape[2], r_range[0], r_range[1], _ptr(lut), lut.shape[0], lut.shape[1],
+                              log_theta[0], log_theta[1], log_x[0], log_x[1], nu, length_cm, ds_max, min_transmit,
+                              _ptr(out["i_nu"]), _ptr(out["tau"]), _ptr(out["cls"]), _ptr(out["steps"]),
+                              threads or default_threads())
+        return out
+
+    def rt_path(self, j, alpha, ds) -> float:
+        j, alpha, ds = (np.ascontiguousarray(v, np.float64) for v in (j, alpha, ds))
+        return float(self.lib.bho_rt_path(len(j), _ptr(j), _ptr(alpha), _ptr(ds)))
 
     def sky_texels(self, x, y, z, size: int) -> np.ndarray:
         x, y, z = (np.ascontiguousarray(v, np.float64) for v in (x, y, z))
@@ -196,6 +219,13 @@ class RefLib(_Base):
             raise FileNotFoundError(f"{path} not built (reference sources absent at build time)")
         self.lib = C.CDLL(str(path))
         L = self.lib
+        for fn in ("ref_synchrotron_j", "ref_synchrotron_alpha"):
+            getattr(L, fn).restype = _f64
+            getattr(L, fn).argtypes = [_f64] * 4
+        L.ref_planck.restype = _f64
+        L.ref_planck.argtypes = [_f64, _f64]
+        L.ref_rte_path.restype = _f64
+        L.ref_rte_path.argtypes = [_i64, _vp, _vp, _vp]
         L.ref_kerr_potentials.argtypes = [_i64, _vp, _vp, _f64, _f64, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
         L.ref_kerr_step_mino.argtypes = [_i64] + [_vp] * 6 + [_f64, _f64, _vp, _vp, _vp, _vp, _f64, _i32]
         L.ref_kerr_trace_rays.argtypes = ([_i64] + [_vp] * 9 + [_f64] * 5 + [_i32] + [_vp] * 7 + [C.c_int])
@@ -218,6 +248,19 @@ class RefLib(_Base):
     def trace_rays(self, state, e, lz, q, mass, a, r_horizon, r_escape, step, max_steps, threads=None):
         return _trace_rays(self.lib.ref_kerr_trace_rays, state, e, lz, q, mass, a, r_horizon, r_escape,
                            step, max_steps, threads or default_threads())
+
+    def synchrotron_j(self, nu, b, n, theta):
+        return self.lib.ref_synchrotron_j(nu, b, n, theta)
+
+    def synchrotron_alpha(self, nu, b, n, theta):
+        return self.lib.ref_synchrotron_alpha(nu, b, n, theta)
+
+    def planck(self, nu, temp):
+        return self.lib.ref_planck(nu, temp)
+
+    def rte_path(self, j, alpha, ds) -> float:
+        j, alpha, ds = (np.ascontiguousarray(v, np.float64) for v in (j, alpha, ds))
+        return float(self.lib.ref_rte_path(len(j), _ptr(j), _ptr(alpha), _ptr(ds)))
 
     def raytracer_defaults(self, mass: float, spin_param: float):
         out = np.zeros(4, np.float64)

@@ -24,6 +24,7 @@
 #include "physics/constants.h"
 #include "physics/kerr.h"
 #include "physics/novikov_thorne.h"
+#include "physics/rte_integrator.h"
 
 #include "../include/bh_kerr.h"
 #include "kerr_oracle.hpp"
@@ -243,6 +244,23 @@ int ref_trace_pixels(const BH_KerrScene *scene, int64_t n, const int64_t *pix_in
     if (out->phi_inf) out->phi_inf[i] = p.phi_inf;
   });
   return 0;
+}
+
+// The reference's own radiative-transfer physics (src/physics/rte_integrator.h).
+double ref_synchrotron_j(double nu, double b, double n, double theta) {
+  return physics::synchrotronThermalEmissivity(nu, b, n, theta);
+}
+double ref_synchrotron_alpha(double nu, double b, double n, double theta) {
+  return physics::synchrotronThermalAbsorption(nu, b, n, theta);
+}
+double ref_planck(double nu, double temp) { return physics::planckFunction(nu, temp); }
+
+// rteStep over segments given near to far, applied far to near as the
+// reference's integrateRtePath orders them.
+double ref_rte_path(int64_t n, const double *j, const double *alpha, const double *ds) {
+  physics::RteState st{};
+  for (int64_t i = n - 1; i >= 0; --i) st = physics::rteStep(st, j[i], alpha[i], ds[i]);
+  return st.iNu;
 }
 
 }  // extern "C"
