@@ -61,6 +61,9 @@ WORKLOADS = {
     "batch4096": dict(integrator=1, max_crossings=1, generator=lambda: batch_frames()),
     "c4_2048": dict(width=2048, height=2048, integrator=1, max_crossings=1, frames=[(0.9, 60.0)], surrogate=True),
     "c2_512": dict(width=512, height=512, integrator=1, max_crossings=1, frames=[(0.94, 17.0)], rt=True),
+    # smaller copies of the two scenes above, for profiler captures
+    "c4_1024": dict(width=1024, height=1024, integrator=1, max_crossings=1, frames=[(0.9, 60.0)], surrogate=True),
+    "c2_128": dict(width=128, height=128, integrator=1, max_crossings=1, frames=[(0.94, 17.0)], rt=True),
 }
 SURROGATE_WEIGHTS = ROOT / "blackhole_b200" / "data" / "surrogate_c4.npz"
 # The sky of escaping rays in the disk16 workload: 6 x 512 x 512 FP16 cubemap,
@@ -425,7 +428,7 @@ def run_surrogate(args, rank: int, world: int, dist):
     fp64_rk4 = 256 * 256 / (statistics.mean(msc0) * 1e-3)
     extra = {
         "fp64_plain": {"value": fp64_dp45, "unit": UNIT, "ms_per_step": statistics.mean(ms64),
-                       "method": "FP64 DP45 rtol 1e-8 on the same 2048^2 frame",
+                       "method": f"FP64 DP45 rtol 1e-8 on the same {smx.width}x{smx.height} frame",
                        "steps_per_ray": float(o64["steps"].double().mean().item())},
         "fp64_plain_rk4": {"value": fp64_rk4, "unit": UNIT, "ms_per_step": statistics.mean(msc0),
                            "method": "FP64 RK4 h = 0.02 min(r, 20), the plain method of the 256^2 frame of this "
@@ -475,7 +478,8 @@ def run_surrogate(args, rank: int, world: int, dist):
         e2e = {"value": n * k / (w1 - w0), "unit": UNIT, "h2d_bytes_per_step": C.sizeof(_abi.KerrScene),
                "d2h_bytes_per_step": sum(t.numel() * t.element_size() for t in pinned.values()),
                "api": "bh_surrogate_trace_image_host", "fields": list(fields)}
-    launches = (1 + 2 * 8 + 1) * args.steps  # inputs, 8 x (inference, refinement), fallback tracer
+    chunks = 2  # the renderer's default chunk count (BH_SurrogatePolicy.chunks = 0)
+    launches = (1 + 2 * chunks + 1) * args.steps  # inputs, chunks x (inference, refinement), fallback tracer
     return dict(value=value, ms_per_step=elapsed_ms / args.steps, e2e=e2e, roofline=roofline, clocks=clocks,
                 total_steps=int(outs["steps"].sum().item()), rays_per_step=n, launches=launches, extra=extra)
 
@@ -494,7 +498,9 @@ def run_rt(args, rank: int, world: int, dist):
     med = rt.Medium(device=dev)
     lut = rt.Lut(device=dev)
     prm = rt.rt_defaults()
-    s = kerr.scene(width=512, height=512, spin=0.94, theta_obs=math.radians(17.0), integrator=1, precision=0,
+    wl = WORKLOADS[args.workload]
+    s = kerr.scene(width=wl["width"], height=wl["height"], spin=0.94, theta_obs=math.radians(17.0), integrator=1,
+                   precision=0,
                    max_crossings=1, max_steps=2000, alpha_min=-20, alpha_max=20, beta_min=-20, beta_max=20)
     n = s.width * s.height
     outs = None
@@ -597,8 +603,9 @@ def main():
                        "network": "192 features -> 4 x 256 SiLU -> 16, BF16 weights, FP32 accumulation",
                        "weights": "blackhole_b200/data/surrogate_c4.npz (trained on 2^26 integrator rays)",
                        "policy": {"min_confidence": 0.99, "critical_band_M": 0.05, "verify": "radial kind"},
-                       "launch": "18 launches per render on two streams (inference || refinement)",
-                       "l2": "outputs (4 Mi pixels x 9 fields) written once per step, larger than L2"})
+                       "launch": "6 launches per render on two streams: inputs, 2 x (inference, refinement), "
+                                 "integrator on the rejected pixels",
+                       "l2": f"outputs ({wl['width']}^2 pixels x 9 fields) written once per step, larger than L2"})
 
     if args.impl == "reference":
         if rank != 0:
