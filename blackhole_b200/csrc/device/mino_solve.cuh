@@ -386,7 +386,10 @@ BHM_HD int solve_tau(const Quad<FAST, KIND>& Q, double T, double lo, double tlo,
     const double step = vn - v;
     tv += Q.integ(v, vn, hmax);
     v = vn;
-    const double tol_v = FAST ? 1e-9 : 1e-14;
+    // Newton converges quadratically here: once a step is below tol_v the
+    // error left is of order tol_v^2 relative, far below FP32 quadrature
+    // noise (~1e-8) in the fast path.
+    const double tol_v = FAST ? 1e-6 : 1e-14;
     if (fabs(step) <= tol_v * fmax(1e-3, fabs(v))) {
       if (fabs(tv - T) <= (FAST ? 1e-6 : 1e-9) * fmax(1.0, T)) {
         v_out = v;
@@ -491,6 +494,10 @@ BHM_HD Crossings crossings(const Radial& q, double a2, double lam, double qTh, d
 // u = cos theta reached at Mino time tau from (u0, pu0) (the ray must cross
 // the equator: theta_motion(...).crosses). chi increases monotonically:
 // u = sqrt(z+) sin chi, Phi(chi) = int_0^chi dchi / sqrt(w + m sin^2 chi).
+// T: precision of the elliptic integrals and of the Newton iteration on chi
+// (the roots z+, w and the period bookkeeping stay FP64); T = float gives u
+// to a few 1e-7.
+template <class T = double>
 BHM_HD double u_at(double a2, double qTh, double lam, double u0, double pu0, double tau) {
   const double c0 = qTh - lam * lam;
   const double b2 = a2 - qTh;
@@ -498,8 +505,8 @@ BHM_HD double u_at(double a2, double qTh, double lam, double u0, double pu0, dou
   const double zp = (b2 > 0.0) ? (b2 + sq) / (2.0 * a2) : 2.0 * c0 / (sq - b2);
   const double w = c0 / zp, m = a2 * zp, rz = sqrt(zp);
   const double s0 = fmax(-1.0, fmin(1.0, u0 / rz));
-  const double K = quarter_period<double>(w, m);
-  const double phi_x = s0 * carlson_rf(w * (1.0 - s0 * s0), w + m * s0 * s0, w);  // odd in s0
+  const double K = (double)quarter_period<T>(T(w), T(m));
+  const double phi_x = s0 * (double)carlson_rf<T>(T(w * (1.0 - s0 * s0)), T(w + m * s0 * s0), T(w));  // odd in s0
   const double phi_start = (pu0 >= 0.0) ? phi_x : 2.0 * K - phi_x;
   double total = phi_start + tau;
   const double n = floor(total / (2.0 * K));
@@ -507,20 +514,22 @@ BHM_HD double u_at(double a2, double qTh, double lam, double u0, double pu0, dou
   const bool second = rem > K;
   if (second) rem = 2.0 * K - rem;   // chi' -> pi - chi' has the same sine
   // Phi(chi) = rem on [0, pi/2]: bracketed Newton.
-  double lo = 0.0, hi = 1.5707963267948966, chi = rem * sqrt(w + 0.5 * m);
+  const T wT = T(w), mT = T(m), remT = T(rem);
+  T lo = T(0), hi = T(1.5707963267948966), chi = T(rem * sqrt(w + 0.5 * m));
   chi = fmin(fmax(chi, lo), hi);
+  const T tol = sizeof(T) == 4 ? T(2e-7) : T(1e-15);
   for (int it = 0; it < 60; ++it) {
-    const double s = sin(chi), c = cos(chi);
-    const double f = s * carlson_rf(w * c * c, w + m * s * s, w) - rem;
-    if (f < 0.0) lo = chi; else hi = chi;
-    double nc = chi - f * sqrt(w + m * s * s);
-    if (!(nc > lo && nc < hi)) nc = 0.5 * (lo + hi);
-    const double step = nc - chi;
+    const T s = sin(chi), c = cos(chi);
+    const T f = s * carlson_rf<T>(wT * c * c, wT + mT * s * s, wT) - remT;
+    if (f < T(0)) lo = chi; else hi = chi;
+    T nc = chi - f * sqrt(wT + mT * s * s);
+    if (!(nc > lo && nc < hi)) nc = T(0.5) * (lo + hi);
+    const T step = nc - chi;
     chi = nc;
-    if (fabs(step) < 1e-15) break;
+    if (fabs(step) < tol) break;
   }
   const double sgn = (fmod(n, 2.0) != 0.0) ? -1.0 : 1.0;
-  return sgn * rz * sin(chi);
+  return sgn * rz * (double)sin(chi);
 }
 
 // Mino time at which the tracer stops (escape or horizon radius), from a

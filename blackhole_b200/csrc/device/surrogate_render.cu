@@ -12,8 +12,8 @@
 //   4. the exact solve disagrees with the network's
 //      class                                          -> integrator
 // Accepted disk pixels get r_hit from the Mino-time solve seeded with the
-// network's radius (FP32 reciprocal square roots in the quadrature by
-// default, all FP64 on request), and g, flux and intensity from r_hit exactly as the
+// network's radius (FP32 quadrature and elliptic integrals by default, all
+// FP64 on request), and g, flux and intensity from r_hit exactly as the
 // tracer computes them; escaped pixels get theta_inf from the exact polar
 // motion at the escape radius; phi_hit and phi_inf are the network's.
 #include <cuda_runtime.h>
@@ -25,7 +25,11 @@
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr double kPanel = 0.125;  // Gauss-Legendre-16 panel width of the Mino-time quadrature
+// Gauss-Legendre-16 panel width of the Mino-time quadrature: 0.125 for the
+// FP64 solve (r to ~1e-8); the FP32 fast path, limited to ~4e-6 in r by its
+// integrand, gets the same accuracy from panels twice as wide.
+template <bool FAST>
+constexpr double kPanel = FAST ? 0.25 : 0.125;
 
 __device__ __forceinline__ void warp_count(unsigned *stats, int slot, bool pred) {
   const unsigned m = __ballot_sync(kFull, pred);
@@ -83,7 +87,7 @@ __global__ void __launch_bounds__(128) k_surrogate_refine(const __grid_constant_
         if (nn_cls == 1 || verify >= 2) {
           const double r_seed = (double)__expf(h[3] + 2.0f);
           c = bhmino::crossings<16, FAST>(q, p.a2, lam, qTh, p.r_in, p.r_out, p.cos_o, pu0, r_seed, p.max_cross,
-                                          kPanel);
+                                          kPanel<FAST>);
           solved = c.status == 0;
           nhit = c.n_hits;
           for (int k = 0; k < 3; ++k) rh[k] = c.r[k];
@@ -101,8 +105,9 @@ __global__ void __launch_bounds__(128) k_surrogate_refine(const __grid_constant_
           if (cls == 2) {
             const bhmino::ThetaMotion tm = bhmino::theta_motion(p.a2, qTh, lam, p.cos_o, pu0);
             if (tm.crosses) {
-              const double te = bhmino::tau_end<16, FAST>(q, c.v_last, c.t_last, kPanel);
-              const double u = bhmino::u_at(p.a2, qTh, lam, p.cos_o, pu0, te);
+              const double te = bhmino::tau_end<16, FAST>(q, c.v_last, c.t_last, kPanel<FAST>);
+              const double u = FAST ? bhmino::u_at<float>(p.a2, qTh, lam, p.cos_o, pu0, te)
+                                    : bhmino::u_at<double>(p.a2, qTh, lam, p.cos_o, pu0, te);
               th_inf = acos(fmin(1.0, fmax(-1.0, u)));
             } else {
               th_inf = acos(fmin(1.0, fmax(-1.0, (double)h[10])));
