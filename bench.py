@@ -485,8 +485,10 @@ def run_surrogate(args, rank: int, world: int, dist):
 
 
 def run_rt(args, rank: int, world: int, dist):
-    """The volumetric workload: one step = one 512^2 render of I_nu through the
-    synthetic 128 x 64 x 64 torus (FP64 DP45 rays, <= 2000 steps)."""
+    """The volumetric workload: one step = one render of I_nu through the
+    synthetic 128 x 64 x 64 torus (DP45 rays, <= 2000 steps), at the
+    requested precision; the FP64 render of the same frame is timed beside it
+    and is the accuracy reference."""
     import torch
 
     from blackhole_b200 import kerr
@@ -499,9 +501,14 @@ def run_rt(args, rank: int, world: int, dist):
     lut = rt.Lut(device=dev)
     prm = rt.rt_defaults()
     wl = WORKLOADS[args.workload]
-    s = kerr.scene(width=wl["width"], height=wl["height"], spin=0.94, theta_obs=math.radians(17.0), integrator=1,
-                   precision=0,
-                   max_crossings=1, max_steps=2000, alpha_min=-20, alpha_max=20, beta_min=-20, beta_max=20)
+    prec = 1 if args.precision == "mixed" else 0
+
+    def scene(pr):
+        return kerr.scene(width=wl["width"], height=wl["height"], spin=0.94, theta_obs=math.radians(17.0),
+                          integrator=1, precision=pr, max_crossings=1, max_steps=2000, alpha_min=-20, alpha_max=20,
+                          beta_min=-20, beta_max=20)
+
+    s = scene(prec)
     n = s.width * s.height
     outs = None
 
@@ -526,11 +533,62 @@ def run_rt(args, rank: int, world: int, dist):
                     "lit_fraction": float((outs["i_nu"] > 0).double().mean().item()),
                     "tau_median": float(outs["tau"].median().item()), "nu_hz": prm.nu_hz,
                     "ds_max_M": prm.ds_max}}
-    roofline = {"bound": "fp64", "achieved": None, "peak": None, "unit": "TFLOP/s", "frac": None, "traffic": None,
-                "kernel": "k_trace_rt_fp64", "launch_ms_mean": statistics.mean(ms),
-                "note": "geodesic + grid/LUT sampling; no FLOP count frozen for the transfer samples yet"}
-    return dict(value=value, ms_per_step=elapsed_ms / args.steps, e2e=None, roofline=roofline, clocks=clocks,
-                total_steps=steps, rays_per_step=n, launches=args.steps, extra=extra)
+    if prec == 1:
+        s64 = scene(0)
+        o64 = None
+
+        def render64():
+            nonlocal o64
+            o64 = rt.trace(s64, med, lut, prm, outs=o64, stream=stream)
+
+        ms64 = _timed_launches(render64, stream, 2, 1)
+        a, b = outs, o64
+        lit = (b["i_nu"] > 1e-6 * b["i_nu"].max()) & (a["cls"] == b["cls"])
+        rel = ((a["i_nu"][lit] - b["i_nu"][lit]).abs() / b["i_nu"][lit]).float()
+        q = torch.quantile(rel, torch.tensor([0.5, 0.99], device=rel.device)).tolist()
+        extra["fp64_plain"] = {"value": n / (statistics.mean(ms64) * 1e-3), "unit": UNIT,
+                               "ms_per_step": statistics.mean(ms64), "method": "FP64 DP45 transfer, same frame"}
+        extra["speedup_vs_fp64_plain"] = value / extra["fp64_plain"]["value"]
+        extra["accuracy_vs_fp64"] = {"class_agreement": float((a["cls"] == b["cls"]).double().mean().item()),
+                                     "i_nu_rel_median": q[0], "i_nu_rel_p99": q[1],
+                                     "pixels_compared": int(lit.sum().item()),
+                                     "note": "the mixed steps differ, so samples sit elsewhere on each ray: "
+                                             "differences are at the sampling's discretization level"}
+    roofline = {"bound": "fp64" if prec == 0 else "fp32", "achieved": None, "peak": None, "unit": "TFLOP/s",
+                "frac": None, "traffic": None, "kernel": "k_trace_rt_fp64" if prec == 0 else "k_trace_rt_mixed",
+                "launch_ms_mean": statistics.mean(ms),
+                "note": "geodesic steps and medium samples; no FLOP count frozen for the samples yet"}
+    # ---- end to end: medium and table uploaded from pinned host memory, I_nu and tau read back ----
+    e2e = None
+    if rank == 0:
+        cells_h = med.cells.cpu().pin_memory()
+        lut_h = lut.table.cpu().pin_memory()
+        out_h = {k: torch.empty(n, dtype=torch.float64).pin_memory() for k in ("i_nu", "tau")}
+
+        def step_e2e():
+            med.cells.copy_(cells_h, non_blocking=True)
+            lut.table.copy_(lut_h, non_blocking=True)
+            torch.cuda.current_stream().synchronize()
+            o = rt.trace(s, med, lut, prm)
+            for k in out_h:
+                out_h[k].copy_(o[k], non_blocking=True)
+            torch.cuda.synchronize()
+
+        step_e2e()
+        k = max(1, min(args.steps, 3))
+        w0 = time.perf_counter()
+        for _ in range(k):
+            step_e2e()
+        w1 = time.perf_counter()
+        e2e = {"value": n * k / (w1 - w0), "unit": UNIT,
+               "h2d_bytes_per_step": cells_h.numel() * cells_h.element_size() + lut_h.numel() * lut_h.element_size(),
+               "d2h_bytes_per_step": sum(t.numel() * t.element_size() for t in out_h.values()),
+               "api": "bh_kerr_trace_rt (device buffers) with the medium uploaded and I_nu, tau read back"}
+    d = lut.desc
+    cpu_inputs = {"scene": scene(0), "cells": med.cells.cpu().numpy(), "lut": lut.table.cpu().numpy(),
+                  "log_theta": (d.log_theta_min, d.log_theta_max), "log_x": (d.log_x_min, d.log_x_max), "rt": prm}
+    return dict(value=value, ms_per_step=elapsed_ms / args.steps, e2e=e2e, roofline=roofline, clocks=clocks,
+                total_steps=steps, rays_per_step=n, launches=args.steps, extra=extra, cpu_inputs=cpu_inputs)
 
 # ---------------------------------------------------------------------------
 # reference arm: the reference's compiled CPU code on the host cores
@@ -557,6 +615,32 @@ def cpu_reference(workload: str, budget_s: float, seed: int = 7):
     return {"value": done / el, "unit": UNIT, "cores": threads, "kind": "reference",
             "sample": f"{done} random pixels spread over the {len(scenes)} frames of {workload}, "
                       f"{el:.1f} s wall on {threads} threads (oracle/_ref: reference kerrPotentials)"}
+
+
+def cpu_reference_rt(inp: dict, budget_s: float, seed: int = 7):
+    """Time the CPU restatement of the transfer (oracle rt_oracle.hpp: FP64
+    DP45 ray, the reference's synchrotron / Planck / rteStep physics) on a
+    bounded random sample of the frame's pixels, all host threads."""
+    from oracle.pyoracle import Oracle, default_threads
+
+    o = Oracle()
+    threads = default_threads()
+    s = inp["scene"]
+    n = s.width * s.height
+    rng = np.random.default_rng(seed)
+    done = 0
+    chunk = max(32, 2 * threads)
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < budget_s:
+        pix = rng.integers(0, n, chunk)
+        p = inp["rt"]
+        o.trace_rt(s, inp["cells"], (2.0, 50.0), inp["lut"], inp["log_theta"], inp["log_x"], p.nu_hz, p.length_cm,
+                   p.ds_max, p.min_transmit, pix=pix, threads=threads)
+        done += chunk
+    el = time.perf_counter() - t0
+    return {"value": done / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{done} random pixels of the {s.width}x{s.height} transfer frame, {el:.1f} s wall on "
+                      f"{threads} threads (oracle: FP64 restatement of the transfer)"}
 
 
 def main():
@@ -596,7 +680,7 @@ def main():
                        "medium": "128x64x64 (log r 2..50 M, theta, phi) FP32 grid: Gaussian torus r_in 6, r_peak 12 "
                                  "x exp(GRF sigma 0.5, correlation 2 M)",
                        "emission": "thermal synchrotron, 256x256 FP32 table over (log Theta_e, log nu/nu_s), "
-                                   "Kirchhoff absorption", "precision": "fp64",
+                                   "Kirchhoff absorption", "precision": args.precision,
                        "launch": "one persistent launch per step"})
     if wl.get("surrogate"):
         config.update({"spin": 0.9, "theta_obs_deg": 60.0, "method": "mixed precision + learned surrogate",
@@ -632,11 +716,14 @@ def main():
     else:
         res = run_ours(args, rank, world, dist)
     if rank == 0:
-        cb = cpu_reference(args.workload, args.cpu_budget) if (world == 1 and args.cpu_budget > 0) else None
+        cb = None
+        if world == 1 and args.cpu_budget > 0:
+            cb = cpu_reference_rt(res["cpu_inputs"], args.cpu_budget) if wl.get("rt") else \
+                cpu_reference(args.workload, args.cpu_budget)
         line = {"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None,
-                "dtype": "bf16+f32+f64" if wl.get("surrogate") else ("f64" if (args.precision == "fp64" or wl.get("rt")) else "f32+f64"),
+                "dtype": "bf16+f32+f64" if wl.get("surrogate") else ("f64" if args.precision == "fp64" else "f32+f64"),
                 "data": "synthetic", "config": config, "precision": args.precision,
                 "steps_per_s": res["total_steps"] * args.steps * world / (res["ms_per_step"] * args.steps * 1e-3),
                 **res["extra"],

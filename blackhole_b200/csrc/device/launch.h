@@ -41,6 +41,9 @@ typedef struct BhkImageOut {
   int32_t *cls, *steps, *n_cross;
   double *r_hit, *phi_hit, *g;  // [max_cross][n]
   double *flux, *intensity, *theta_inf, *phi_inf;
+  // mixed tracer only: unit direction of motion of escaped rays, [3][n]
+  // Cartesian (x, y, z) with x toward the observer's azimuth (zero if not escaped)
+  float *esc_dir;
 } BhkImageOut;
 
 typedef struct BhkLaunch {
@@ -136,6 +139,9 @@ typedef struct BhkRtParams {
   double nu, length_cm, ds_max, min_transmit;
 } BhkRtParams;
 
+// The same on the mixed-precision tracer with FP32 samples (trace_image_mixed.cu).
+int bhk_trace_rt_mixed(const BhkImageParams *p, const BhkRtParams *q, double *i_nu, double *tau, int32_t *cls,
+                       int32_t *steps, unsigned long long *work_counter, void *stream);
 int bhk_trace_rt_fp64(const BhkImageParams *p, const BhkRtParams *q, double *i_nu, double *tau, int32_t *cls,
                       int32_t *steps, unsigned long long *work_counter, int grid, int block, void *stream);
 
@@ -150,6 +156,52 @@ int bhk_sky_fill(uint16_t *tex, int size, uint64_t seed, const long long *star_i
                  int n_stars, void *stream);
 
 // FMA-throughput probe (probe.cu).
+// A camera at finite distance (the reference renderer's camera model, in M
+// units): pixel (px, py) looks along d = normalize(-u right - v up + fwd),
+// u = (2 (px + 1/2) / width - 1) fov aspect + shift_x, v likewise with
+// height and shift_y; the ray is the past-directed null geodesic whose
+// direction in the camera's locally non-rotating frame is d.
+typedef struct BhkCamera {
+  double right[3], up[3], fwd[3];
+  double fov, aspect, shift_x, shift_y;
+  double r0, u0;      // camera radius [M] and cos(theta)
+  double cphi, sphi;  // camera azimuth: cos, sin (the outputs' azimuths are relative to it)
+  int32_t width, height;
+} BhkCamera;
+
+// Traces every pixel of a camera with the mixed tracer (p: spin, horizon,
+// escape and disk radii, integrator, tolerances; p.r_obs = cam.r0, Carter
+// potentials).
+int bhk_trace_camera_mixed(const BhkImageParams *p, const BhkCamera *cam, const BhkImageOut *o,
+                           unsigned long long *work_counter, BhkLaunch L, void *stream);
+int bhk_trace_camera_mixed_occupancy(int block, int *blocks_per_sm);
+
+// Positions (x, y, z) [M] after every FP64 RK4 step of image-plane rays, up
+// to max_points per ray (initial point included): xyz [n][max_points][3],
+// counts [n].
+int bhk_trace_paths_fp64(const BhkImageParams *p, float *xyz, int32_t *counts, int max_points, void *stream);
+
+// Legacy RGBA shading (legacy.cu).
+typedef struct BhkShade {
+  int64_t n;
+  int32_t width;
+  int32_t redshift_enabled, background_enabled, use_luts;
+  float adisk_lit, background_intensity;
+  float t_peak;          // disk temperature at the flux peak [K]
+  float lut_r_min, lut_r_max, spec_r_min, spec_r_max;  // table domains in r / rs = r [M] / 2
+  float cphi, sphi;      // camera azimuth (rotates escape directions into the world frame)
+  unsigned long long tex_emissivity, tex_spectral, tex_galaxy, tex_equirect;
+  float exposure;        // > 0: exposure then ACES tone map; 0: linear output
+  float pad;
+} BhkShade;
+int bhk_legacy_set_blackbody(const float *rgb_table, int n, float log2_t0, float log2_t1);
+int bhk_legacy_shade(const BhkShade *s, const int32_t *cls, const double *r_hit, const double *g, const double *flux,
+                     const float *esc_dir, float *rgba, void *stream);
+int bhk_legacy_lensing(int64_t n, const int32_t *cls, const double *r_hit, const double *g, float *rgba,
+                       void *stream);
+int bhk_legacy_disk_texture(double a, double r_isco, double r_out, double nt_flux_peak, double incl, float t_peak,
+                            int width, int height, float *rgba, void *stream);
+
 int bhk_fma_probe(int fp64, int iters, int repeats, double *tflops);
 
 // Last CUDA error string of the device layer (thread-local).

@@ -124,3 +124,138 @@ __device__ __forceinline__ void synchrotron(const BhkRtParams &q, double n, doub
 }
 
 }  // namespace bhrt
+
+// ---- FP32 variants (the mixed-precision transfer) ------------------------------
+//
+// The same physics in FP32 with the emission and the source function carried
+// as logarithms: ln j = ln n_e + ln nu_B + J (J the table value), Kirchhoff
+// alpha = j / B_nu, so the observed source function g^3 B_nu and the
+// observed opacity alpha / g never leave the FP32 exponent range (j itself
+// reaches 1e-40 and below, under FP32's normal range).
+
+namespace bhrt {
+
+struct MediumF {
+  const float4 *cells;
+  const float *lut;
+  int n_r, n_th, n_ph, n_lt, n_lx;
+  float r_min, r_max, fr_scale;  // (n_r - 1) / log(r_max / r_min)
+  float lt0, lt_scale, lx0, lx1, lx_scale;
+  float ln_nu, ln_len, ds_max, min_transmit;
+  float x_coef;        // h nu / (m_e c^2): x = x_coef / (g Theta_e)
+  float ln_nub_gauss;  // ln(e / (2 pi m_e c)): ln nu_B per ln gauss
+  float ln_2h_c2;      // ln(2 h / c^2)
+};
+
+__host__ __device__ inline MediumF medium_f(const BhkRtParams &q) {
+  MediumF m;
+  m.cells = reinterpret_cast<const float4 *>(q.cells);
+  m.lut = q.lut;
+  m.n_r = q.n_r;
+  m.n_th = q.n_th;
+  m.n_ph = q.n_ph;
+  m.n_lt = q.n_lt;
+  m.n_lx = q.n_lx;
+  m.r_min = (float)q.r_min;
+  m.r_max = (float)q.r_max;
+  m.fr_scale = (float)(q.inv_log_range * (double)(q.n_r - 1));
+  m.lt0 = (float)q.lt0;
+  m.lt_scale = (float)((double)(q.n_lt - 1) / (q.lt1 - q.lt0));
+  m.lx0 = (float)q.lx0;
+  m.lx1 = (float)q.lx1;
+  m.lx_scale = (float)((double)(q.n_lx - 1) / (q.lx1 - q.lx0));
+  m.ln_nu = (float)log(q.nu);
+  m.ln_len = (float)log(q.length_cm);
+  m.ds_max = (float)q.ds_max;
+  m.min_transmit = (float)q.min_transmit;
+  m.x_coef = (float)(kH * q.nu / (kMe * kC * kC));
+  m.ln_nub_gauss = (float)log(kE / (kTwoPi * kMe * kC));
+  m.ln_2h_c2 = (float)log(2.0 * kH / (kC * kC));
+  return m;
+}
+
+#ifdef __CUDACC__
+__device__ __forceinline__ bool sample_f(const MediumF &q, float r, float u, float phi, float &n, float &th,
+                                         float &b) {
+  if (!(r >= q.r_min && r <= q.r_max)) return false;
+  const float fr = __logf(r / q.r_min) * q.fr_scale;
+  const int i0 = min(max((int)floorf(fr), 0), q.n_r - 2);
+  const float tr = fminf(fmaxf(fr - (float)i0, 0.0f), 1.0f);
+  const float theta = acosf(fminf(fmaxf(u, -1.0f), 1.0f));
+  const float ft = theta * (0.31830988618f * (float)q.n_th) - 0.5f;
+  const int j0 = min(max((int)floorf(ft), 0), q.n_th - 2);
+  const float tt = fminf(fmaxf(ft - (float)j0, 0.0f), 1.0f);
+  const float fp = phi * (0.15915494309f * (float)q.n_ph);
+  const float fl = floorf(fp);
+  const float tp = fp - fl;
+  int k0 = (int)fmodf(fl, (float)q.n_ph);
+  if (k0 < 0) k0 += q.n_ph;
+  const int k1 = (k0 + 1 == q.n_ph) ? 0 : k0 + 1;
+  float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
+#pragma unroll
+  for (int di = 0; di < 2; ++di)
+#pragma unroll
+    for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+      for (int dk = 0; dk < 2; ++dk) {
+        const float w = (di ? tr : 1.0f - tr) * (dj ? tt : 1.0f - tt) * (dk ? tp : 1.0f - tp);
+        const float4 v = __ldg(q.cells + ((long long)(i0 + di) * q.n_th + (j0 + dj)) * q.n_ph + (dk ? k1 : k0));
+        a0 = fmaf(w, v.x, a0);
+        a1 = fmaf(w, v.y, a1);
+        a2 = fmaf(w, v.z, a2);
+      }
+  n = a0;
+  th = a1;
+  b = a2;
+  return true;
+}
+
+// FP32 redshift of the circular-orbit emitter (see redshift above).
+__device__ __forceinline__ float redshift_f(float a, float r, float u, float lam) {
+  const float u2 = u * u;
+  const float s2 = (1.0f - u) * (1.0f + u);
+  const float sig = fmaf(r, r, a * a * u2);
+  const float delta = fmaf(r, r - 2.0f, a * a);
+  const float rr = fmaf(r, r, a * a);
+  const float A = fmaf(rr, rr, -a * a * delta * s2);
+  const float om = 1.0f / fmaf(r, sqrtf(r), a);
+  const float inv_sig = 1.0f / sig;
+  const float gtt = -(1.0f - 2.0f * r * inv_sig);
+  const float gtp = -2.0f * a * r * s2 * inv_sig;
+  const float gpp = A * s2 * inv_sig;
+  const float norm = -(gtt + om * fmaf(gpp, om, 2.0f * gtp));
+  if (!(norm > 0.0f)) return 0.0f;
+  const float den = (1.0f - om * lam) * rsqrtf(norm);
+  return den > 0.0f ? 1.0f / den : 0.0f;
+}
+
+// ln(j_obs) - ln(S_obs) and ln(S_obs) of one sample: S_obs = g^3 B_nu(nu/g),
+// alpha_obs = (j / B_nu) / g. Returns false where there is no emission.
+__device__ __forceinline__ bool ln_emission_f(const MediumF &q, float n, float theta_e, float b, float g,
+                                              float &ln_alpha_obs, float &ln_s_obs) {
+  if (!(n > 0.0f && theta_e > 0.0f && b > 0.0f && g > 0.0f)) return false;
+  const float ln_g = __logf(g);
+  const float ln_nu_e = q.ln_nu - ln_g;
+  const float ln_nub = __logf(b) + q.ln_nub_gauss;
+  const float lt = __logf(theta_e);
+  const float lx = ln_nu_e - 0.40546511f - ln_nub - 2.0f * lt;  // ln(nu_e / nu_s), nu_s = 3/2 nu_B Theta^2
+  if (lx > q.lx1) return false;
+  const float ft = fminf(fmaxf((lt - q.lt0) * q.lt_scale, 0.0f), (float)(q.n_lt - 1));
+  const float fx = fminf(fmaxf((lx - q.lx0) * q.lx_scale, 0.0f), (float)(q.n_lx - 1));
+  const int i0 = min((int)ft, q.n_lt - 2), k0 = min((int)fx, q.n_lx - 2);
+  const float ti = ft - (float)i0, tk = fx - (float)k0;
+  const float *L = q.lut + i0 * q.n_lx + k0;
+  const float J = (1.0f - ti) * fmaf(tk, __ldg(L + 1) - __ldg(L), __ldg(L)) +
+                  ti * fmaf(tk, __ldg(L + q.n_lx + 1) - __ldg(L + q.n_lx), __ldg(L + q.n_lx));
+  const float ln_j = __logf(n) + ln_nub + J;
+  // ln B_nu(nu_e, T) = ln(2 h / c^2) + 3 ln nu_e - ln(e^x - 1), x = h nu_e / (k T) = x_coef / (g Theta_e)
+  const float x = __fdividef(q.x_coef, g * theta_e);
+  const float ln_em1 = x > 20.0f ? x : __logf(expm1f(x));
+  const float ln_bnu = q.ln_2h_c2 + 3.0f * ln_nu_e - ln_em1;
+  ln_alpha_obs = ln_j - ln_bnu - ln_g;
+  ln_s_obs = 3.0f * ln_g + ln_bnu;
+  return true;
+}
+#endif
+
+}  // namespace bhrt

@@ -408,3 +408,47 @@ extern "C" int bhk_trace_rt_fp64(const BhkImageParams *p, const BhkRtParams *q, 
   if (e != cudaSuccess) return set_err(e, "k_trace_rt_fp64 launch");
   return 0;
 }
+
+namespace bhk {
+
+// Paths of image-plane rays (the Blender bridge's geodesic export): one
+// thread per ray, classical RK4 with the image tracer's affine step rule,
+// the position written before the first step and after every step until the
+// ray reaches the horizon or escape radius or max_points are written.
+__global__ void __launch_bounds__(128) k_trace_paths_fp64(const __grid_constant__ BhkImageParams p,
+                                                          float *__restrict__ xyz, int32_t *__restrict__ counts,
+                                                          int max_points) {
+  const long long pix = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (pix >= p.n_pix) return;
+  RayFp64 R;
+  init_ray(p, pix, R);
+  float *out = xyz + pix * (long long)max_points * 3;
+  int n = 0;
+  for (;;) {
+    const double s = sqrt(dmax_(0.0, (1.0 - R.y.u) * (1.0 + R.y.u)));
+    const double ph = phi_of_psi(R.y.phi, R.y.r, p);
+    out[3 * n + 0] = (float)(R.y.r * s * cos(ph));
+    out[3 * n + 1] = (float)(R.y.r * s * sin(ph));
+    out[3 * n + 2] = (float)(R.y.r * R.y.u);
+    ++n;
+    if (n >= max_points || R.y.r <= p.r_hor || R.y.r >= p.r_esc) break;
+    const double hh = p.step_coeff * dmin_(R.y.r, p.step_rcap);
+    const double h = hh / ((R.y.r * R.y.r) + ((p.a2 * R.y.u) * R.y.u));
+    R.y = rk4(R.y, h, R.c, rhs(R.y, R.c));
+    project(R.y, R.c);
+  }
+  counts[pix] = n;
+}
+
+}  // namespace bhk
+
+extern "C" int bhk_trace_paths_fp64(const BhkImageParams *p, float *xyz, int32_t *counts, int max_points,
+                                    void *stream) {
+  if (p->n_pix <= 0) return 0;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const long long blocks = (p->n_pix + 127) / 128;
+  bhk::k_trace_paths_fp64<<<(unsigned)blocks, 128, 0, s>>>(*p, xyz, counts, max_points);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(e, "k_trace_paths_fp64 launch");
+  return 0;
+}

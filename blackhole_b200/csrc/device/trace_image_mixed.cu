@@ -26,6 +26,7 @@
 #include "hermite.cuh"
 #include "image_mixed.cuh"
 #include "launch.h"
+#include "rt.cuh"
 
 namespace bhm {
 
@@ -98,6 +99,84 @@ __device__ __forceinline__ void init_ray(const BhkImageParams &p, long long pix,
   R.k1 = rhs(R.y, R.c);
 }
 
+// A ray of a camera at finite distance (BhkCamera): the pixel's direction d
+// in the world frame, taken as the direction in the camera's locally
+// non-rotating frame (Bardeen, Press & Teukolsky 1972) at (r0, theta0). The
+// photon the pixel sees arrives moving along -d; with the frame's lapse
+// alpha_L = sqrt(Sigma Delta / A), rotation omega = 2 a r / A and cylindrical
+// radius varpi = sqrt(A / Sigma) sin(theta) its constants per unit energy are
+//   lambda = varpi v_phi / (alpha_L + omega varpi v_phi),
+//   Theta(theta0) = (sqrt(Sigma) v_theta / (alpha_L + omega varpi v_phi))^2,
+// v = -d in the (r, theta, phi) frame; eta = Theta - a^2 cos^2 + lambda^2 cot^2
+// (textbook Carter potentials: q_R = eta, q_Th = eta + lambda^2). The traced
+// (past-directed) ray moves along d: p_r has the sign of d_r, p_u the sign of
+// -d_theta. Azimuths are measured from the camera's.
+__device__ __forceinline__ void init_ray_camera(const BhkImageParams &p, const BhkCamera &cam, long long pix,
+                                                RayMx &R) {
+  const long long i = pix % cam.width, j = pix / cam.width;
+  const double uu = (2.0 * ((double)i + 0.5) / (double)cam.width - 1.0) * cam.fov * cam.aspect + cam.shift_x;
+  const double vv = (2.0 * ((double)j + 0.5) / (double)cam.height - 1.0) * cam.fov + cam.shift_y;
+  double d[3];
+  for (int k = 0; k < 3; ++k) d[k] = -uu * cam.right[k] - vv * cam.up[k] + cam.fwd[k];
+  const double dn = 1.0 / sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  for (int k = 0; k < 3; ++k) d[k] *= dn;
+  // local spherical frame at the camera (azimuth phi0 = 0 after rotating by the camera's azimuth)
+  const double u0 = cam.u0, s0 = sqrt(fmax(0.0, (1.0 - u0) * (1.0 + u0)));
+  const double dx = cam.cphi * d[0] + cam.sphi * d[1], dy = -cam.sphi * d[0] + cam.cphi * d[1], dz = d[2];
+  const double n_r = s0 * dx + u0 * dz;
+  const double n_th = u0 * dx - s0 * dz;
+  const double n_ph = dy;
+  const double a = p.a, a2 = p.a2, r = cam.r0;
+  const double sig = r * r + a2 * u0 * u0;
+  const double del = r * r - 2.0 * r + a2;
+  const double AA = (r * r + a2) * (r * r + a2) - a2 * del * s0 * s0;
+  const double lapse = sqrt(sig * del / AA);
+  const double omega = 2.0 * a * r / AA;
+  const double varpi = sqrt(AA / sig) * s0;
+  const double v_ph = -n_ph, v_th = -n_th;
+  const double e = lapse + omega * varpi * v_ph;  // E / E_local
+  const double lam = varpi * v_ph / e;
+  const double pth = sqrt(sig) * v_th / e;
+  const double cot2 = s0 > 1e-12 ? (u0 * u0) / (s0 * s0) : 0.0;
+  const double eta = pth * pth - a2 * u0 * u0 + lam * lam * cot2;
+  const double qTh = eta + lam * lam;
+  const double K = eta + (lam - a) * (lam - a);
+  const double A = r * r + a2 - a * lam;
+  const double Rv = A * A - del * K;
+  const double Uv = (qTh + a2 * u0 * u0) * (1.0 - u0 * u0) - lam * lam;
+  R.c.a = (float)a;
+  R.c.a2 = (float)a2;
+  R.c.lam = (float)lam;
+  R.c.qTh = (float)qTh;
+  R.c.K = (float)K;
+  R.c.a2_minus_alam = (float)(a2 - a * lam);
+  R.c.c_pu = (float)(a2 - qTh);
+  R.cd.a = a;
+  R.cd.lam = lam;
+  R.cd.qTh = qTh;
+  R.cd.K = K;
+  split(r, R.y.r, R.lo.r);
+  split(u0, R.y.u, R.lo.u);
+  R.y.phi = 0.0f;
+  R.lo.phi = 0.0f;
+  const double mr = sqrt(Rv < 0.0 ? 0.0 : Rv), mu = sqrt(Uv < 0.0 ? 0.0 : Uv);
+  R.y.pr = (float)(n_r < 0.0 ? -mr : mr);
+  R.y.pu = (float)(n_th > 0.0 ? -mu : mu);
+  R.inten = 0.0;
+  R.pix = pix;
+  R.steps = 0;
+  R.attempts = 0;
+  R.ncross = 0;
+  R.r_hor = (float)p.r_hor;
+  R.r_esc = (float)p.r_esc;
+  R.rtol = (float)p.rtol;
+  R.atol = (float)p.atol;
+  project(R.y, R.lo, R.cd);
+  const float hh = (float)p.step_coeff * fminf(R.y.r, (float)p.step_rcap);
+  R.h = hh / fmaf(R.c.a2 * R.y.u, R.y.u, R.y.r * R.y.r);
+  R.k1 = rhs(R.y, R.c);
+}
+
 // phi = psi + a (G(r) - G(r_obs)) at the outputs (image_fp64.cuh).
 __device__ __forceinline__ double phi_of_psi(double psi, double r, const BhkImageParams &p) {
   if (p.a == 0.0) return psi;
@@ -150,17 +229,31 @@ __device__ __forceinline__ void finish(const BhkImageParams &p, const BhkImageOu
     if (o.g) o.g[off] = 0.0;
   }
   double th = 0.0, ph = 0.0, inten = R.inten;
+  float dir[3] = {0.0f, 0.0f, 0.0f};
   if (cls == 2) {
     const double u = to_f64(R.y.u, R.lo.u);
     th = acos(fmin(1.0, fmax(-1.0, u)));
     ph = phi_of_psi(to_f64(R.y.phi, R.lo.phi), to_f64(R.y.r, R.lo.r), p);
-    if (p.sky) {  // dphi/dtau = dpsi/dtau + a p_r / Delta  (phi = psi + a G(r), G' = 1 / Delta)
+    if (p.sky || o.esc_dir) {  // dphi/dtau = dpsi/dtau + a p_r / Delta  (phi = psi + a G(r), G' = 1 / Delta)
       const Yf k = rhs(R.y, R.c);
       const double r = to_f64(R.y.r, R.lo.r);
       const double delta = r * r - 2.0 * r + p.a2;
       const double dphi = (double)k.phi + p.a * (double)R.y.pr / delta;
-      inten += bhsky::radiance(p.sky, p.sky_size, r, u, ph, (double)R.y.pr, (double)R.y.pu, dphi);
+      if (p.sky) inten += bhsky::radiance(p.sky, p.sky_size, r, u, ph, (double)R.y.pr, (double)R.y.pu, dphi);
+      double x, y, z;
+      bhsky::direction_of_motion(r, u, ph, (double)R.y.pr, (double)R.y.pu, dphi, x, y, z);
+      const double nn = sqrt(x * x + y * y + z * z);
+      if (nn > 0.0) {
+        dir[0] = (float)(x / nn);
+        dir[1] = (float)(y / nn);
+        dir[2] = (float)(z / nn);
+      }
     }
+  }
+  if (o.esc_dir) {
+    o.esc_dir[pix] = dir[0];
+    o.esc_dir[p.n_pix + pix] = dir[1];
+    o.esc_dir[2 * p.n_pix + pix] = dir[2];
   }
   if (o.intensity) o.intensity[pix] = inten;
   if (o.theta_inf) o.theta_inf[pix] = th;
@@ -231,6 +324,30 @@ __device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOu
   }
 }
 
+// The pixels of one camera frame.
+struct CameraSrc {
+  const BhkImageParams &p;
+  const BhkCamera &cam;
+  const BhkImageOut &o;
+  __device__ __forceinline__ long long total() const { return p.n_pix; }
+  __device__ __forceinline__ int frame_of(long long w, long long &pix) const {
+    pix = w;
+    return 0;
+  }
+  __device__ __forceinline__ const BhkImageParams &params(int) const { return p; }
+  __device__ __forceinline__ const BhkImageOut &out(int) const { return o; }
+  __device__ __forceinline__ void pixel_done(int) const {}
+};
+
+// A ray's initial state: image-plane pixels for every source but the camera.
+template <class Src>
+__device__ __forceinline__ void init_from(const Src &src, int f, long long pix, RayMx &R) {
+  init_ray(src.params(f), pix, R);
+}
+__device__ __forceinline__ void init_from(const CameraSrc &src, int, long long pix, RayMx &R) {
+  init_ray_camera(src.p, src.cam, pix, R);
+}
+
 // The persistent loop shared by the single-frame and batch kernels (see
 // trace_image_fp64.cu).
 template <int INTEG, class Src>
@@ -253,7 +370,7 @@ __device__ __forceinline__ void trace_loop(const Src &src, unsigned long long *_
         if (mine < total) {
           long long pix;
           const int f = src.frame_of((long long)mine, pix);
-          init_ray(src.params(f), pix, R);
+          init_from(src, f, pix, R);
           R.f = f;
           active = true;
         } else {
@@ -292,6 +409,13 @@ __global__ void __launch_bounds__(128) k_trace_list_mixed(const __grid_constant_
   trace_loop<INTEG>(bhsrc::ListSrc{p, o, list, count}, counter, refill);
 }
 
+__global__ void __launch_bounds__(128) k_trace_camera_mixed(const __grid_constant__ BhkImageParams p,
+                                                            const __grid_constant__ BhkCamera cam,
+                                                            const __grid_constant__ BhkImageOut o,
+                                                            unsigned long long *__restrict__ counter, int refill) {
+  trace_loop<1>(CameraSrc{p, cam, o}, counter, refill);
+}
+
 template <int INTEG>
 __global__ void __launch_bounds__(128) k_trace_batch_mixed(const __grid_constant__ BhkBatchDev b,
                                                            unsigned long long *__restrict__ counter, int refill) {
@@ -299,7 +423,130 @@ __global__ void __launch_bounds__(128) k_trace_batch_mixed(const __grid_constant
   trace_loop<INTEG>(bhsrc::BatchSrc{b}, counter, refill);
 }
 
+// ---- along-ray transfer on the mixed tracer ---------------------------------------
+//
+// The FP64 transfer kernel (trace_image_fp64.cu, k_trace_rt_fp64) with the
+// geodesic from the mixed tracer and every sample in FP32 (rt.cuh, FP32
+// variants): positions by cubic Hermite interpolation of the accepted step,
+// at most ds_max apart in affine length; intensity and optical depth summed
+// in FP64.
+__device__ __forceinline__ void rt_segment_f(const BhkImageParams &p, const bhrt::MediumF &q, const RayCf &c,
+                                             const Yf &y0, const Yf &k0, const Yf &y1, const Yf &k1, float h,
+                                             double &I, float &T, double &tau) {
+  const float a2 = c.a2;
+  const float rm = fmaf(0.125f * h, k0.r - k1.r, 0.5f * (y0.r + y1.r));
+  const float um = fmaf(0.125f * h, k0.u - k1.u, 0.5f * (y0.u + y1.u));
+  const float sig_m = fmaf(rm, rm, a2 * um * um);
+  const float ns = fminf(fmaxf(ceilf(__fdividef(sig_m * h, q.ds_max)), 1.0f), 64.0f);
+  const int nsub = (int)ns;
+  const float dt = __fdividef(h, ns);
+  const float rp = (float)p.r_plus, rmn = (float)p.r_minus, ro = (float)p.r_obs;
+  const float gscale = c.a == 0.0f ? 0.0f : __fdividef(c.a, rp - rmn);
+  const float g_obs = __fdividef(ro - rmn, ro - rp);
+  for (int m = 0; m < nsub; ++m) {
+    const float t = __fdividef((float)m + 0.5f, ns);
+    const float t2 = t * t, t3 = t2 * t;
+    const float h00 = 2.0f * t3 - 3.0f * t2 + 1.0f, h10 = t3 - 2.0f * t2 + t;
+    const float h01 = -2.0f * t3 + 3.0f * t2, h11 = t3 - t2;
+    const float r = h00 * y0.r + h10 * h * k0.r + h01 * y1.r + h11 * h * k1.r;
+    const float u = h00 * y0.u + h10 * h * k0.u + h01 * y1.u + h11 * h * k1.u;
+    const float psi = h00 * y0.phi + h10 * h * k0.phi + h01 * y1.phi + h11 * h * k1.phi;
+    const float phi = psi + gscale * __logf(__fdividef(r - rp, r - rmn) * g_obs);  // phi = psi + a (G(r) - G(r_obs))
+    float n, th, b;
+    if (!bhrt::sample_f(q, r, u, phi, n, th, b)) continue;
+    const float g = bhrt::redshift_f(c.a, r, u, c.lam);
+    float ln_alpha, ln_s;
+    if (!bhrt::ln_emission_f(q, n, th, b, g, ln_alpha, ln_s)) continue;
+    const float dl = fmaf(r, r, a2 * u * u) * dt;  // affine length of the sample, M
+    const float ts = __expf(ln_alpha + __logf(dl) + q.ln_len);
+    const float om = ts < 1.0e-4f ? ts * (1.0f - 0.5f * ts) : -expm1f(-ts);
+    I += (double)(T * __expf(ln_s) * om);
+    T *= 1.0f - om;
+    tau += (double)ts;
+  }
+}
+
+__global__ void __launch_bounds__(128) k_trace_rt_mixed(const __grid_constant__ BhkImageParams p,
+                                                        const __grid_constant__ bhrt::MediumF q,
+                                                        double *__restrict__ i_nu, double *__restrict__ tau_out,
+                                                        int *__restrict__ cls_out, int *__restrict__ steps_out,
+                                                        unsigned long long *__restrict__ counter) {
+  const unsigned lane = threadIdx.x & 31u;
+  for (;;) {
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(counter, 32ull);
+    base = __shfl_sync(kFull, base, 0);
+    if (base >= (unsigned long long)p.n_pix) break;
+    const long long pix = (long long)base + lane;
+    if (pix >= p.n_pix) continue;
+    RayMx R;
+    init_ray(p, pix, R);
+    double I = 0.0, tau = 0.0;
+    float T = 1.0f;
+    int cls = 3;
+    const long long max_attempts = 4LL * p.max_steps + 64;
+    for (;;) {
+      if (R.steps >= p.max_steps || R.attempts >= max_attempts) {
+        cls = 3;
+        break;
+      }
+      if (R.y.r <= R.r_hor) {
+        cls = 0;
+        break;
+      }
+      if (R.y.r >= R.r_esc) {
+        cls = 2;
+        break;
+      }
+      ++R.attempts;
+      const float h = R.h;
+      const DPf d = dp45(R.y, h, R.c, R.k1, R.rtol, R.atol, true);
+      if (d.err <= 1.0f) {
+        ++R.steps;
+        const Yf y0 = R.y, k0 = R.k1;
+        comp_add(R.y.r, R.lo.r, d.d.r);
+        comp_add(R.y.u, R.lo.u, d.d.u);
+        comp_add(R.y.phi, R.lo.phi, d.d.phi);
+        R.y.pr += d.d.pr;
+        R.y.pu += d.d.pu;
+        rt_segment_f(p, q, R.c, y0, k0, R.y, d.k7, h, I, T, tau);
+        project(R.y, R.lo, R.cd);
+        R.k1 = d.k7;
+        R.k1.r = R.y.pr;
+        R.k1.u = R.y.pu;
+        R.h = h * step_factor(d.err, true);
+        if (T < q.min_transmit) {
+          cls = 4;
+          break;
+        }
+      } else {
+        R.h = h * step_factor(d.err, false);
+      }
+    }
+    if (i_nu) i_nu[pix] = I;
+    if (tau_out) tau_out[pix] = tau;
+    if (cls_out) cls_out[pix] = cls;
+    if (steps_out) steps_out[pix] = R.steps;
+  }
+}
+
 }  // namespace bhm
+
+extern "C" int bhk_trace_rt_mixed(const BhkImageParams *p, const BhkRtParams *q, double *i_nu, double *tau,
+                                  int32_t *cls, int32_t *steps, unsigned long long *counter, void *stream) {
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s) != cudaSuccess) return -1;
+  int dev = 0, sms = 0, per_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bhm::k_trace_rt_mixed, 128, 0) != cudaSuccess)
+    return -1;
+  const long long need = (p->n_pix + 127) / 128;
+  const int grid = (int)(need < (long long)sms * per_sm ? need : (long long)sms * per_sm);
+  const bhrt::MediumF m = bhrt::medium_f(*q);
+  bhm::k_trace_rt_mixed<<<grid > 0 ? grid : 1, 128, 0, s>>>(*p, m, i_nu, tau, cls, steps, counter);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
 
 extern "C" int bhk_trace_image_mixed(const BhkImageParams *p, const BhkImageOut *o, unsigned long long *counter,
                                      BhkLaunch launch, void *stream) {
@@ -330,6 +577,21 @@ extern "C" int bhk_trace_list_mixed(const BhkImageParams *p, const BhkImageOut *
   else
     bhm::k_trace_list_mixed<1><<<L.grid, L.block, 0, s>>>(*p, *o, list, count, counter, L.refill);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+extern "C" int bhk_trace_camera_mixed(const BhkImageParams *p, const BhkCamera *cam, const BhkImageOut *o,
+                                      unsigned long long *counter, BhkLaunch L, void *stream) {
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s) != cudaSuccess) return -1;
+  bhm::k_trace_camera_mixed<<<L.grid, L.block, 0, s>>>(*p, *cam, *o, counter, L.refill);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+extern "C" int bhk_trace_camera_mixed_occupancy(int block, int *blocks_per_sm) {
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhm::k_trace_camera_mixed, block, 0) ==
+                 cudaSuccess
+             ? 0
+             : -1;
 }
 
 extern "C" int bhk_trace_batch_mixed(const BhkBatchDev *b, int integrator, unsigned long long *counter, BhkLaunch L,

@@ -116,7 +116,8 @@ int bh_kerr_trace_rt(const BH_KerrScene *scene, const BH_GrmhdGrid *grid, const 
   if (rt) r = *rt;
   if (!(r.nu_hz > 0.0 && r.length_cm > 0.0 && r.ds_max > 0.0)) return bhh_fail("bh_kerr_trace_rt: bad transfer parameters");
   BH_KerrScene sc = *scene;
-  sc.precision = BH_PRECISION_FP64;
+  const bool mixed = scene->precision == BH_PRECISION_MIXED;
+  sc.precision = BH_PRECISION_FP64;  // launch shape of the FP64 kernel; the mixed one sizes its own grid
   BhkImageParams p;
   BhkLaunch L;
   if (bhh_prepare_image_launch(&sc, &p, &L) != 0) return -1;
@@ -142,6 +143,11 @@ int bh_kerr_trace_rt(const BH_KerrScene *scene, const BH_GrmhdGrid *grid, const 
   q.min_transmit = r.min_transmit;
   unsigned long long *counter = nullptr;
   if (bhh_work_counter(&counter) != 0) return -1;
+  if (mixed) {
+    if (bhk_trace_rt_mixed(&p, &q, i_nu, tau, cls, steps, counter, stream) != 0)
+      return bhh_fail("bh_kerr_trace_rt: k_trace_rt_mixed launch failed");
+    return 0;
+  }
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

@@ -83,8 +83,13 @@ typedef struct BH_RtParams {
 
 void bh_rt_defaults(BH_RtParams *rt);
 
-/* Trace every pixel of `scene` (DP45 integrator, FP64; the thin disk is
- * ignored) through the medium. Outputs per pixel (device,
+/* Trace every pixel of `scene` (DP45 integrator; the thin disk is ignored)
+ * through the medium. scene->precision BH_PRECISION_FP64: FP64 geodesic and
+ * samples; BH_PRECISION_MIXED: the mixed-precision geodesic (FP32 bulk) and
+ * FP32 samples with the emission carried as logarithms, intensity and depth
+ * summed in FP64 (its accepted steps, hence its sample points, differ from
+ * the FP64 ones: results agree to the sampling's discretization error).
+ * Outputs per pixel (device,
  * NULL = not wanted): I_nu at the observer (erg s^-1 cm^-2 Hz^-1 sr^-1),
  * optical depth along the ray, class (0 captured, 2 escaped, 3 steps
  * exhausted, 4 stopped opaque) and accepted steps. */

@@ -675,14 +675,64 @@ inline void record_crossing(const Scene &s, const SceneDerived<T> &d, const RayC
 // Trace one pixel. Loop order follows raytracer.h:338-365: step budget,
 // horizon test, escape test, step; then the equatorial-crossing test.
 // MakeRhs(c) returns the right-hand-side callable for the ray constants c.
+// A camera at finite distance (the library's legacy renderer): pixel (i, j)
+// looks along d = normalize(-u right - v up + fwd), u = (2 (i + 1/2) / W - 1)
+// fov aspect + shift_x, v = (2 (j + 1/2) / H - 1) fov + shift_y; d is the
+// direction in the locally non-rotating frame (Bardeen, Press & Teukolsky
+// 1972) at the camera (r0, u0 = cos theta0, azimuth 0 after rotating the
+// world by -phi_cam). The photon seen arrives along -d: with lapse
+// alpha_L = sqrt(Sigma Delta / A), omega = 2 a r / A, varpi = sqrt(A / Sigma)
+// sin theta, lambda = varpi v_phi / (alpha_L + omega varpi v_phi) and
+// Theta = (sqrt(Sigma) v_theta / (alpha_L + omega varpi v_phi))^2 for
+// v = -d; eta = Theta - a^2 cos^2 + lambda^2 cot^2 (textbook Carter form).
+struct Camera {
+  double right[3], up[3], fwd[3];
+  double fov, aspect, shift_x, shift_y;
+  double r0, u0, cphi, sphi;
+  int32_t width, height;
+};
+
+inline void init_ray_camera(const SceneDerived<double> &dd, const Camera &cam, int64_t pix, RayConsts<double> &c,
+                            Y<double> &y) {
+  const int64_t i = pix % cam.width, j = pix / cam.width;
+  const double uu = (2.0 * (double(i) + 0.5) / double(cam.width) - 1.0) * cam.fov * cam.aspect + cam.shift_x;
+  const double vv = (2.0 * (double(j) + 0.5) / double(cam.height) - 1.0) * cam.fov + cam.shift_y;
+  double d[3];
+  for (int k = 0; k < 3; ++k) d[k] = -uu * cam.right[k] - vv * cam.up[k] + cam.fwd[k];
+  const double dn = 1.0 / std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  for (double &v : d) v *= dn;
+  const double u0 = cam.u0, s0 = std::sqrt(std::max(0.0, (1.0 - u0) * (1.0 + u0)));
+  const double dx = cam.cphi * d[0] + cam.sphi * d[1], dy = -cam.sphi * d[0] + cam.cphi * d[1], dz = d[2];
+  const double n_r = s0 * dx + u0 * dz, n_th = u0 * dx - s0 * dz, n_ph = dy;
+  const double a = dd.a, a2 = a * a, r = cam.r0;
+  const double sig = r * r + a2 * u0 * u0;
+  const double del = r * r - 2.0 * r + a2;
+  const double AA = (r * r + a2) * (r * r + a2) - a2 * del * s0 * s0;
+  const double lapse = std::sqrt(sig * del / AA);
+  const double omega = 2.0 * a * r / AA;
+  const double varpi = std::sqrt(AA / sig) * s0;
+  const double e = lapse + omega * varpi * (-n_ph);
+  c.a = a;
+  c.lam = varpi * (-n_ph) / e;
+  const double pth = std::sqrt(sig) * (-n_th) / e;
+  const double cot2 = s0 > 1e-12 ? (u0 * u0) / (s0 * s0) : 0.0;
+  const double eta = pth * pth - a2 * u0 * u0 + c.lam * c.lam * cot2;
+  c.qTh = eta + c.lam * c.lam;
+  c.qR = eta;
+  c.K = eta + (c.lam - a) * (c.lam - a);
+  y.r = r;
+  y.u = u0;
+  y.phi = 0.0;
+  const double mr = std::sqrt(std::max(pot_R(r, c), 0.0)), mu = std::sqrt(std::max(pot_U(u0, c), 0.0));
+  y.pr = n_r < 0.0 ? -mr : mr;
+  y.pu = n_th > 0.0 ? -mu : mu;
+}
+
 template <class T, class MakeRhs>
-inline PixelResult<T> trace_pixel(const Scene &s, const SceneDerived<T> &d, T alpha, T beta,
-                                  const MakeRhs &make_rhs) {
+inline PixelResult<T> trace_pixel_from(const Scene &s, const SceneDerived<T> &d, const RayConsts<T> &c, Y<T> y,
+                                       const MakeRhs &make_rhs) {
   PixelResult<T> out{};
   out.cls = CLS_MAX_STEPS;
-  RayConsts<T> c;
-  Y<T> y;
-  init_ray(d, s, alpha, beta, c, y);
   const auto f = make_rhs(c);
   // Start on the first integrals too: the projection is then idempotent on
   // any state it has produced, so re-applying it to an unchanged state (a
@@ -759,6 +809,15 @@ inline PixelResult<T> trace_pixel(const Scene &s, const SceneDerived<T> &d, T al
     }
   }
   return out;
+}
+
+template <class T, class MakeRhs>
+inline PixelResult<T> trace_pixel(const Scene &s, const SceneDerived<T> &d, T alpha, T beta,
+                                  const MakeRhs &make_rhs) {
+  RayConsts<T> c;
+  Y<T> y;
+  init_ray(d, s, alpha, beta, c, y);
+  return trace_pixel_from(s, d, c, y, make_rhs);
 }
 
 template <class T> inline PixelResult<T> trace_pixel(const Scene &s, const SceneDerived<T> &d, T alpha, T beta) {

@@ -150,14 +150,20 @@ static int64_t sky_texel(double x, double y, double z, int N) {
 // Direction of motion of the ray at its escape point (the sky point it comes
 // from): the Cartesian velocity of (r, theta, phi) with dr = p_r,
 // du = p_u (u = cos theta) and dphi.
-static double sky_radiance(const uint16_t *tex, int N, double r, double u, double phi, double pr, double pu,
-                           double dphi) {
+static void motion_dir(double r, double u, double phi, double pr, double pu, double dphi, double &x, double &y,
+                       double &z) {
   const double st = std::sqrt((1.0 - u) * (1.0 + u));
   const double cp = std::cos(phi), sp = std::sin(phi);
   const double dst = st > 1e-300 ? -u * pu / st : 0.0;
-  const double x = (pr * st + r * dst) * cp - (r * st * dphi) * sp;
-  const double y = (pr * st + r * dst) * sp + (r * st * dphi) * cp;
-  const double z = pr * u + r * pu;
+  x = (pr * st + r * dst) * cp - (r * st * dphi) * sp;
+  y = (pr * st + r * dst) * sp + (r * st * dphi) * cp;
+  z = pr * u + r * pu;
+}
+
+static double sky_radiance(const uint16_t *tex, int N, double r, double u, double phi, double pr, double pu,
+                           double dphi) {
+  double x, y, z;
+  motion_dir(r, u, phi, pr, pu, dphi, x, y, z);
   const _Float16 h = std::bit_cast<_Float16>(tex[sky_texel(x, y, z, N)]);
   return double(float(h));
 }
@@ -177,6 +183,92 @@ int bho_trace_pixels_sky(const BH_KerrScene *scene, int64_t n, const int64_t *pi
       p.intensity = p.intensity + sky_radiance(sky, sky_size, p.r_end, p.u_inf, p.phi_inf, p.pr_end, p.pu_end,
                                                p.dphi_end);
     store(out, i, n, maxc, p);
+  });
+  return 0;
+}
+
+// Rays of a camera at finite distance (kerr_oracle.hpp Camera; cam_f64 =
+// right[3], up[3], fwd[3], fov, aspect, shift_x, shift_y, r0, u0, cphi, sphi;
+// cam_i32 = width, height). scene: spin, r_obs = r0, escape and disk radii,
+// integrator and tolerances (the camera sets the initial data). esc_dir
+// (3 n, may be NULL): unit direction of motion of escaped rays in the
+// camera-azimuth frame, zero otherwise.
+int bho_trace_camera(const BH_KerrScene *scene, const double *cam_f64, const int32_t *cam_i32, int64_t n,
+                     const int64_t *pix_index, const BH_KerrImageOut *out, double *esc_dir, int threads) {
+  const bho::Scene s = to_scene(scene);
+  const auto d = bho::derive<double>(s);
+  const int maxc = std::max(1, std::min(3, int(s.max_crossings)));
+  bho::Camera cam{};
+  for (int k = 0; k < 3; ++k) {
+    cam.right[k] = cam_f64[k];
+    cam.up[k] = cam_f64[3 + k];
+    cam.fwd[k] = cam_f64[6 + k];
+  }
+  cam.fov = cam_f64[9];
+  cam.aspect = cam_f64[10];
+  cam.shift_x = cam_f64[11];
+  cam.shift_y = cam_f64[12];
+  cam.r0 = cam_f64[13];
+  cam.u0 = cam_f64[14];
+  cam.cphi = cam_f64[15];
+  cam.sphi = cam_f64[16];
+  cam.width = cam_i32[0];
+  cam.height = cam_i32[1];
+  parallel_for(n, threads, [&](int64_t i) {
+    const int64_t pix = pix_index ? pix_index[i] : i;
+    bho::RayConsts<double> c;
+    bho::Y<double> y;
+    bho::init_ray_camera(d, cam, pix, c, y);
+    const auto p = bho::trace_pixel_from<double>(s, d, c, y, [](const bho::RayConsts<double> &cc) {
+      return bho::PolyRhs<double>{cc};
+    });
+    store(out, i, n, maxc, p);
+    if (esc_dir) {
+      double x = 0, yy = 0, z = 0;
+      if (p.cls == 2) {
+        motion_dir(p.r_end, p.u_inf, p.phi_inf, p.pr_end, p.pu_end, p.dphi_end, x, yy, z);
+        const double nn = std::sqrt(x * x + yy * yy + z * z);
+        x /= nn;
+        yy /= nn;
+        z /= nn;
+      }
+      esc_dir[i] = x;
+      esc_dir[n + i] = yy;
+      esc_dir[2 * n + i] = z;
+    }
+  });
+  return 0;
+}
+
+// Paths of image-plane rays at explicit (alpha, beta): the position (x, y, z)
+// before the first step and after every classical RK4 step (affine step
+// step_coeff min(r, step_rcap), Mino step over Sigma, projection after each
+// step) until the horizon or escape radius or max_points; xyz [n][max][3].
+int bho_trace_paths(const BH_KerrScene *scene, int64_t n, const double *alpha, const double *beta, int max_points,
+                    double *xyz, int32_t *counts, int threads) {
+  const bho::Scene s = to_scene(scene);
+  const auto d = bho::derive<double>(s);
+  parallel_for(n, threads, [&](int64_t i) {
+    bho::RayConsts<double> c;
+    bho::Y<double> y;
+    bho::init_ray(d, s, alpha[i], beta[i], c, y);
+    const bho::PolyRhs<double> f{c};
+    f.project(y);
+    double *o = xyz + i * int64_t(max_points) * 3;
+    int m = 0;
+    for (;;) {
+      const double st = std::sqrt(std::max(0.0, (1.0 - y.u) * (1.0 + y.u)));
+      const double ph = bho::phi_of_psi(y.phi, y.r, s.r_obs, d.a, d.r_plus, d.r_minus);
+      o[3 * m + 0] = y.r * st * std::cos(ph);
+      o[3 * m + 1] = y.r * st * std::sin(ph);
+      o[3 * m + 2] = y.r * y.u;
+      ++m;
+      if (m >= max_points || y.r <= d.r_hor || y.r >= d.r_esc) break;
+      const double h = bho::mino_step(s, y, d.a);
+      y = bho::img_rk4(y, h, f, f(y));
+      f.project(y);
+    }
+    counts[i] = m;
   });
   return 0;
 }

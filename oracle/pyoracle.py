@@ -89,6 +89,9 @@ class Oracle(_Base):
         L.bho_trace_pixels_sky.argtypes = [C.POINTER(KerrScene), _i64, _vp, C.POINTER(KerrImageOut), C.c_int, _vp,
                                            C.c_int]
         L.bho_sky_texels.argtypes = [_i64, _vp, _vp, _vp, C.c_int, _vp]
+        L.bho_trace_camera.argtypes = [C.POINTER(KerrScene), _vp, _vp, _i64, _vp, C.POINTER(KerrImageOut), _vp,
+                                       C.c_int]
+        L.bho_trace_paths.argtypes = [C.POINTER(KerrScene), _i64, _vp, _vp, C.c_int, _vp, _vp, C.c_int]
         L.bho_trace_rt.argtypes = ([C.POINTER(KerrScene), _i64, _vp, _vp, C.c_int, C.c_int, C.c_int, _f64, _f64, _vp,
                                     C.c_int, C.c_int] + [_f64] * 8 + [_vp] * 4 + [C.c_int])
         L.bho_rt_path.restype = _f64
@@ -122,6 +125,36 @@ class Oracle(_Base):
         fn = lambda sc, n, idx, o, th: self.lib.bho_trace_pixels_sky(sc, n, idx, o, th, _ptr(sky), size)  # noqa: E731
         n = scene.width * scene.height if pix is None else len(pix)
         return self._trace(fn, scene, pix, n, threads or default_threads())
+
+    def trace_camera(self, scene: KerrScene, cam_f64: np.ndarray, cam_i32: np.ndarray, pix: np.ndarray | None = None,
+                     threads: int | None = None):
+        """Rays of a finite-distance camera (kerr_oracle.hpp Camera): the image
+        outputs plus esc_dir [3][n] (unit escape direction, camera-azimuth frame)."""
+        n = int(cam_i32[0]) * int(cam_i32[1]) if pix is None else len(pix)
+        cf = np.ascontiguousarray(cam_f64, np.float64)
+        ci = np.ascontiguousarray(cam_i32, np.int32)
+        idx = None if pix is None else np.ascontiguousarray(pix, np.int64)
+        maxc = max(1, min(MAX_CROSSINGS, scene.max_crossings))
+        arrs = host_outputs(n, maxc)
+        o = out_struct(arrs)
+        esc = np.zeros((3, n))
+        rc = self.lib.bho_trace_camera(C.byref(scene), _ptr(cf), _ptr(ci), n, _ptr(idx), C.byref(o), _ptr(esc),
+                                       threads or default_threads())
+        if rc != 0:
+            raise RuntimeError("oracle camera trace failed")
+        arrs["esc_dir"] = esc
+        return arrs
+
+    def trace_paths(self, scene: KerrScene, alpha, beta, max_points: int, threads: int | None = None):
+        """Positions after every RK4 step of rays at (alpha, beta): xyz [n][max][3], counts [n]."""
+        al = np.ascontiguousarray(alpha, np.float64)
+        be = np.ascontiguousarray(beta, np.float64)
+        n = len(al)
+        xyz = np.zeros((n, max_points, 3))
+        cnt = np.zeros(n, np.int32)
+        self.lib.bho_trace_paths(C.byref(scene), n, _ptr(al), _ptr(be), max_points, _ptr(xyz), _ptr(cnt),
+                                 threads or default_threads())
+        return xyz, cnt
 
     def trace_rt(self, scene: KerrScene, cells: np.ndarray, r_range, lut: np.ndarray, log_theta, log_x, nu,
                  length_cm, ds_max, min_transmit, pix: np.ndarray | None = None, threads: int | None = None):
