@@ -47,8 +47,10 @@ UNIT = "rays/s"
 # Algorithmic FLOPs (add, mul, div, sqrt each 1) per accepted integration
 # step, frozen from the oracle's counting scalar over seeded pixels of each
 # workload (tests/test_flop_constants.py re-derives them). The mixed path runs
-# the same algorithm, so the same count applies to it.
-FLOPS_PER_STEP = {"dp45": 506.0, "rk4": 213.0}
+# the same algorithm, so the same count applies to it. "rt": one accepted DP45
+# step of the volumetric transfer (c2_512) with its medium samples (2.1 per
+# step on average; exp/log/acos not counted as FLOPs).
+FLOPS_PER_STEP = {"dp45": 506.0, "rk4": 213.0, "rt": 1001.0}
 
 WORKLOADS = {
     # name: (frames, width, integrator, max_crossings)
@@ -554,10 +556,18 @@ def run_rt(args, rank: int, world: int, dist):
                                      "pixels_compared": int(lit.sum().item()),
                                      "note": "the mixed steps differ, so samples sit elsewhere on each ray: "
                                              "differences are at the sampling's discretization level"}
-    roofline = {"bound": "fp64" if prec == 0 else "fp32", "achieved": None, "peak": None, "unit": "TFLOP/s",
-                "frac": None, "traffic": None, "kernel": "k_trace_rt_fp64" if prec == 0 else "k_trace_rt_mixed",
+    from blackhole_b200 import _abi
+
+    peak = C.c_double(0.0)
+    _abi.check(_abi.load_library().bh_measure_fma_peak(1 if prec == 0 else 0, 5, C.byref(peak)))
+    achieved = FLOPS_PER_STEP["rt"] * steps / (statistics.mean(ms) * 1e-3) / 1e12
+    roofline = {"bound": "fp64" if prec == 0 else "fp32", "achieved": achieved, "peak": peak.value,
+                "unit": "TFLOP/s", "frac": achieved / peak.value if peak.value else None, "traffic": None,
+                "peak_source": "measured FMA-pipe probe (bh_measure_fma_peak), FMA = 2 FLOPs",
+                "flops_per_step": FLOPS_PER_STEP["rt"], "steps_per_launch": steps,
+                "kernel": "k_trace_rt_fp64" if prec == 0 else "k_trace_rt_mixed",
                 "launch_ms_mean": statistics.mean(ms),
-                "note": "geodesic steps and medium samples; no FLOP count frozen for the samples yet"}
+                "note": "DP45 geodesic step plus its medium samples; the grid and table are L2-resident"}
     # ---- end to end: medium and table uploaded from pinned host memory, I_nu and tau read back ----
     e2e = None
     if rank == 0:

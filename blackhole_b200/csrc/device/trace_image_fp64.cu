@@ -251,6 +251,10 @@ __device__ __forceinline__ void rt_segment(const BhkImageParams &p, const BhkRtP
   const double rm = 0.5 * (y0.r + y1.r) + 0.125 * h * (k0.r - k1.r);
   const double um = 0.5 * (y0.u + y1.u) + 0.125 * h * (k0.u - k1.u);
   const double sig_m = rm * rm + p.a2 * um * um;
+  // a step that stays beyond r_max samples nothing: on t in [0, 1] the cubic
+  // Hermite r(t) >= min(r0, r1) - (4/27) |h| (|r0'| + |r1'|)
+  const double rlow = (y0.r < y1.r ? y0.r : y1.r) - (4.0 / 27.0) * fabs(h) * (fabs(k0.r) + fabs(k1.r));
+  if (rlow > q.r_max) return;
   double ns = ceil((sig_m * h) / q.ds_max);
   ns = ns < 1.0 ? 1.0 : (ns > 64.0 ? 64.0 : ns);
   const int nsub = (int)ns;

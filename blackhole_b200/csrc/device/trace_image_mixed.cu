@@ -436,6 +436,9 @@ __device__ __forceinline__ void rt_segment_f(const BhkImageParams &p, const bhrt
   const float a2 = c.a2;
   const float rm = fmaf(0.125f * h, k0.r - k1.r, 0.5f * (y0.r + y1.r));
   const float um = fmaf(0.125f * h, k0.u - k1.u, 0.5f * (y0.u + y1.u));
+  // a step that stays beyond r_max samples nothing (see the FP64 transfer)
+  const float rlow = fminf(y0.r, y1.r) - (4.0f / 27.0f) * fabsf(h) * (fabsf(k0.r) + fabsf(k1.r));
+  if (rlow > q.r_max) return;
   const float sig_m = fmaf(rm, rm, a2 * um * um);
   const float ns = fminf(fmaxf(ceilf(__fdividef(sig_m * h, q.ds_max)), 1.0f), 64.0f);
   const int nsub = (int)ns;

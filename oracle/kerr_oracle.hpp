@@ -51,6 +51,11 @@ inline double s_abs(double x) { return std::fabs(x); }
 inline double s_acos(double x) { return std::acos(x); }
 inline double s_cbrt(double x) { return std::cbrt(x); }
 inline double s_pow(double x, double y) { return std::pow(x, y); }
+inline double s_log(double x) { return std::log(x); }
+inline double s_exp(double x) { return std::exp(x); }
+inline double s_expm1(double x) { return std::expm1(x); }
+inline double s_floor(double x) { return std::floor(x); }
+inline double s_ceil(double x) { return std::ceil(x); }
 inline long double s_sqrt(long double x) { return std::sqrt(x); }
 inline long double s_sin(long double x) { return std::sin(x); }
 inline long double s_cos(long double x) { return std::cos(x); }

@@ -280,6 +280,39 @@ int bho_sky_texels(int64_t n, const double *x, const double *y, const double *z,
 }
 
 // ---- along-ray radiative transfer (rt_oracle.hpp) ----
+
+// Operation counts of the transfer of the given pixels with the counting
+// scalar (single thread): counts[0..6] as bho_count_ops summed over the
+// pixels, counts[7] accepted steps, counts[8] medium samples.
+int bho_count_rt_ops(const BH_KerrScene *scene, int64_t n, const int64_t *pix_index, const float *cells, int n_r,
+                     int n_th, int n_ph, double r_min, double r_max, const float *lut, int n_lt, int n_lx, double lt0,
+                     double lt1, double lx0, double lx1, double nu, double length_cm, double ds_max,
+                     double min_transmit, int64_t *counts) {
+  const bho::Scene s = to_scene(scene);
+  const auto d = bho::derive<bho::Counted>(s);
+  const bho_rt::Medium q{cells, n_r, n_th, n_ph, r_min, r_max, 1.0 / std::log(r_max / r_min), lut, n_lt, n_lx,
+                         lt0, lt1, lx0, lx1, nu, length_cm, ds_max, min_transmit};
+  for (int k = 0; k < 9; ++k) counts[k] = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    double alpha, beta;
+    bho::pixel_alpha_beta(s, pix_index[i], alpha, beta);
+    bho::g_counts = bho::OpCounts{};
+    int64_t samples = 0;
+    const bho_rt::Result r =
+        bho_rt::trace_pixel_rt(s, d, bho::Counted(alpha), bho::Counted(beta), q, &samples);
+    const bho::OpCounts c = bho::g_counts;
+    counts[0] += c.add;
+    counts[1] += c.mul;
+    counts[2] += c.div;
+    counts[3] += c.sqrt;
+    counts[4] += c.trig;
+    counts[5] += c.pow;
+    counts[6] += c.cmp;
+    counts[7] += r.steps;
+    counts[8] += samples;
+  }
+  return 0;
+}
 int bho_trace_rt(const BH_KerrScene *scene, int64_t n, const int64_t *pix_index, const float *cells, int n_r,
                  int n_th, int n_ph, double r_min, double r_max, const float *lut, int n_lt, int n_lx, double lt0,
                  double lt1, double lx0, double lx1, double nu, double length_cm, double ds_max, double min_transmit,

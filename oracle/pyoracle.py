@@ -92,6 +92,8 @@ class Oracle(_Base):
         L.bho_trace_camera.argtypes = [C.POINTER(KerrScene), _vp, _vp, _i64, _vp, C.POINTER(KerrImageOut), _vp,
                                        C.c_int]
         L.bho_trace_paths.argtypes = [C.POINTER(KerrScene), _i64, _vp, _vp, C.c_int, _vp, _vp, C.c_int]
+        L.bho_count_rt_ops.argtypes = ([C.POINTER(KerrScene), _i64, _vp, _vp, C.c_int, C.c_int, C.c_int, _f64, _f64,
+                                        _vp, C.c_int, C.c_int] + [_f64] * 8 + [_vp])
         L.bho_trace_rt.argtypes = ([C.POINTER(KerrScene), _i64, _vp, _vp, C.c_int, C.c_int, C.c_int, _f64, _f64, _vp,
                                     C.c_int, C.c_int] + [_f64] * 8 + [_vp] * 4 + [C.c_int])
         L.bho_rt_path.restype = _f64
@@ -144,6 +146,19 @@ class Oracle(_Base):
             raise RuntimeError("oracle camera trace failed")
         arrs["esc_dir"] = esc
         return arrs
+
+    def count_rt_ops(self, scene: KerrScene, cells: np.ndarray, r_range, lut: np.ndarray, log_theta, log_x, nu,
+                     length_cm, ds_max, min_transmit, pix: np.ndarray) -> dict:
+        """Operation counts of the transfer over the given pixels (counting scalar)."""
+        cells = np.ascontiguousarray(cells, np.float32)
+        lut = np.ascontiguousarray(lut, np.float32)
+        idx = np.ascontiguousarray(pix, np.int64)
+        c = np.zeros(9, np.int64)
+        self.lib.bho_count_rt_ops(C.byref(scene), len(idx), _ptr(idx), _ptr(cells), cells.shape[0], cells.shape[1],
+                                  cells.shape[2], r_range[0], r_range[1], _ptr(lut), lut.shape[0], lut.shape[1],
+                                  log_theta[0], log_theta[1], log_x[0], log_x[1], nu, length_cm, ds_max,
+                                  min_transmit, _ptr(c))
+        return dict(zip(["add", "mul", "div", "sqrt", "trig", "pow", "cmp", "steps", "samples"], c.tolist()))
 
     def trace_paths(self, scene: KerrScene, alpha, beta, max_points: int, threads: int | None = None):
         """Positions after every RK4 step of rays at (alpha, beta): xyz [n][max][3], counts [n]."""

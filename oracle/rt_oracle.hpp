@@ -17,6 +17,14 @@
 
 namespace bho_rt {
 
+using bho::s_acos;
+using bho::s_ceil;
+using bho::s_exp;
+using bho::s_expm1;
+using bho::s_floor;
+using bho::s_log;
+using bho::s_sqrt;
+
 struct Medium {
   const float *cells;  // float4 [n_r][n_th][n_ph]
   int n_r, n_th, n_ph;
@@ -35,35 +43,39 @@ struct Result {
 inline constexpr double kE = 4.80320425e-10, kMe = 9.1093837015e-28, kC = 2.99792458e10, kKb = 1.380649e-16,
                         kH = 6.62607015e-27, kTwoPi = 6.283185307179586;
 
-inline bool sample(const Medium &q, double r, double u, double phi, double &n, double &th, double &b) {
-  if (!(r >= q.r_min && r <= q.r_max)) return false;
-  const double fr = (std::log(r / q.r_min) * q.inv_log_range) * double(q.n_r - 1);
-  int i0 = int(std::floor(fr));
+// Every function is templated on the scalar: double for the oracle itself,
+// bho::Counted to count the operations per accepted step (the roofline's
+// FLOP constant). Integer index arithmetic runs on plain values.
+template <class T>
+inline bool sample(const Medium &q, T r, T u, T phi, T &n, T &th, T &b) {
+  if (!(r >= T(q.r_min) && r <= T(q.r_max))) return false;
+  const T fr = (s_log(r / T(q.r_min)) * T(q.inv_log_range)) * T(double(q.n_r - 1));
+  int i0 = int(double(s_floor(fr)));
   i0 = i0 < 0 ? 0 : (i0 > q.n_r - 2 ? q.n_r - 2 : i0);
-  double tr = fr - double(i0);
-  tr = tr < 0.0 ? 0.0 : (tr > 1.0 ? 1.0 : tr);
-  const double theta = std::acos(u < -1.0 ? -1.0 : (u > 1.0 ? 1.0 : u));
-  const double ft = (theta * (1.0 / 3.141592653589793)) * double(q.n_th) - 0.5;
-  int j0 = int(std::floor(ft));
+  T tr = fr - T(double(i0));
+  tr = tr < T(0.0) ? T(0.0) : (tr > T(1.0) ? T(1.0) : tr);
+  const T theta = s_acos(u < T(-1.0) ? T(-1.0) : (u > T(1.0) ? T(1.0) : u));
+  const T ft = (theta * T(1.0 / 3.141592653589793)) * T(double(q.n_th)) - T(0.5);
+  int j0 = int(double(s_floor(ft)));
   j0 = j0 < 0 ? 0 : (j0 > q.n_th - 2 ? q.n_th - 2 : j0);
-  double tt = ft - double(j0);
-  tt = tt < 0.0 ? 0.0 : (tt > 1.0 ? 1.0 : tt);
-  const double fp = (phi * (1.0 / kTwoPi)) * double(q.n_ph);
-  const double fl = std::floor(fp);
-  const double tp = fp - fl;
-  long long k0 = (long long)fl % q.n_ph;
+  T tt = ft - T(double(j0));
+  tt = tt < T(0.0) ? T(0.0) : (tt > T(1.0) ? T(1.0) : tt);
+  const T fp = (phi * T(1.0 / kTwoPi)) * T(double(q.n_ph));
+  const T fl = s_floor(fp);
+  const T tp = fp - fl;
+  long long k0 = (long long)double(fl) % q.n_ph;
   if (k0 < 0) k0 += q.n_ph;
   const long long k1 = (k0 + 1) % q.n_ph;
-  double acc[3] = {0.0, 0.0, 0.0};
+  T acc[3] = {T(0.0), T(0.0), T(0.0)};
   for (int di = 0; di < 2; ++di)
     for (int dj = 0; dj < 2; ++dj)
       for (int dk = 0; dk < 2; ++dk) {
-        const double w = (di ? tr : 1.0 - tr) * (dj ? tt : 1.0 - tt) * (dk ? tp : 1.0 - tp);
+        const T w = (di ? tr : T(1.0) - tr) * (dj ? tt : T(1.0) - tt) * (dk ? tp : T(1.0) - tp);
         const long long idx = ((long long)(i0 + di) * q.n_th + (j0 + dj)) * q.n_ph + (dk ? k1 : k0);
         const float *v = q.cells + 4 * idx;
-        acc[0] = acc[0] + w * double(v[0]);
-        acc[1] = acc[1] + w * double(v[1]);
-        acc[2] = acc[2] + w * double(v[2]);
+        acc[0] = acc[0] + w * T(double(v[0]));
+        acc[1] = acc[1] + w * T(double(v[1]));
+        acc[2] = acc[2] + w * T(double(v[2]));
       }
   n = acc[0];
   th = acc[1];
@@ -71,78 +83,83 @@ inline bool sample(const Medium &q, double r, double u, double phi, double &n, d
   return true;
 }
 
-inline double redshift(double a, double r, double u, double lam) {
-  const double u2 = u * u;
-  const double s2 = (1.0 - u) * (1.0 + u);
-  const double sig = r * r + a * a * u2;
-  const double delta = r * r - 2.0 * r + a * a;
-  const double A = (r * r + a * a) * (r * r + a * a) - a * a * delta * s2;
-  const double om = 1.0 / (r * std::sqrt(r) + a);
-  const double gtt = -(1.0 - 2.0 * r / sig);
-  const double gtp = -2.0 * a * r * s2 / sig;
-  const double gpp = A * s2 / sig;
-  const double norm = -(gtt + 2.0 * gtp * om + gpp * om * om);
-  if (!(norm > 0.0)) return 0.0;
-  const double ut = 1.0 / std::sqrt(norm);
-  const double den = ut * (1.0 - om * lam);
-  return den > 0.0 ? 1.0 / den : 0.0;
+template <class T>
+inline T redshift(T a, T r, T u, T lam) {
+  const T u2 = u * u;
+  const T s2 = (T(1.0) - u) * (T(1.0) + u);
+  const T sig = r * r + a * a * u2;
+  const T delta = r * r - T(2.0) * r + a * a;
+  const T A = (r * r + a * a) * (r * r + a * a) - a * a * delta * s2;
+  const T om = T(1.0) / (r * s_sqrt(r) + a);
+  const T gtt = -(T(1.0) - T(2.0) * r / sig);
+  const T gtp = -T(2.0) * a * r * s2 / sig;
+  const T gpp = A * s2 / sig;
+  const T norm = -(gtt + T(2.0) * gtp * om + gpp * om * om);
+  if (!(norm > T(0.0))) return T(0.0);
+  const T ut = T(1.0) / s_sqrt(norm);
+  const T den = ut * (T(1.0) - om * lam);
+  return den > T(0.0) ? T(1.0) / den : T(0.0);
 }
 
-inline double planck(double nu, double temp) {
-  const double x = (kH * nu) / (kKb * temp);
-  const double den = (x > 500.0) ? std::exp(x) : std::expm1(x);
-  if (!(den > 0.0)) return 0.0;
-  return (2.0 * kH * nu * nu * nu / (kC * kC)) / den;
+template <class T>
+inline T planck(T nu, T temp) {
+  const T x = (T(kH) * nu) / (T(kKb) * temp);
+  const T den = (x > T(500.0)) ? s_exp(x) : s_expm1(x);
+  if (!(den > T(0.0))) return T(0.0);
+  return (T(2.0) * T(kH) * nu * nu * nu / (T(kC) * T(kC))) / den;
 }
 
-inline void synchrotron(const Medium &q, double n, double theta_e, double b, double nu_e, double &j, double &alpha) {
-  j = 0.0;
-  alpha = 0.0;
-  if (!(n > 0.0 && theta_e > 0.0 && b > 0.0 && nu_e > 0.0)) return;
-  const double nu_b = kE * b / (kTwoPi * kMe * kC);
-  const double nu_s = 1.5 * nu_b * theta_e * theta_e;
-  const double lx = std::log(nu_e / nu_s);
-  if (lx > q.lx1) return;
-  const double lt = std::log(theta_e);
-  double ft = (lt - q.lt0) / (q.lt1 - q.lt0) * double(q.n_lt - 1);
-  double fx = (lx - q.lx0) / (q.lx1 - q.lx0) * double(q.n_lx - 1);
-  ft = ft < 0.0 ? 0.0 : (ft > double(q.n_lt - 1) ? double(q.n_lt - 1) : ft);
-  fx = fx < 0.0 ? 0.0 : (fx > double(q.n_lx - 1) ? double(q.n_lx - 1) : fx);
-  int i0 = int(std::floor(ft)), k0 = int(std::floor(fx));
+template <class T>
+inline void synchrotron(const Medium &q, T n, T theta_e, T b, T nu_e, T &j, T &alpha) {
+  j = T(0.0);
+  alpha = T(0.0);
+  if (!(n > T(0.0) && theta_e > T(0.0) && b > T(0.0) && nu_e > T(0.0))) return;
+  const T nu_b = T(kE) * b / (T(kTwoPi) * T(kMe) * T(kC));
+  const T nu_s = T(1.5) * nu_b * theta_e * theta_e;
+  const T lx = s_log(nu_e / nu_s);
+  if (lx > T(q.lx1)) return;
+  const T lt = s_log(theta_e);
+  T ft = (lt - T(q.lt0)) / (T(q.lt1) - T(q.lt0)) * T(double(q.n_lt - 1));
+  T fx = (lx - T(q.lx0)) / (T(q.lx1) - T(q.lx0)) * T(double(q.n_lx - 1));
+  ft = ft < T(0.0) ? T(0.0) : (ft > T(double(q.n_lt - 1)) ? T(double(q.n_lt - 1)) : ft);
+  fx = fx < T(0.0) ? T(0.0) : (fx > T(double(q.n_lx - 1)) ? T(double(q.n_lx - 1)) : fx);
+  int i0 = int(double(s_floor(ft))), k0 = int(double(s_floor(fx)));
   i0 = i0 > q.n_lt - 2 ? q.n_lt - 2 : i0;
   k0 = k0 > q.n_lx - 2 ? q.n_lx - 2 : k0;
-  const double ti = ft - double(i0), tk = fx - double(k0);
+  const T ti = ft - T(double(i0)), tk = fx - T(double(k0));
   const float *L = q.lut;
-  const double v00 = L[i0 * q.n_lx + k0], v01 = L[i0 * q.n_lx + k0 + 1];
-  const double v10 = L[(i0 + 1) * q.n_lx + k0], v11 = L[(i0 + 1) * q.n_lx + k0 + 1];
-  const double J = ((1.0 - ti) * ((1.0 - tk) * v00 + tk * v01)) + (ti * ((1.0 - tk) * v10 + tk * v11));
-  j = n * nu_b * std::exp(J);
-  const double bnu = planck(nu_e, theta_e * kMe * kC * kC / kKb);
-  alpha = bnu > 0.0 ? j / bnu : 0.0;
+  const T v00 = T(double(L[i0 * q.n_lx + k0])), v01 = T(double(L[i0 * q.n_lx + k0 + 1]));
+  const T v10 = T(double(L[(i0 + 1) * q.n_lx + k0])), v11 = T(double(L[(i0 + 1) * q.n_lx + k0 + 1]));
+  const T J = ((T(1.0) - ti) * ((T(1.0) - tk) * v00 + tk * v01)) + (ti * ((T(1.0) - tk) * v10 + tk * v11));
+  j = n * nu_b * s_exp(J);
+  const T bnu = planck(nu_e, theta_e * T(kMe) * T(kC) * T(kC) / T(kKb));
+  alpha = bnu > T(0.0) ? j / bnu : T(0.0);
 }
 
 // One front-to-back segment of the formal solution.
-inline void segment(double jo, double ao, double ds, double &I, double &T, double &tau) {
-  const double ts = ao * ds;
-  const double om = (ts < 1.0e-4) ? ts * (1.0 - 0.5 * ts) : -std::expm1(-ts);
-  I = (ao > 0.0) ? I + T * ((jo / ao) * om) : I + T * (jo * ds);
-  T = T * (1.0 - om);
+template <class T>
+inline void segment(T jo, T ao, T ds, T &I, T &Tr, T &tau) {
+  const T ts = ao * ds;
+  const T om = (ts < T(1.0e-4)) ? ts * (T(1.0) - T(0.5) * ts) : -s_expm1(-ts);
+  I = (ao > T(0.0)) ? I + Tr * ((jo / ao) * om) : I + Tr * (jo * ds);
+  Tr = Tr * (T(1.0) - om);
   tau = tau + ts;
 }
 
-inline Result trace_pixel_rt(const bho::Scene &s, const bho::SceneDerived<double> &d, double alpha, double beta,
-                             const Medium &q) {
+template <class T>
+inline Result trace_pixel_rt(const bho::Scene &s, const bho::SceneDerived<T> &d, T alpha, T beta, const Medium &q,
+                             int64_t *samples = nullptr) {
   using namespace bho;
   Result out{0.0, 0.0, 3, 0};
-  RayConsts<double> c;
-  Y<double> y;
+  RayConsts<T> c;
+  Y<T> y;
   init_ray(d, s, alpha, beta, c, y);
-  const PolyRhs<double> f{c};
+  const PolyRhs<T> f{c};
   f.project(y);
-  const double a2 = d.a * d.a;
-  double h = mino_step(s, y, d.a);
-  Y<double> k1 = f(y);
-  double I = 0.0, T = 1.0, tau = 0.0;
+  const T a2 = d.a * d.a;
+  T h = mino_step(s, y, d.a);
+  Y<T> k1 = f(y);
+  T I = T(0.0), Tr = T(1.0), tau = T(0.0);
   int64_t attempts = 0;
   const int64_t max_attempts = int64_t(4) * s.max_steps + 64;
   for (;;) {
@@ -150,48 +167,54 @@ inline Result trace_pixel_rt(const bho::Scene &s, const bho::SceneDerived<double
     if (y.r <= d.r_hor) { out.cls = 0; break; }
     if (y.r >= d.r_esc) { out.cls = 2; break; }
     ++attempts;
-    const DPOut<double> o = img_dp45(y, h, f, k1, s.rtol, s.atol, true);
-    if (o.err <= 1.0) {
+    const DPOut<T> o = img_dp45(y, h, f, k1, T(s.rtol), T(s.atol), true);
+    if (o.err <= T(1.0)) {
       ++out.steps;
-      const Y<double> &y0 = y, &k0 = k1, &y1 = o.y5, &kk = o.k7;
-      const double rm = 0.5 * (y0.r + y1.r) + 0.125 * h * (k0.r - kk.r);
-      const double um = 0.5 * (y0.u + y1.u) + 0.125 * h * (k0.u - kk.u);
-      const double sig_m = rm * rm + a2 * um * um;
-      double ns = std::ceil((sig_m * h) / q.ds_max);
-      ns = ns < 1.0 ? 1.0 : (ns > 64.0 ? 64.0 : ns);
-      const int nsub = int(ns);
-      const double dt = h / ns;
+      const Y<T> &y0 = y, &k0 = k1, &y1 = o.y5, &kk = o.k7;
+      const T rm = T(0.5) * (y0.r + y1.r) + T(0.125) * h * (k0.r - kk.r);
+      const T um = T(0.5) * (y0.u + y1.u) + T(0.125) * h * (k0.u - kk.u);
+      const T sig_m = rm * rm + a2 * um * um;
+      // A step that stays beyond r_max samples nothing: on t in [0, 1] the
+      // cubic Hermite r(t) >= min(r0, r1) - (4/27) |h| (|r0'| + |r1'|).
+      const T rlow = (y0.r < y1.r ? y0.r : y1.r) - T(4.0 / 27.0) * (h < T(0.0) ? -h : h) *
+                                                         ((k0.r < T(0.0) ? -k0.r : k0.r) + (kk.r < T(0.0) ? -kk.r : kk.r));
+      const bool outside = rlow > T(q.r_max);
+      T ns = s_ceil((sig_m * h) / T(q.ds_max));
+      ns = ns < T(1.0) ? T(1.0) : (ns > T(64.0) ? T(64.0) : ns);
+      const int nsub = outside ? 0 : int(double(ns));
+      const T dt = h / ns;
       for (int m = 0; m < nsub; ++m) {
-        const double t = (double(m) + 0.5) / ns;
-        const double t2 = t * t, t3 = t2 * t;
-        const double h00 = 2.0 * t3 - 3.0 * t2 + 1.0, h10 = t3 - 2.0 * t2 + t;
-        const double h01 = -2.0 * t3 + 3.0 * t2, h11 = t3 - t2;
-        const double r = h00 * y0.r + h10 * h * k0.r + h01 * y1.r + h11 * h * kk.r;
-        const double u = h00 * y0.u + h10 * h * k0.u + h01 * y1.u + h11 * h * kk.u;
-        const double psi = h00 * y0.phi + h10 * h * k0.phi + h01 * y1.phi + h11 * h * kk.phi;
-        const double dl = (r * r + a2 * u * u) * dt;
-        double n, th, b;
-        const double phi = phi_of_psi(psi, r, s.r_obs, d.a, d.r_plus, d.r_minus);
+        const T t = (T(double(m)) + T(0.5)) / ns;
+        const T t2 = t * t, t3 = t2 * t;
+        const T h00 = T(2.0) * t3 - T(3.0) * t2 + T(1.0), h10 = t3 - T(2.0) * t2 + t;
+        const T h01 = -T(2.0) * t3 + T(3.0) * t2, h11 = t3 - t2;
+        const T r = h00 * y0.r + h10 * h * k0.r + h01 * y1.r + h11 * h * kk.r;
+        const T u = h00 * y0.u + h10 * h * k0.u + h01 * y1.u + h11 * h * kk.u;
+        const T psi = h00 * y0.phi + h10 * h * k0.phi + h01 * y1.phi + h11 * h * kk.phi;
+        const T dl = (r * r + a2 * u * u) * dt;
+        T n, th, b;
+        const T phi = phi_of_psi(psi, r, T(s.r_obs), d.a, d.r_plus, d.r_minus);
+        if (samples) ++*samples;
         if (!sample(q, r, u, phi, n, th, b)) continue;
-        const double g = redshift(d.a, r, u, c.lam);
-        if (!(g > 0.0)) continue;
-        double j, al;
-        synchrotron(q, n, th, b, q.nu / g, j, al);
-        segment(g * g * j, al / g, dl * q.length_cm, I, T, tau);
+        const T g = redshift(d.a, r, u, c.lam);
+        if (!(g > T(0.0))) continue;
+        T j, al;
+        synchrotron(q, n, th, b, T(q.nu) / g, j, al);
+        segment(g * g * j, al / g, dl * T(q.length_cm), I, Tr, tau);
       }
       y = o.y5;
       k1 = o.k7;
       f.project(y);
       k1.r = y.pr;
       k1.u = y.pu;
-      h = h * step_factor(o.err, true);
-      if (T < q.min_transmit) { out.cls = 4; break; }
+      h = h * T(step_factor(double(o.err), true));
+      if (Tr < T(q.min_transmit)) { out.cls = 4; break; }
     } else {
-      h = h * step_factor(o.err, false);
+      h = h * T(step_factor(double(o.err), false));
     }
   }
-  out.I = I;
-  out.tau = tau;
+  out.I = double(I);
+  out.tau = double(tau);
   return out;
 }
 

@@ -43,6 +43,12 @@ inline Counted s_acos(Counted x) { ++g_counts.trig; return Counted(std::acos(x.v
 inline Counted s_abs(Counted x) { return Counted(std::fabs(x.v)); }
 inline Counted s_cbrt(Counted x) { ++g_counts.pow; return Counted(std::cbrt(x.v)); }
 inline Counted s_pow(Counted x, Counted y) { ++g_counts.pow; return Counted(std::pow(x.v, y.v)); }
+// exp / log family: counted with the transcendental functions (trig), not as FLOPs
+inline Counted s_log(Counted x) { ++g_counts.trig; return Counted(std::log(x.v)); }
+inline Counted s_exp(Counted x) { ++g_counts.trig; return Counted(std::exp(x.v)); }
+inline Counted s_expm1(Counted x) { ++g_counts.trig; return Counted(std::expm1(x.v)); }
+inline Counted s_floor(Counted x) { return Counted(std::floor(x.v)); }
+inline Counted s_ceil(Counted x) { return Counted(std::ceil(x.v)); }
 
 using f128 = __float128;
 inline f128 s_sqrt(f128 x) { return sqrtq(x); }

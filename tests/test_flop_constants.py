@@ -43,3 +43,30 @@ def test_rhs_operation_count(oracle):
     assert (rhs["add"], rhs["mul"], rhs["div"]) == (12, 13, 2)
     assert step["add"] + step["mul"] + step["div"] == 184
     assert math.isclose(step["div"], 10)
+
+
+def test_transfer_flops_constant(oracle, lib):
+    """FLOPs per accepted step of the volumetric transfer (c2_512: DP45 step
+    plus its medium samples), counted over seeded pixels of the frame."""
+    import ctypes as C_
+
+    import bench
+    from blackhole_b200 import rt
+    from blackhole_b200._abi import default_scene
+    from oracle import grmhd_oracle
+
+    cells = grmhd_oracle.grid(128, 64, 64, 2.0, 50.0)
+    desc = rt.SynchrotronLut(None, 256, 256, math.log(0.1), math.log(1000.0), math.log(1e-4), math.log(1e4))
+    tab = np.empty((256, 256), np.float32)
+    rt._lib()
+    assert lib.bh_synchrotron_lut_host(C_.byref(desc), tab.ctypes.data) == 0
+    s = default_scene(width=512, height=512, spin=0.94, theta_obs=math.radians(17.0), integrator=1,
+                      max_crossings=1, precision=0)
+    s.max_steps = 2000
+    s.alpha_min, s.alpha_max, s.beta_min, s.beta_max = -20.0, 20.0, -20.0, 20.0
+    p = rt.rt_defaults()
+    pix = np.random.default_rng(3).integers(0, 512 * 512, 400)
+    c = oracle.count_rt_ops(s, cells, (2.0, 50.0), tab, (desc.log_theta_min, desc.log_theta_max),
+                            (desc.log_x_min, desc.log_x_max), p.nu_hz, p.length_cm, p.ds_max, p.min_transmit, pix)
+    f = (c["add"] + c["mul"] + c["div"] + c["sqrt"]) / c["steps"]
+    assert f == pytest.approx(bench.FLOPS_PER_STEP["rt"], rel=0.05)

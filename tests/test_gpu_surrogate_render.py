@@ -92,3 +92,42 @@ def test_trained_network_meets_targets(cuda, oracle):
     d = (got["n_cross"] > 0) & (ref["n_cross"] > 0)
     rel = np.abs(got["g"][0][d] - ref["g"][0][d]) / ref["g"][0][d]
     assert np.median(rel) <= 1e-4 and rel.max() <= 1e-3, (np.median(rel), rel.max())
+
+
+@pytest.mark.skipif(not WEIGHTS.exists(), reason="trained weights not shipped")
+def test_trained_network_gain_over_the_integrator(cuda):
+    """Ablation: the same renderer with the trained network against the
+    method without it (an untrained network sends every pixel to the
+    integrator; the plain mixed tracer traces every pixel). The network
+    removes >= 95 % of the integration steps and renders >= 1.5x faster, at
+    the same accuracy (checked above)."""
+    from blackhole_b200 import kerr
+    from blackhole_b200 import surrogate as S
+
+    s = c4_scene(1024, precision=1)
+    trained = S.Surrogate(max_batch=128)
+    trained.load(WEIGHTS)
+    blank = S.Surrogate(max_batch=128, seed=3)
+    o_t = trained.trace_image(s)
+    o_b = blank.trace_image(s)
+    o_m = kerr.trace_image(s)
+    torch.cuda.synchronize()
+    steps_t = int(o_t["steps"].sum().item())
+    steps_b = int(o_b["steps"].sum().item())
+    assert steps_b == int(o_m["steps"].sum().item())  # no network: the integrator on every pixel
+    assert steps_t <= 0.05 * steps_b, (steps_t, steps_b)
+
+    def ms(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    t_net = ms(lambda: trained.trace_image(s, o_t))
+    t_plain = ms(lambda: kerr.trace_image(s, o_m))
+    assert t_plain >= 1.5 * t_net, (t_plain, t_net)
