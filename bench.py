@@ -52,6 +52,13 @@ UNIT = "rays/s"
 # step on average; exp/log/acos not counted as FLOPs).
 FLOPS_PER_STEP = {"dp45": 506.0, "rk4": 213.0, "rt": 1001.0}
 
+# DRAM bytes (read + write) of one k_mlp_infer launch on the 2048^2 frame,
+# from one single-pass ncu capture of this script's default run
+# (profiles/k_mlp_infer_c4_1024.md gives the command): 67.8 MB read (inputs and
+# weights), 214.6 MB written (the rest of the 268 MB of outputs is still in L2
+# when the kernel ends).
+INFER_DRAM_BYTES_2048 = 67833856 + 214636288
+
 WORKLOADS = {
     # name: (frames, width, integrator, max_crossings)
     "disk16": dict(width=1024, height=1024, integrator=1, max_crossings=3, sky=True,
@@ -452,7 +459,9 @@ def run_surrogate(args, rank: int, world: int, dist):
     peak = peaks.get("bf16_tflops")
     achieved = SURROGATE_FLOPS_PER_RAY * n / (statistics.mean(fwd_ms) * 1e-3) / 1e12
     roofline = {"bound": "tensor", "achieved": achieved, "peak": peak or 1590.0, "unit": "TFLOP/s",
-                "frac": achieved / (peak or 1590.0), "traffic": None,
+                "frac": achieved / (peak or 1590.0),
+                "traffic": INFER_DRAM_BYTES_2048 if (smx.width, smx.height) == (2048, 2048) else None,
+                "traffic_unit": "bytes per launch (dram read + write, ncu)",
                 "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst, of measured)" if peak else "fallback 1.59 PF",
                 "kernel": "k_mlp_infer", "flops_per_ray": SURROGATE_FLOPS_PER_RAY, "rays_per_launch": n,
                 "launch_ms_mean": statistics.mean(fwd_ms),

@@ -146,6 +146,10 @@ int bhk_trace_rt_fp64(const BhkImageParams *p, const BhkRtParams *q, double *i_n
                       int32_t *steps, unsigned long long *work_counter, int grid, int block, void *stream);
 
 // Synthetic torus grid (grmhd.cu): modes [n_modes] of (kx, ky, kz, phase).
+// Resample packed simulation frames into the medium grid (grmhd.cu).
+int bhk_grmhd_from_packed(float *cells, int n_r, int n_th, int n_ph, double r_min, double r_max, const float *left,
+                          const float *right, double alpha, int pnr, int pnt, int pnp, double pr_min, double pr_max,
+                          double n_scale, double theta_scale, double b_scale, void *stream);
 int bhk_grmhd_fill(float *cells, int n_r, int n_th, int n_ph, double r_min, double r_max, double r_in, double r_peak,
                    double width, double n0, double theta0, double b0, double amp, const double *modes, int n_modes,
                    void *stream);

@@ -33,6 +33,16 @@ class SynchrotronLut(C.Structure):
                 ("log_x_min", C.c_double), ("log_x_max", C.c_double)]
 
 
+class PackedGrmhdInfo(C.Structure):
+    _fields_ = [("n_r", C.c_int32), ("n_theta", C.c_int32), ("n_phi", C.c_int32), ("reserved", C.c_int32),
+                ("r_min", C.c_float), ("r_max", C.c_float), ("min_value", C.c_float * 4),
+                ("max_value", C.c_float * 4), ("channels", (C.c_char * 32) * 4)]
+
+
+class PackedConversion(C.Structure):
+    _fields_ = [("n_scale", C.c_double), ("theta_scale", C.c_double), ("b_scale", C.c_double)]
+
+
 class RtParams(C.Structure):
     _fields_ = [("nu_hz", C.c_double), ("length_cm", C.c_double), ("ds_max", C.c_double),
                 ("min_transmit", C.c_double)]
@@ -55,12 +65,40 @@ def _lib():
         lib.bh_kerr_trace_rt.restype = C.c_int
         lib.bh_kerr_trace_rt.argtypes = [C.POINTER(KerrScene), C.POINTER(GrmhdGrid), C.POINTER(SynchrotronLut),
                                          C.POINTER(RtParams), vp, vp, vp, vp, vp]
+        lib.bh_grmhd_packed_read.restype = C.c_int
+        lib.bh_grmhd_packed_read.argtypes = [C.c_char_p, C.POINTER(PackedGrmhdInfo), vp, C.c_int64]
+        lib.bh_packed_conversion_defaults.restype = None
+        lib.bh_packed_conversion_defaults.argtypes = [C.POINTER(PackedConversion)]
+        lib.bh_grmhd_from_packed.restype = C.c_int
+        lib.bh_grmhd_from_packed.argtypes = [C.POINTER(GrmhdGrid), C.POINTER(PackedGrmhdInfo), vp, vp, C.c_double,
+                                             C.POINTER(PackedConversion), vp]
         lib._rt_declared = True
     return lib
 
 
 def _stream(stream):
     return None if stream is None else (stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+
+
+def read_packed(json_path, samples: bool = True) -> tuple[PackedGrmhdInfo, np.ndarray | None]:
+    """bh_grmhd_packed_read: metadata and (optionally) the float samples
+    [n_r][n_theta][n_phi][4] of a nubhlight_pack dataset."""
+    lib = _lib()
+    info = PackedGrmhdInfo()
+    check(lib.bh_grmhd_packed_read(str(json_path).encode(), C.byref(info), None, 0))
+    if not samples:
+        return info, None
+    out = np.empty((info.n_r, info.n_theta, info.n_phi, 4), np.float32)
+    check(lib.bh_grmhd_packed_read(str(json_path).encode(), C.byref(info), out.ctypes.data, out.size))
+    return info, out
+
+
+def conversion_defaults(**kw) -> PackedConversion:
+    c = PackedConversion()
+    _lib().bh_packed_conversion_defaults(C.byref(c))
+    for k, v in kw.items():
+        setattr(c, k, v)
+    return c
 
 
 def torus_defaults(**kw) -> TorusParams:
@@ -80,14 +118,30 @@ def rt_defaults(**kw) -> RtParams:
 
 
 class Medium:
-    """The grid (n_e, Theta_e, |B|) on the device and its descriptor."""
+    """The grid (n_e, Theta_e, |B|) on the device and its descriptor: the
+    synthetic torus by default, or frames of simulation output
+    (``from_packed``)."""
 
     def __init__(self, n_r=128, n_theta=64, n_phi=64, r_min=2.0, r_max=50.0, torus: TorusParams | None = None,
-                 device="cuda", stream=None):
+                 device="cuda", stream=None, synthetic: bool = True):
         self.cells = torch.empty(n_r, n_theta, n_phi, 4, dtype=torch.float32, device=device)
         self.desc = GrmhdGrid(self.cells.data_ptr(), n_r, n_theta, n_phi, 0, r_min, r_max)
         self.torus = torus or torus_defaults()
-        check(_lib().bh_grmhd_synthetic(C.byref(self.desc), C.byref(self.torus), _stream(stream)))
+        if synthetic:
+            check(_lib().bh_grmhd_synthetic(C.byref(self.desc), C.byref(self.torus), _stream(stream)))
+
+    @classmethod
+    def from_packed(cls, info: PackedGrmhdInfo, left: torch.Tensor, right: torch.Tensor | None = None,
+                    alpha: float = 0.0, conversion: PackedConversion | None = None, n_r=128, n_theta=64, n_phi=64,
+                    r_min=2.0, r_max=50.0, stream=None) -> "Medium":
+        """bh_grmhd_from_packed: the grid resampled from one packed frame (a
+        device float32 tensor [n_r][n_theta][n_phi][4]) or the blend of two."""
+        m = cls(n_r, n_theta, n_phi, r_min, r_max, device=left.device, synthetic=False)
+        conv = conversion or conversion_defaults()
+        check(_lib().bh_grmhd_from_packed(C.byref(m.desc), C.byref(info), left.data_ptr(),
+                                          None if right is None else right.data_ptr(), alpha, C.byref(conv),
+                                          _stream(stream)))
+        return m
 
 
 class Lut:

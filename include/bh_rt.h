@@ -57,6 +57,53 @@ void bh_torus_defaults(BH_TorusParams *torus);  /* r_in 6, r_peak 12, width 3, n
 /* Fill grid->cells (already allocated: n_r * n_theta * n_phi float4). */
 int bh_grmhd_synthetic(const BH_GrmhdGrid *grid, const BH_TorusParams *torus, void *stream);
 
+/* ---- ingestion of simulation output ---------------------------------------
+ *
+ * A dataset written by the reference's tools/nubhlight_pack.cpp: a JSON
+ * metadata file ("format" "RGBA32F", "bin" or legacy "binary_file": the blob
+ * next to it, "grid_dims" [n_r, n_theta, n_phi], optional
+ * "checksum_fnv1a64", "channels", "min", "max", "r_min", "r_max") and a blob
+ * of float4 samples, raw values of four fields (rho, u, v1, v2 by default),
+ * index (i_r n_theta + i_theta) n_phi + i_phi. Its sample positions follow the
+ * reference renderer's 3-D texture (src/cuda/device_physics.cuh:1789-1829):
+ * r_i = r_min + (i + 1/2)(r_max - r_min) / n_r (clamped outside), theta_j =
+ * (j + 1/2) pi / n_theta, phi_k = (k + 1/2) 2 pi / n_phi (periodic).
+ * Replaces loadGrmhdPackedTexture (src/grmhd_packed_loader.h:70-71). */
+typedef struct BH_PackedGrmhdInfo {
+    int32_t n_r, n_theta, n_phi, reserved;
+    float r_min, r_max;     /* radial extent [M] ("r_min", "r_max"; 1 and 50 when absent) */
+    float min_value[4], max_value[4];  /* per-channel ranges from the metadata (0 when absent) */
+    char channels[4][32];   /* field names */
+} BH_PackedGrmhdInfo;
+
+/* Parse and validate the metadata at json_path and read its blob: format
+ * RGBA32F, four channels, blob size n_r n_theta n_phi 4 floats, FNV-1a 64
+ * checksum when present. host_samples (n_r n_theta n_phi 4 floats, may be
+ * NULL: metadata only) receives the samples. Host only; no device work. */
+int bh_grmhd_packed_read(const char *json_path, BH_PackedGrmhdInfo *info, float *host_samples,
+                         int64_t capacity_floats);
+
+/* From the fields to the emitting medium (channel 0 rho, channel 1 u, the
+ * internal energy density, both in code units):
+ *   n_e = n_scale rho,  Theta_e = theta_scale u / rho,  |B| = b_scale sqrt(u)
+ * (temperature from u / rho; magnetic pressure a fixed fraction of the gas
+ * pressure). The scales are the caller's unit choice. */
+typedef struct BH_PackedConversion {
+    double n_scale;      /* cm^-3 per unit rho (1e5) */
+    double theta_scale;  /* Theta_e per unit u / rho (10) */
+    double b_scale;      /* gauss per unit sqrt(u) (30) */
+} BH_PackedConversion;
+
+void bh_packed_conversion_defaults(BH_PackedConversion *conv);
+
+/* Fill grid->cells (device) by sampling packed frames (device float4 arrays
+ * as read above) trilinearly at every grid node, blending frame_left and
+ * frame_right as (1 - alpha) left + alpha right (frame_right may be NULL:
+ * alpha ignored), then converting. The reference blends two texture frames
+ * the same way (device_physics.cuh:1816-1828). */
+int bh_grmhd_from_packed(const BH_GrmhdGrid *grid, const BH_PackedGrmhdInfo *info, const void *frame_left,
+                         const void *frame_right, double alpha, const BH_PackedConversion *conv, void *stream);
+
 /* Thermal synchrotron table: float [n_theta][n_x] of ln(j_nu / (n_e nu_B))
  * (CGS emissivity per unit electron density and gyrofrequency) at nodes of
  * log Theta_e and log x (x = nu / nu_s, nu_s = 3/2 nu_B Theta_e^2) evenly
