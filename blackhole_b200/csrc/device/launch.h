@@ -195,8 +195,6 @@ typedef struct BhkShade {
   float lut_r_min, lut_r_max, spec_r_min, spec_r_max;  // table domains in r / rs = r [M] / 2
   float cphi, sphi;      // camera azimuth (rotates escape directions into the world frame)
   unsigned long long tex_emissivity, tex_spectral, tex_galaxy, tex_equirect;
-  float exposure;        // > 0: exposure then ACES tone map; 0: linear output
-  float pad;
 } BhkShade;
 int bhk_legacy_set_blackbody(const float *rgb_table, int n, float log2_t0, float log2_t1);
 int bhk_legacy_shade(const BhkShade *s, const int32_t *cls, const double *r_hit, const double *g, const double *flux,
@@ -205,6 +203,15 @@ int bhk_legacy_lensing(int64_t n, const int32_t *cls, const double *r_hit, const
                        void *stream);
 int bhk_legacy_disk_texture(double a, double r_isco, double r_out, double nt_flux_peak, double incl, float t_peak,
                             int width, int height, float *rgba, void *stream);
+
+// Bloom and tone mapping (postprocess.cu). Taps: the normalized Gaussians
+// of half-width 4, 8, 16, 32 (sigma = r / 2), 2r + 1 each, concatenated.
+typedef struct BhkPostTaps {
+  float w[124];
+} BhkPostTaps;
+int64_t bhk_post_scratch_floats(int w, int h);
+int bhk_post_process(float *fb, int w, int h, const BhkPostTaps *taps, float threshold, float strength,
+                     float exposure, float *scratch, void *stream);
 
 int bhk_fma_probe(int fp64, int iters, int repeats, double *tflops);
 

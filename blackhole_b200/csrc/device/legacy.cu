@@ -80,8 +80,6 @@ __global__ void __launch_bounds__(256) k_legacy_shade(const __grid_constant__ Bh
     }
     col = make_float3(b.x * s.background_intensity, b.y * s.background_intensity, b.z * s.background_intensity);
   }
-  if (s.exposure > 0.0f)
-    col = make_float3(aces(s.exposure * col.x), aces(s.exposure * col.y), aces(s.exposure * col.z));
   rgba[i] = make_float4(col.x, col.y, col.z, 1.0f);
 }
 

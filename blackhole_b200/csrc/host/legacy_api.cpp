@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <numbers>
@@ -98,6 +99,8 @@ struct Scratch {
   double *r_hit = nullptr, *g = nullptr, *flux = nullptr;
   float *esc_dir = nullptr;
   unsigned long long *counter = nullptr;
+  float *post = nullptr;  // bloom planes and composite of bhb_cuda_postprocess
+  int64_t post_cap = 0;
   bool blackbody = false;
   int sms = 0;
 };
@@ -217,7 +220,7 @@ int launch_shape(const Scratch &sc, int64_t n, BhkLaunch *L) {
 }
 
 // Trace and shade one frame into the device framebuffer.
-int render(void *fb, const BH_LaunchParams *lp, int variant, float exposure, cudaStream_t st) {
+int render(void *fb, const BH_LaunchParams *lp, int variant, cudaStream_t st) {
   if (!fb) return fail_msg("legacy: framebuffer is NULL");
   if (!lp) return fail_msg("legacy: params is NULL");
   if (variant >= BH_KERNEL_COUNT) return fail_msg("legacy: unknown kernel variant %d", variant);
@@ -256,27 +259,110 @@ int render(void *fb, const BH_LaunchParams *lp, int variant, float exposure, cud
   sh.tex_spectral = g_lut[2];
   sh.tex_galaxy = g_lut[4];
   sh.tex_equirect = g_equirect;
-  sh.exposure = exposure;
   if (bhk_legacy_shade(&sh, sc->cls, sc->r_hit, sc->g, sc->flux, sc->esc_dir, static_cast<float *>(fb), st) != 0)
     return cuda_check(cudaGetLastError(), "k_legacy_shade launch");
   return 0;
 }
 
-// The Blender bridge's camera: on the (y, z) circle of radius observer_r
-// [rs] at the inclination from +z, looking at the origin; right = forward x
-// (0, 1, 0), up = right x forward (src/blender_bridge/cuda_renderer.cu:425-498,
-// rs = 1, step 0.08, max_dist 500, max_steps 600, disk lit 0.35, background 0.8).
-void bridge_params(BH_LaunchParams *p, float spin, float observer_r, float incl, float fov, int w, int h) {
+// ---- bridge defaults and environment overrides -----------------------------------
+//
+// The bridge reads its render settings from BLACKHOLE_BRIDGE_* variables
+// (src/blender_bridge/cuda_renderer.cu:28-68): an empty or unparsable value
+// keeps the default; a flag is off for "0", "false", "FALSE", "off", "OFF".
+
+float env_float(const char *name, float fallback) {
+  const char *raw = std::getenv(name);
+  if (!raw || !*raw) return fallback;
+  char *end = nullptr;
+  const float v = std::strtof(raw, &end);
+  return end != raw ? v : fallback;
+}
+
+int env_int(const char *name, int fallback) {
+  const char *raw = std::getenv(name);
+  if (!raw || !*raw) return fallback;
+  char *end = nullptr;
+  const long v = std::strtol(raw, &end, 10);
+  return end != raw ? int(v) : fallback;
+}
+
+int env_flag(const char *name, int fallback) {
+  const char *raw = std::getenv(name);
+  if (!raw || !*raw) return fallback;
+  for (const char *off : {"0", "false", "FALSE", "off", "OFF"})
+    if (std::strcmp(raw, off) == 0) return 0;
+  return 1;
+}
+
+// Bardeen-Press-Teukolsky prograde ISCO in rs (= 2 M), in float as the
+// bridge evaluates it (cuda_renderer.cu:433-439).
+float bridge_isco_rs(float a) {
+  const float z1 = 1.0f + std::pow(1.0f - a * a, 1.0f / 3.0f) *
+                              (std::pow(1.0f + a, 1.0f / 3.0f) + std::pow(1.0f - a, 1.0f / 3.0f));
+  const float z2 = std::sqrt(3.0f * a * a + z1 * z1);
+  return 0.5f * (3.0f + z2 - std::sqrt((3.0f - z1) * (3.0f + z1 + 2.0f * z2)));
+}
+
+// Everything but the camera (cuda_renderer.cu:425-447, 520-522).
+void bridge_common(BH_LaunchParams *p, float spin, float fov, int w, int h) {
   std::memset(p, 0, sizeof(*p));
   p->rs = 1.0f;
   p->spin = spin;
-  p->isco = float(0.5 * bhh::isco_prograde(1.0, std::clamp(double(spin), -0.999999, 0.999999)));
-  p->step_size = 0.08f;
+  p->isco = bridge_isco_rs(spin);
+  p->step_size = env_float("BLACKHOLE_BRIDGE_STEP_SIZE", 0.08f);
   p->fov_scale = std::max(fov, 0.05f);
-  p->max_dist = 500.0f;
-  p->max_steps = 600;
+  p->max_dist = env_float("BLACKHOLE_BRIDGE_MAX_DIST", 500.0f);
+  p->max_steps = env_int("BLACKHOLE_BRIDGE_MAX_STEPS", 600);
   p->width = w;
   p->height = h;
+}
+
+// Feature switches and the background layers, after the camera is placed
+// (cuda_renderer.cu:500-552; the layer offsets follow the camera position).
+void bridge_features(BH_LaunchParams *p) {
+  p->frame_shift_x = env_float("BLACKHOLE_BRIDGE_FRAME_SHIFT_X", 0.0f);
+  p->frame_shift_y = env_float("BLACKHOLE_BRIDGE_FRAME_SHIFT_Y", 0.0f);
+  p->adisk_enabled = env_flag("BLACKHOLE_BRIDGE_ADISK_ENABLED", 1);
+  p->redshift_enabled = env_flag("BLACKHOLE_BRIDGE_REDSHIFT_ENABLED", 1);
+  p->kerr_enabled = std::fabs(p->spin) > 1e-6f ? 1 : 0;
+  p->use_luts = 0;
+  p->time_sec = 0.0f;
+  p->doppler_strength = env_float("BLACKHOLE_BRIDGE_DOPPLER_STRENGTH", 1.0f);
+  p->background_intensity = env_float("BLACKHOLE_BRIDGE_BACKGROUND_INTENSITY", 0.8f);
+  p->background_enabled = env_flag("BLACKHOLE_BRIDGE_BACKGROUND_ENABLED", 1);
+  p->photon_glow_strength = env_float("BLACKHOLE_BRIDGE_PHOTON_GLOW_STRENGTH", 1.0f);
+  constexpr float deg = std::numbers::pi_v<float> / 180.0f;
+  p->background_yaw_rad = env_float("BLACKHOLE_BRIDGE_BACKGROUND_YAW_DEG", 0.0f) * deg;
+  p->background_pitch_rad = env_float("BLACKHOLE_BRIDGE_BACKGROUND_PITCH_DEG", 0.0f) * deg;
+  p->background_filter_radius = env_float("BLACKHOLE_BRIDGE_BACKGROUND_FILTER_RADIUS", 0.0f);
+  const float parallax = env_float("BLACKHOLE_BRIDGE_BACKGROUND_PARALLAX_STRENGTH", 0.0006f);
+  const float drift = env_float("BLACKHOLE_BRIDGE_BACKGROUND_DRIFT_STRENGTH", 0.01f);
+  static const char *const kVar[3][4] = {
+      {"BLACKHOLE_BRIDGE_BACKGROUND_LAYER0_DEPTH", "BLACKHOLE_BRIDGE_BACKGROUND_LAYER0_SCALE",
+       "BLACKHOLE_BRIDGE_BACKGROUND_LAYER0_INTENSITY", "BLACKHOLE_BRIDGE_BACKGROUND_LAYER0_LOD_BIAS"},
+      {"BLACKHOLE_BRIDGE_BACKGROUND_LAYER1_DEPTH", "BLACKHOLE_BRIDGE_BACKGROUND_LAYER1_SCALE",
+       "BLACKHOLE_BRIDGE_BACKGROUND_LAYER1_INTENSITY", "BLACKHOLE_BRIDGE_BACKGROUND_LAYER1_LOD_BIAS"},
+      {"BLACKHOLE_BRIDGE_BACKGROUND_LAYER2_DEPTH", "BLACKHOLE_BRIDGE_BACKGROUND_LAYER2_SCALE",
+       "BLACKHOLE_BRIDGE_BACKGROUND_LAYER2_INTENSITY", "BLACKHOLE_BRIDGE_BACKGROUND_LAYER2_LOD_BIAS"}};
+  static const float kDefault[3][4] = {{0.2f, 1.0f, 1.0f, 0.0f}, {0.5f, 1.08f, 0.6f, 1.0f}, {0.9f, 1.16f, 0.35f, 2.0f}};
+  const float px = p->cam_pos[0] * parallax, py = p->cam_pos[1] * parallax;
+  const float dx = std::cos(p->time_sec * 0.02f) * drift, dy = std::sin(p->time_sec * 0.02f) * drift;
+  for (int i = 0; i < 3; ++i) {
+    const float depth = env_float(kVar[i][0], kDefault[i][0]);
+    p->background_layer_params[4 * i + 0] = dx + px * depth;
+    p->background_layer_params[4 * i + 1] = dy + py * depth;
+    p->background_layer_params[4 * i + 2] = env_float(kVar[i][1], kDefault[i][1]);
+    p->background_layer_params[4 * i + 3] = env_float(kVar[i][2], kDefault[i][2]);
+    p->background_layer_lod_bias[i] = std::max(env_float(kVar[i][3], kDefault[i][3]), 0.0f);
+  }
+  p->adisk_lit = env_float("BLACKHOLE_BRIDGE_ADISK_LIT", 0.35f);
+}
+
+// The Blender bridge's camera: on the (y, z) circle of radius observer_r
+// [rs] at the inclination from +z, looking at the origin; right = forward x
+// (0, 1, 0), up = right x forward (cuda_renderer.cu:452-492).
+void bridge_params(BH_LaunchParams *p, float spin, float observer_r, float incl, float fov, int w, int h) {
+  bridge_common(p, spin, fov, w, h);
   const float ci = std::cos(incl), si = std::sin(incl);
   p->cam_pos[0] = 0.0f;
   p->cam_pos[1] = observer_r * si;
@@ -296,26 +382,70 @@ void bridge_params(BH_LaunchParams *p, float spin, float observer_r, float incl,
     p->cam_basis[3 + k] = u[k];
     p->cam_basis[6 + k] = f[k];
   }
-  p->adisk_enabled = 1;
-  p->redshift_enabled = 1;
-  p->kerr_enabled = std::fabs(spin) > 1e-6f ? 1 : 0;
-  p->doppler_strength = 1.0f;
-  p->background_intensity = 0.8f;
-  p->background_enabled = 1;
-  p->photon_glow_strength = 1.0f;
-  p->adisk_lit = 0.35f;
+  bridge_features(p);
 }
 
-constexpr float kBridgeExposure = 12.0f;  // the bridge's exposure gain before tone mapping
+// ---- bloom and tone mapping -------------------------------------------------------
 
-// Render to a temporary device framebuffer, copy to the host buffer.
+// The normalized Gaussian taps of half-width 4, 8, 16, 32 with sigma = r / 2,
+// evaluated in float as the reference's blur passes do
+// (cuda_postprocess.cu:42-64): g = exp(-dx^2 / (2 sigma^2)), divided by their sum.
+BhkPostTaps post_taps() {
+  BhkPostTaps t{};
+  int off = 0;
+  for (int r : {4, 8, 16, 32}) {
+    const float sigma = float(r) * 0.5f, inv2s2 = 1.0f / (2.0f * sigma * sigma);
+    float wt = 0.0f;
+    for (int dx = -r; dx <= r; ++dx) wt += std::exp(-float(dx * dx) * inv2s2);
+    const float inv = 1.0f / wt;
+    for (int dx = -r; dx <= r; ++dx) t.w[off + dx + r] = std::exp(-float(dx * dx) * inv2s2) * inv;
+    off += 2 * r + 1;
+  }
+  return t;
+}
+
+// Bloom (bright-pass over the threshold, four blur scales, added with the
+// strength), then exposure, vignette, ACES and gamma, in place on the
+// float4 framebuffer. Caller holds g_mu.
+int postprocess_locked(float *fb, int w, int h, float threshold, float strength, float exposure, cudaStream_t st) {
+  if (!fb) return fail_msg("postprocess: framebuffer is NULL");
+  if (w <= 0 || h <= 0) return fail_msg("postprocess: image size %dx%d", w, h);
+  if ((int64_t)w * h > (int64_t(1) << 31)) return fail_msg("postprocess: image exceeds 2^31 pixels");
+  Scratch *sc = nullptr;
+  if (scratch(0, &sc) != 0) return -1;
+  const int64_t need = bhk_post_scratch_floats(w, h);
+  if (need > sc->post_cap) {
+    if (sc->post) cudaFree(sc->post);
+    sc->post = nullptr;
+    sc->post_cap = 0;
+    if (int rc = cuda_check(cudaMalloc(reinterpret_cast<void **>(&sc->post), size_t(need) * 4),
+                            "cudaMalloc(postprocess scratch)"))
+      return rc;
+    sc->post_cap = need;
+  }
+  static const BhkPostTaps taps = post_taps();
+  if (bhk_post_process(fb, w, h, &taps, threshold, strength, exposure, sc->post, st) != 0)
+    return cuda_check(cudaGetLastError(), "postprocess launch");
+  return 0;
+}
+
+// Render to a temporary device framebuffer, post-process as the bridge does
+// (bloom threshold 1, strength 0, exposure 12 unless overridden:
+// cuda_renderer.cu:665-673), copy to the host buffer.
 int render_to_host(const BH_LaunchParams *lp, float *out_rgba) {
   if (!out_rgba) return fail_msg("bridge: output buffer is NULL");
   if (!(lp->width > 0 && lp->height > 0)) return fail_msg("bridge: image size %dx%d", lp->width, lp->height);
   const size_t bytes = size_t(lp->width) * size_t(lp->height) * 16;
   void *fb = nullptr;
   if (int rc = cuda_check(cudaMalloc(&fb, bytes), "cudaMalloc(bridge framebuffer)")) return rc;
-  int rc = render(fb, lp, BH_KERNEL_FP32_BASELINE, kBridgeExposure, nullptr);
+  int rc = render(fb, lp, BH_KERNEL_FP32_BASELINE, nullptr);
+  if (rc == 0) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    rc = postprocess_locked(static_cast<float *>(fb), lp->width, lp->height,
+                            env_float("BLACKHOLE_BRIDGE_BLOOM_THRESHOLD", 1.0f),
+                            env_float("BLACKHOLE_BRIDGE_BLOOM_STRENGTH", 0.0f),
+                            env_float("BLACKHOLE_BRIDGE_EXPOSURE", 12.0f), nullptr);
+  }
   if (rc == 0) rc = cuda_check(cudaMemcpy(out_rgba, fb, bytes, cudaMemcpyDeviceToHost), "bridge copy-out");
   cudaFree(fb);
   return rc;
@@ -326,7 +456,7 @@ int render_to_host(const BH_LaunchParams *lp, float *out_rgba) {
 // ---- kernel launch ABI ----------------------------------------------------------
 
 int bh_launch_geodesic_kernel(void *framebuffer, const BH_LaunchParams *params, int variant, void *stream) {
-  return render(framebuffer, params, variant, 0.0f, static_cast<cudaStream_t>(stream));
+  return render(framebuffer, params, variant, static_cast<cudaStream_t>(stream));
 }
 
 int bh_select_kernel_variant(void) { return BH_KERNEL_FP32_BASELINE; }
@@ -376,7 +506,7 @@ int bhCudaRenderFrame(BH_CudaBackend *b, const BH_LaunchParams *params) {
   if (params->width != b->width || params->height != b->height)
     return fail_msg("backend: params are %dx%d, framebuffer %dx%d (bhCudaResize first)", params->width,
                     params->height, b->width, b->height);
-  if (render(b->fb, params, b->variant, 0.0f, b->stream) != 0) return -1;
+  if (render(b->fb, params, b->variant, b->stream) != 0) return -1;
   return cuda_check(cudaStreamSynchronize(b->stream), "bhCudaRenderFrame");
 }
 
@@ -443,8 +573,11 @@ int bhbCudaResetDevice(void) {
   if (dev >= 0 && dev < kMaxDevices) {
     Scratch &s = g_scratch[dev];
     if (s.base) cudaFree(s.base);
+    if (s.post) cudaFree(s.post);
     s.base = nullptr;
     s.cap = 0;
+    s.post = nullptr;
+    s.post_cap = 0;
   }
   return 0;
 }
@@ -465,9 +598,10 @@ int bhbCudaRenderRaytracedView(float spin, const float *camPos, const float *cam
                                int height, float *outRgba) {
   if (!camPos || !camBasis) return fail_msg("bridge: camera position or basis is NULL");
   BH_LaunchParams p;
-  bridge_params(&p, spin, 1.0f, 0.0f, fovScale, width, height);
+  bridge_common(&p, spin, fovScale, width, height);  // cuda_renderer.cu:557-585
   std::memcpy(p.cam_pos, camPos, sizeof(p.cam_pos));
   std::memcpy(p.cam_basis, camBasis, sizeof(p.cam_basis));
+  bridge_features(&p);
   return render_to_host(&p, outRgba);
 }
 
@@ -577,6 +711,15 @@ int bhbCudaTraceGeodesics(double aStar, double observerRRg, double inclinationRa
   if (rc == 0) rc = cuda_check(cudaMemcpy(outCounts, cnt, b_cnt, cudaMemcpyDeviceToHost), "counts copy-out");
   cudaFree(d);
   return rc;
+}
+
+int bhb_cuda_postprocess(float *d_framebuffer, int width, int height, float bloom_threshold, float bloom_strength,
+                         float exposure_gain, float /*time_sec: the reference's film grain is not implemented*/) {
+  std::lock_guard<std::mutex> lock(g_mu);
+  if (int rc = postprocess_locked(d_framebuffer, width, height, bloom_threshold, bloom_strength, exposure_gain,
+                                  nullptr))
+    return rc;
+  return cuda_check(cudaStreamSynchronize(nullptr), "bhb_cuda_postprocess");
 }
 
 int bhb_cuda_render_raytraced(float spin, float observer_r, float inclination_rad, int width, int height,

@@ -55,16 +55,27 @@ def isco_prograde(a: float) -> float:
     return 3 + z2 - math.sqrt((3 - z1) * (3 + z1 + 2 * z2))
 
 
+def bridge_isco_rs(spin: float) -> float:
+    """The bridge's ISCO in rs, in float32 (src/blender_bridge/cuda_renderer.cu:433-439)."""
+    f32 = np.float32
+    a = f32(spin)
+    third = f32(1.0) / f32(3.0)
+    z1 = f32(1) + np.power(f32(1) - a * a, third) * (np.power(f32(1) + a, third) + np.power(f32(1) - a, third))
+    z2 = np.sqrt(f32(3) * a * a + z1 * z1)
+    return float(f32(0.5) * (f32(3) + z2 - np.sqrt((f32(3) - z1) * (f32(3) + z1 + f32(2) * z2))))
+
+
 def bridge_params(spin: float, observer_r: float, incl: float, fov: float, width: int, height: int) -> LaunchParams:
-    """The Blender bridge's camera and defaults (legacy_api.cpp bridge_params,
-    after src/blender_bridge/cuda_renderer.cu:425-498): camera on the (y, z)
-    circle of radius observer_r [rs] at the inclination from +z, looking at
-    the origin, basis columns right = forward x (0, 1, 0), up, forward."""
+    """The Blender bridge's camera and defaults with no BLACKHOLE_BRIDGE_*
+    overrides set (legacy_api.cpp bridge_params, after
+    src/blender_bridge/cuda_renderer.cu:425-552): camera on the (y, z) circle
+    of radius observer_r [rs] at the inclination from +z, looking at the
+    origin, basis columns right = forward x (0, 1, 0), up, forward."""
     f32 = np.float32
     p = LaunchParams()
     p.rs = 1.0
     p.spin = spin
-    p.isco = 0.5 * isco_prograde(min(max(spin, -0.999999), 0.999999))
+    p.isco = bridge_isco_rs(spin)
     p.step_size = 0.08
     p.fov_scale = max(fov, 0.05)
     p.max_dist = 500.0
@@ -87,6 +98,13 @@ def bridge_params(spin: float, observer_r: float, incl: float, fov: float, width
     p.background_intensity = 0.8
     p.background_enabled = 1
     p.photon_glow_strength = 1.0
+    drift, parallax = f32(0.01), f32(0.0006)
+    for i, (depth, scale, inten, lod) in enumerate(((0.2, 1.0, 1.0, 0.0), (0.5, 1.08, 0.6, 1.0),
+                                                    (0.9, 1.16, 0.35, 2.0))):
+        p.background_layer_params[4 * i:4 * i + 4] = [
+            float(drift + f32(p.cam_pos[0]) * parallax * f32(depth)),
+            float(f32(0.0) + f32(p.cam_pos[1]) * parallax * f32(depth)), scale, inten]
+        p.background_layer_lod_bias[i] = lod
     p.adisk_lit = 0.35
     return p
 
@@ -124,6 +142,7 @@ def _declare(lib: C.CDLL) -> C.CDLL:
     lib.bhb_cuda_render_raytraced_view.argtypes = lib.bhbCudaRenderRaytracedView.argtypes
     lib.bhb_cuda_render_lensing_map.argtypes = [f, f, f, i, i, vp]
     lib.bhb_cuda_render_disk_texture.argtypes = [f, f, f, i, i, vp]
+    lib.bhb_cuda_postprocess.argtypes = [vp, i, i, f, f, f, f]
     lib._legacy_declared = True
     return lib
 
@@ -150,6 +169,15 @@ def render_raytraced(spin: float, observer_r: float, incl: float, width: int, he
     else:
         check(lib.bhbCudaRenderRaytracedCamera(spin, observer_r, incl, fov, width, height, out.ctypes.data))
     return out
+
+
+def postprocess(framebuffer, width: int, height: int, bloom_threshold: float = 1.0, bloom_strength: float = 0.0,
+                exposure_gain: float = 12.0, time_sec: float = 0.0) -> None:
+    """bhb_cuda_postprocess in place on a device float4 framebuffer (a torch
+    tensor of width * height * 4 float32 on the current device)."""
+    lib = library()
+    check(lib.bhb_cuda_postprocess(C.c_void_p(framebuffer.data_ptr()), width, height, bloom_threshold,
+                                   bloom_strength, exposure_gain, time_sec))
 
 
 def lensing_map(a: float, r_obs: float, incl: float, width: int, height: int) -> np.ndarray:

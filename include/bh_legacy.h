@@ -187,8 +187,13 @@ int bhbCudaResetDevice(void);
 
 /* Camera on the (y, z) circle of radius observerR [rs] at inclination from
  * +z, looking at the hole, field of view fovScale (1.0 for the plain call);
- * the frame is exposed (x 12) and tone mapped (ACES fit of Narkowicz 2015)
- * into outRgba (host, width * height * 4 floats). */
+ * the frame is post-processed by bhb_cuda_postprocess (bloom threshold 1,
+ * strength 0, exposure 12) into outRgba (host, width * height * 4 floats).
+ * BLACKHOLE_BRIDGE_* environment variables override the render settings as in
+ * src/blender_bridge/cuda_renderer.cu:425-552, 665-673 (STEP_SIZE, MAX_DIST,
+ * MAX_STEPS, FRAME_SHIFT_X/Y, ADISK_ENABLED, REDSHIFT_ENABLED,
+ * DOPPLER_STRENGTH, BACKGROUND_*, PHOTON_GLOW_STRENGTH, ADISK_LIT,
+ * BLOOM_THRESHOLD, BLOOM_STRENGTH, EXPOSURE). */
 int bhbCudaRenderRaytraced(float spin, float observerR, float inclinationRad, int width, int height,
                            float *outRgba);
 int bhbCudaRenderRaytracedCamera(float spin, float observerR, float inclinationRad, float fovScale, int width,
@@ -223,6 +228,22 @@ int bhbCudaRenderDiskTexture(const struct BhbDiskParams *params, int width, int 
 int bhbCudaTraceGeodesics(double aStar, double observerRRg, double inclinationRad, double alphaMin, double alphaMax,
                           int nAlpha, double betaMin, double betaMax, int nBeta, int maxSteps, double stepSize,
                           float *outXyz, int *outCounts);
+
+/* Post-processing of a device float4 framebuffer (width * height RGBA), in
+ * place (src/blender_bridge/cuda_postprocess.cu:237-275): bloom = the sum over
+ * half-widths 4, 8, 16, 32 of the Gaussian blur (sigma = half-width / 2,
+ * clamped edges) of the bright-pass (colour scaled by max(0, L - threshold) / L,
+ * L the Rec. 709 luminance, 0 where L <= 0.001), added times bloom_strength
+ * (skipped when it is 0); then per pixel: x exposure_gain, x the vignette
+ * sqrt(max(0, 1 - d^2 / 2)) (d the distance from the centre in uv), the ACES
+ * fit of Narkowicz (2015) clamped to [0, 1], gamma 1 / 2.2, alpha 1. Red and
+ * blue are read at (int(u w), int(v h)) of the float uv, as the reference's
+ * chromatic-aberration lookup at strength 0 does. time_sec is accepted and
+ * unused (the reference's film grain is absent from its kernel too). Returns
+ * 0 after the work has finished, -1 on a NULL framebuffer, a non-positive
+ * size or a CUDA error. */
+int bhb_cuda_postprocess(float *d_framebuffer, int width, int height, float bloom_threshold, float bloom_strength,
+                         float exposure_gain, float time_sec);
 
 /* snake_case aliases used by the add-on's ctypes binding (float arguments). */
 int bhb_cuda_render_raytraced(float spin, float observer_r, float inclination_rad, int width, int height,

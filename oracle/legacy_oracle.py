@@ -1,9 +1,10 @@
 """Numpy restatement of the legacy RGBA layer (test infrastructure only).
 
-Mirrors blackhole_b200/csrc/host/legacy_api.cpp and device/legacy.cu: the
-camera derived from BH_LaunchParams, the blackbody colour table, the disk /
-background shading, the ACES tone map, the lensing-map channels and the disk
-emission texture. Geometry (which pixel hits what) comes from the C++ oracle
+Mirrors blackhole_b200/csrc/host/legacy_api.cpp, device/legacy.cu and
+device/postprocess.cu: the camera derived from BH_LaunchParams, the blackbody
+colour table, the disk / background shading, the bridge's post-processing
+(bloom, exposure, vignette, ACES, gamma: src/blender_bridge/cuda_postprocess.cu),
+the lensing-map channels and the disk emission texture. Geometry (which pixel hits what) comes from the C++ oracle
 (pyoracle.Oracle.trace_camera / trace_pixels); only tests import this.
 """
 from __future__ import annotations
@@ -93,7 +94,7 @@ def scene_of(kw: dict):
     return s
 
 
-def shade(fields: dict, p, cphi: float, sphi: float, exposure: float = 0.0, tab=None) -> np.ndarray:
+def shade(fields: dict, p, cphi: float, sphi: float, tab=None) -> np.ndarray:
     """RGBA [n][4] of legacy.cu k_legacy_shade without textures (black background)."""
     tab = blackbody_table() if tab is None else tab
     cls = fields["cls"]
@@ -105,9 +106,53 @@ def shade(fields: dict, p, cphi: float, sphi: float, exposure: float = 0.0, tab=
     inten = np.float32(p.adisk_lit) * (gg * gg) * (gg * gg) * F
     col = blackbody(t, tab) * inten[:, None]
     col[cls != 1] = 0.0
-    if exposure > 0:
-        col = aces(exposure * col)
     return np.concatenate([col, np.ones((n, 1), np.float32)], axis=1)
+
+
+def _blur(img: np.ndarray, r: int, axis: int) -> np.ndarray:
+    """Normalized Gaussian of half-width r, sigma = r / 2, clamped edges
+    (cuda_postprocess.cu:42-98), along one axis of an [h, w, 3] image."""
+    dx = np.arange(-r, r + 1)
+    g = np.exp(-(dx * dx) / (2.0 * (0.5 * r) ** 2))
+    g /= g.sum()
+    n = img.shape[axis]
+    out = np.zeros_like(img)
+    for k, d in enumerate(dx):
+        idx = np.clip(np.arange(n) + d, 0, n - 1)
+        out += g[k] * np.take(img, idx, axis=axis)
+    return out
+
+
+def postprocess(fb: np.ndarray, threshold: float, strength: float, exposure: float) -> np.ndarray:
+    """bhb_cuda_postprocess of an [h, w, 4] framebuffer (cuda_postprocess.cu:237-275):
+    bright-pass, blur at half-widths 4, 8, 16, 32 of that same bright-pass,
+    summed and added times the strength; then exposure, vignette, ACES,
+    gamma 1/2.2, with red and blue read at (int(u w), int(v h)) of the
+    float32 uv. Float64 arithmetic except the uv and that index."""
+    h, w = fb.shape[:2]
+    col = fb[..., :3].astype(np.float64)
+    if strength != 0.0:
+        lum = 0.2126 * col[..., 0] + 0.7152 * col[..., 1] + 0.0722 * col[..., 2]
+        scale = np.where(lum > 0.001, np.maximum(0.0, lum - threshold) / np.where(lum > 0.001, lum, 1.0), 0.0)
+        bright = col * scale[..., None]
+        acc = np.zeros_like(col)
+        for r in (4, 8, 16, 32):
+            acc += _blur(_blur(bright, r, 1), r, 0)
+        col = col + strength * acc
+    f32 = np.float32
+    u = np.arange(w, dtype=f32) / f32(w)
+    v = np.arange(h, dtype=f32) / f32(h)
+    rx = np.clip(np.floor(u * f32(w)).astype(np.int64), 0, w - 1)
+    ry = np.clip(np.floor(v * f32(h)).astype(np.int64), 0, h - 1)
+    red = col[ry[:, None], rx[None, :], 0]
+    blue = col[ry[:, None], rx[None, :], 2]
+    out = np.stack([red, col[..., 1], blue], axis=-1)
+    uu, vv = np.meshgrid(u.astype(np.float64), v.astype(np.float64))
+    d2 = (uu - 0.5) ** 2 + (vv - 0.5) ** 2
+    vig = np.sqrt(np.maximum(1.0 - d2 * 0.5, 0.0))
+    out = aces(out * exposure * vig[..., None])
+    out = np.maximum(out, 0.0) ** (1.0 / 2.2)
+    return np.concatenate([out, np.ones((h, w, 1))], axis=-1)
 
 
 def lensing(fields: dict) -> np.ndarray:

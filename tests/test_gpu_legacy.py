@@ -1,11 +1,15 @@
 """The reference renderer's launch ABI on the GPU (include/bh_legacy.h), through
 the C ABI: camera rays, shading, the backend, the Blender-bridge calls, the
-lensing map, the disk texture and the geodesic paths, each against the CPU
-oracle (kerr_oracle.hpp camera/paths, oracle/legacy_oracle.py shading)."""
+post-processing, the lensing map, the disk texture and the geodesic paths,
+each against the CPU oracle (kerr_oracle.hpp camera/paths,
+oracle/legacy_oracle.py shading and post-processing), and the post-processing
+also against the reference's own kernels (oracle/_ref/libbh_ref_post.so, built
+from src/blender_bridge/cuda_postprocess.cu)."""
 from __future__ import annotations
 
 import ctypes as C
 import math
+from pathlib import Path
 
 import numpy as np
 import pytest
@@ -107,16 +111,29 @@ def test_backend_renders_the_same_frame(cuda, leg, lib):
         L.bhCudaShutdown(b)
 
 
-def test_bridge_render_is_tonemapped_shading(cuda, leg, oracle):
-    spin, r_rs, incl, w, h = 0.8, 25.0, 1.25, 48, 36
+def _gather_source(w: int, h: int) -> np.ndarray:
+    """Flat index of the pixel each pixel's red and blue come from in the tone map."""
+    f32 = np.float32
+    rx = np.floor((np.arange(w, dtype=f32) / f32(w)) * f32(w)).astype(np.int64)
+    ry = np.floor((np.arange(h, dtype=f32) / f32(h)) * f32(h)).astype(np.int64)
+    return (ry[:, None] * w + rx[None, :]).ravel()
+
+
+def test_bridge_render_is_postprocessed_shading(cuda, leg, oracle, monkeypatch):
+    for var in ("BLACKHOLE_BRIDGE_EXPOSURE", "BLACKHOLE_BRIDGE_BLOOM_STRENGTH", "BLACKHOLE_BRIDGE_BLOOM_THRESHOLD"):
+        monkeypatch.delenv(var, raising=False)
+    spin, r_rs, incl, w, h = 0.8, 25.0, 1.25, 47, 36  # width 47: six columns take red and blue from the left
     img = leg.render_raytraced(spin, r_rs, incl, w, h).reshape(-1, 4)
     p = leg.bridge_params(spin, r_rs, incl, 1.0, w, h)
     ref, cf = _oracle_frame(oracle, p)
-    want = LO.shade(ref, p, cf[15], cf[16], exposure=12.0)
+    want = LO.postprocess(LO.shade(ref, p, cf[15], cf[16]).reshape(h, w, 4), 1.0, 0.0, 12.0).reshape(-1, 4)
     assert np.all(img[:, 3] == 1.0) and img.min() >= 0.0 and img.max() <= 1.0
-    same = (img[:, :3].sum(1) > 0) == (ref["cls"] == 1)
-    assert same.mean() >= 0.99
-    np.testing.assert_allclose(img[same], want[same], rtol=2e-4, atol=2e-6)
+    src = _gather_source(w, h)
+    assert (src != np.arange(w * h)).any()
+    agree = (img[:, 1] > 0) == (ref["cls"] == 1)  # green is the pixel's own
+    assert agree.mean() >= 0.99
+    ok = agree & agree[src]
+    np.testing.assert_allclose(img[ok], want[ok], rtol=2e-4, atol=2e-6)
     alias = np.zeros((h, w, 4), np.float32)
     assert leg.library().bhb_cuda_render_raytraced(spin, r_rs, incl, w, h, alias.ctypes.data) == 0
     np.testing.assert_array_equal(alias.reshape(-1, 4), img)
@@ -171,3 +188,81 @@ def test_trace_geodesics_matches_oracle_paths(cuda, leg, oracle):
     assert cnt.min() >= 2
     for k in range(len(cnt)):
         np.testing.assert_allclose(xyz[k, :cnt[k]], rxyz[k, :cnt[k]], rtol=1e-5, atol=1e-4)
+
+
+def _hdr_frame(w: int, h: int, seed: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    fb = rng.lognormal(-1.0, 1.5, (h, w, 4)).astype(np.float32)
+    fb[rng.random((h, w)) < 0.3] = 0.0  # black patches: luminance below 0.001
+    fb[..., 3] = rng.random((h, w)).astype(np.float32)
+    return fb
+
+
+@pytest.mark.parametrize("w,h,threshold,strength,exposure", [
+    (61, 37, 0.8, 0.6, 3.0), (130, 96, 1.0, 0.0, 12.0), (200, 70, 0.25, 1.5, 0.7), (5, 3, 0.5, 1.0, 2.0),
+    (1, 1, 0.1, 2.0, 1.0), (64, 200, 1.0, 0.3, 12.0)])
+def test_postprocess_matches_restatement(cuda, leg, w, h, threshold, strength, exposure):
+    fb = _hdr_frame(w, h, w * 1000 + h)
+    d = torch.from_numpy(fb).cuda().reshape(-1)
+    leg.postprocess(d, w, h, threshold, strength, exposure, 0.5)
+    got = d.cpu().numpy().reshape(h, w, 4)
+    want = LO.postprocess(fb, threshold, strength, exposure)
+    np.testing.assert_allclose(got, want, rtol=2e-5, atol=1e-6)
+
+
+def test_postprocess_rejects_bad_arguments(cuda, leg):
+    L = leg.library()
+    assert L.bhb_cuda_postprocess(None, 4, 4, 1.0, 0.0, 1.0, 0.0) == -1
+    d = torch.zeros(16 * 4, device="cuda")
+    assert L.bhb_cuda_postprocess(C.c_void_p(d.data_ptr()), 0, 4, 1.0, 0.0, 1.0, 0.0) == -1
+    assert L.bhb_cuda_postprocess(C.c_void_p(d.data_ptr()), 4, -1, 1.0, 0.0, 1.0, 0.0) == -1
+
+
+REF_POST = Path(__file__).resolve().parents[1] / "oracle" / "_ref" / "libbh_ref_post.so"
+
+
+@pytest.mark.skipif(not REF_POST.exists(), reason="reference post-processing build absent (oracle/_ref)")
+@pytest.mark.parametrize("w,h,threshold,strength,exposure", [(61, 37, 0.8, 0.6, 3.0), (160, 90, 1.0, 0.0, 12.0),
+                                                             (96, 130, 0.3, 1.2, 1.5)])
+def test_postprocess_matches_reference_build(cuda, leg, w, h, threshold, strength, exposure):
+    """Against the reference's own bhb_cuda_postprocess, compiled from its
+    source. Its tone map reads the left or upper neighbour's red and blue in
+    place, racing with that neighbour's write; those pixels are excluded."""
+    ref_lib = C.CDLL(str(REF_POST))
+    ref_lib.bhb_cuda_postprocess.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float,
+                                             C.c_float]
+    fb = _hdr_frame(w, h, 7 * w + h)
+    a = torch.from_numpy(fb).cuda().reshape(-1)
+    b = a.clone()
+    torch.cuda.synchronize()
+    assert ref_lib.bhb_cuda_postprocess(C.c_void_p(a.data_ptr()), w, h, threshold, strength, exposure, 0.0) == 0
+    torch.cuda.synchronize()
+    leg.postprocess(b, w, h, threshold, strength, exposure, 0.0)
+    ra, rb = a.cpu().numpy().reshape(-1, 4), b.cpu().numpy().reshape(-1, 4)
+    own = _gather_source(w, h) == np.arange(w * h)
+    assert own.mean() > 0.75
+    np.testing.assert_allclose(rb[own], ra[own], rtol=2e-5, atol=1e-6)
+    np.testing.assert_allclose(rb[:, 1], ra[:, 1], rtol=2e-5, atol=1e-6)  # green is always the pixel's own
+
+
+def test_bridge_environment_overrides(cuda, leg, oracle, monkeypatch):
+    """BLACKHOLE_BRIDGE_* variables reach the render and the post-processing
+    (src/blender_bridge/cuda_renderer.cu:425-552, 665-673): exposure 3 and
+    disk brightness 0.7 give the oracle's frame with those settings; an
+    unparsable value keeps the default."""
+    spin, r_rs, incl, w, h = 0.6, 30.0, 1.1, 40, 30
+    monkeypatch.setenv("BLACKHOLE_BRIDGE_EXPOSURE", "3")
+    monkeypatch.setenv("BLACKHOLE_BRIDGE_ADISK_LIT", "0.7")
+    monkeypatch.setenv("BLACKHOLE_BRIDGE_BLOOM_STRENGTH", "not-a-number")
+    img = leg.render_raytraced(spin, r_rs, incl, w, h).reshape(-1, 4)
+    p = leg.bridge_params(spin, r_rs, incl, 1.0, w, h)
+    p.adisk_lit = 0.7
+    ref, cf = _oracle_frame(oracle, p)
+    want = LO.postprocess(LO.shade(ref, p, cf[15], cf[16]).reshape(h, w, 4), 1.0, 0.0, 3.0).reshape(-1, 4)
+    agree = (img[:, 1] > 0) == (ref["cls"] == 1)
+    assert agree.mean() >= 0.99
+    ok = agree & agree[_gather_source(w, h)]
+    np.testing.assert_allclose(img[ok], want[ok], rtol=2e-4, atol=2e-6)
+    monkeypatch.setenv("BLACKHOLE_BRIDGE_ADISK_ENABLED", "off")
+    dark = leg.render_raytraced(spin, r_rs, incl, w, h).reshape(-1, 4)
+    assert np.all(dark[:, :3] == 0.0)  # no disk, no background texture: black

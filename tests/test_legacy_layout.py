@@ -83,3 +83,27 @@ def test_bridge_camera_basis_is_orthonormal_and_looks_at_the_hole(lib, incl):
     pos = np.array(p.cam_pos, np.float64)
     assert np.allclose(B[:, 2], -pos / np.linalg.norm(pos), atol=1e-6)
     assert np.isclose(np.linalg.norm(pos), 40.0)
+
+
+def test_postprocess_restatement_properties():
+    """The post-processing restatement (oracle/legacy_oracle.py) on cases with
+    a closed form: a constant frame blurs to itself, so the composite adds
+    4 x strength x its bright-pass; above every pixel's luminance the bloom
+    is nothing; the tone map of 0 is 0 and saturates at 1."""
+    from oracle import legacy_oracle as LO
+
+    h, w = 9, 13
+    c = np.array([2.0, 1.0, 0.5], np.float32)
+    fb = np.broadcast_to(np.append(c, 0.25), (h, w, 4)).astype(np.float32)
+    lum = 0.2126 * 2.0 + 0.7152 * 1.0 + 0.0722 * 0.5
+    bright = c.astype(np.float64) * (lum - 0.4) / lum
+    composite = np.concatenate([np.broadcast_to(c + 0.5 * 4 * bright, (h, w, 3)), np.ones((h, w, 1))], -1)
+    plain = LO.postprocess(composite, 1e9, 0.0, 2.0)
+    np.testing.assert_allclose(LO.postprocess(fb, 0.4, 0.5, 2.0), plain, rtol=1e-12)
+    rng = np.random.default_rng(3)
+    x = rng.random((h, w, 4)).astype(np.float32)
+    np.testing.assert_array_equal(LO.postprocess(x, 10.0, 3.0, 1.5), LO.postprocess(x, 10.0, 0.0, 1.5))
+    out = LO.postprocess(np.zeros((h, w, 4), np.float32), 1.0, 1.0, 12.0)
+    assert np.all(out[..., :3] == 0.0) and np.all(out[..., 3] == 1.0)
+    out = LO.postprocess(np.full((h, w, 4), 1e6, np.float32), 1.0, 0.0, 12.0)
+    np.testing.assert_allclose(out[..., :3], 1.0)
