@@ -16,7 +16,7 @@ LIB_PATH = PKG_DIR / "lib" / "libblackhole_b200.so"
 # enum BH_PixelClass
 CLASS_CAPTURED, CLASS_DISK, CLASS_ESCAPED, CLASS_MAX_STEPS = 0, 1, 2, 3
 # enum BH_Integrator
-INTEGRATOR_RK4, INTEGRATOR_DP45 = 0, 1
+INTEGRATOR_RK4, INTEGRATOR_DP45, INTEGRATOR_ANALYTIC = 0, 1, 2
 # enum BH_Precision
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 # enum BH_PotentialForm

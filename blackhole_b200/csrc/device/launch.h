@@ -122,8 +122,11 @@ int bhh_prepare_image_launch(const struct BH_KerrScene *scene, BhkImageParams *p
 // Validates one scene and fills its kernel parameters (no device call).
 int bhh_make_params(const struct BH_KerrScene *scene, BhkImageParams *p);
 // Launches the image kernel of p->precision (work counter zeroed on stream).
+// The analytic integrator also needs a list of n_pix ints for the pixels it
+// leaves to the DP45 tracer: `list`, or the device's grow-only list when NULL
+// (its count lives in counter[1]; counter must hold two words).
 int bhh_launch_image(const BhkImageParams *p, const BhkImageOut *o, unsigned long long *counter, BhkLaunch L,
-                     void *stream);
+                     void *stream, int *list);
 int bhh_fail(const char *msg);
 // The current device's persistent-kernel work counter (allocated once).
 int bhh_work_counter(unsigned long long **counter);
@@ -212,6 +215,13 @@ typedef struct BhkPostTaps {
 int64_t bhk_post_scratch_floats(int w, int h);
 int bhk_post_process(float *fb, int w, int h, const BhkPostTaps *taps, float threshold, float strength,
                      float exposure, float *scratch, void *stream);
+
+// Closed-form tracer (trace_image_analytic.cu): pixels it does not cover go to list[0..*count).
+int bhk_trace_image_analytic(const BhkImageParams *p, const BhkImageOut *o, int *list, unsigned int *count,
+                             BhkLaunch L, void *stream);
+int bhk_trace_image_analytic_occupancy(int block, int *blocks_per_sm);
+int bhk_trace_list_fp64(const BhkImageParams *p, const BhkImageOut *o, const int *list, const unsigned int *count,
+                        unsigned long long *counter, BhkLaunch L, void *stream);
 
 int bhk_fma_probe(int fp64, int iters, int repeats, double *tflops);
 

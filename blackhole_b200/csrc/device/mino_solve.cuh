@@ -146,7 +146,9 @@ BHM_HD ThetaMotion theta_motion(double a2, double qTh, double lam, double u0, do
   const double m = a2 * zp;
   double s = fabs(u0) / sqrt(zp);  // sin chi_obs
   s = fmin(s, 1.0);
-  const T phi_obs = T(s) * carlson_rf<T>(T(w * (1.0 - s * s)), T(w + m * s * s), T(w));
+  // cos^2 chi_obs = pu0^2 / ((a^2 u0^2 + w) z+) (U(u0) = pu0^2): no cancellation near s = 1
+  const double c2 = pu0 * pu0 / ((a2 * u0 * u0 + w) * zp);
+  const T phi_obs = T(s) * carlson_rf<T>(T(w * c2), T(w + m * s * s), T(w));
   const T K = quarter_period<T>(T(w), T(m));
   const bool toward = (pu0 * u0) < 0.0;
   t.crosses = true;
@@ -506,7 +508,8 @@ BHM_HD double u_at(double a2, double qTh, double lam, double u0, double pu0, dou
   const double w = c0 / zp, m = a2 * zp, rz = sqrt(zp);
   const double s0 = fmax(-1.0, fmin(1.0, u0 / rz));
   const double K = (double)quarter_period<T>(T(w), T(m));
-  const double phi_x = s0 * (double)carlson_rf<T>(T(w * (1.0 - s0 * s0)), T(w + m * s0 * s0), T(w));  // odd in s0
+  const double c2 = pu0 * pu0 / ((a2 * u0 * u0 + w) * zp);  // cos^2 chi_obs, as in theta_motion
+  const double phi_x = s0 * (double)carlson_rf<T>(T(w * c2), T(w + m * s0 * s0), T(w));  // odd in s0
   const double phi_start = (pu0 >= 0.0) ? phi_x : 2.0 * K - phi_x;
   double total = phi_start + tau;
   const double n = floor(total / (2.0 * K));

@@ -69,11 +69,13 @@ extern "C" int bh_kerr_trace_image_host_noalloc(const BH_KerrScene *scene, const
                     h->phi_inf};
   const size_t bytes[10] = {4 * n, 4 * n, 4 * n, 8 * n * mc, 8 * n * mc, 8 * n * mc, 8 * n, 8 * n, 8 * n, 8 * n};
   size_t off[10];
-  size_t used = 256;  // work counter
+  size_t used = 256;  // work counter (and the analytic integrator's list count)
   for (int i = 0; i < 10; ++i) {
     off[i] = used;
     if (host[i]) used += round256(bytes[i]);
   }
+  const size_t list_off = used;  // the analytic integrator's fallback list
+  if (p.integrator == BH_INTEGRATOR_ANALYTIC) used += round256(4 * n);
   if (used > size_t(BH_NOALLOC_SCRATCH_BYTES)) {
     char msg[320];
     std::snprintf(msg, sizeof(msg),
@@ -95,7 +97,9 @@ extern "C" int bh_kerr_trace_image_host_noalloc(const BH_KerrScene *scene, const
                       static_cast<double *>(d[9])};
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   // bhh_launch_image zeroes the work counter on s before the launch.
-  if (bhh_launch_image(&p, &o, reinterpret_cast<unsigned long long *>(b), L, stream) != 0) return -1;
+  if (bhh_launch_image(&p, &o, reinterpret_cast<unsigned long long *>(b), L, stream,
+                       reinterpret_cast<int *>(b + list_off)) != 0)
+    return -1;
   for (int i = 0; i < 10; ++i) {
     if (!host[i]) continue;
     const cudaError_t e = cudaMemcpyAsync(host[i], d[i], bytes[i], cudaMemcpyDeviceToHost, s);

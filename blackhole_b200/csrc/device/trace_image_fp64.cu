@@ -234,6 +234,15 @@ __global__ void __launch_bounds__(128, 4) k_trace_image_fp64(const __grid_consta
 }
 
 template <int INTEG>
+__global__ void __launch_bounds__(128, 4) k_trace_list_fp64(const __grid_constant__ BhkImageParams p,
+                                                         const __grid_constant__ BhkImageOut o,
+                                                         const int *__restrict__ list,
+                                                         const unsigned int *__restrict__ count,
+                                                         unsigned long long *__restrict__ counter, int refill) {
+  trace_loop<INTEG>(bhsrc::ListSrc{p, o, list, count}, counter, refill);
+}
+
+template <int INTEG>
 __global__ void __launch_bounds__(128, 4) k_trace_batch_fp64(const __grid_constant__ BhkBatchDev b,
                                                           unsigned long long *__restrict__ counter, int refill) {
   if (threadIdx.x == 0) atomicMin(b.start_ns, bhsrc::globaltimer_ns());
@@ -364,6 +373,21 @@ extern "C" int bhk_trace_image_fp64(const BhkImageParams *p, const BhkImageOut *
     bhk::k_trace_image_fp64<1><<<launch.grid, launch.block, 0, s>>>(*p, *o, counter, launch.refill);
   e = cudaGetLastError();
   if (e != cudaSuccess) return set_err(e, "k_trace_image_fp64 launch");
+  return 0;
+}
+
+extern "C" int bhk_trace_list_fp64(const BhkImageParams *p, const BhkImageOut *o, const int *list,
+                                   const unsigned int *count, unsigned long long *counter, BhkLaunch L,
+                                   void *stream) {
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return set_err(e, "work-counter reset");
+  if (p->integrator == 0)
+    bhk::k_trace_list_fp64<0><<<L.grid, L.block, 0, s>>>(*p, *o, list, count, counter, L.refill);
+  else
+    bhk::k_trace_list_fp64<1><<<L.grid, L.block, 0, s>>>(*p, *o, list, count, counter, L.refill);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(e, "k_trace_list_fp64 launch");
   return 0;
 }
 

@@ -125,6 +125,10 @@ BH_KerrBatch *bh_kerr_batch_create(const BH_KerrScene *scenes, const BH_KerrImag
     b->prefix[i + 1] = b->prefix[i] + b->frames[i].p.n_pix;
   }
   b->n_total = b->prefix[n_frames];
+  if (scenes[0].integrator == BH_INTEGRATOR_ANALYTIC) {
+    fail_msg("the analytic integrator traces single frames (bh_kerr_trace_image); batches step RK4 or DP45");
+    return nullptr;
+  }
   b->integrator = scenes[0].integrator;
   b->precision = scenes[0].precision;
   if (cuda_check(cudaGetDevice(&b->device), "cudaGetDevice") ||

@@ -40,8 +40,10 @@ int cuda_fail(cudaError_t e, const char *what) {
 // ---- per-device scratch -----------------------------------------------------
 constexpr int kMaxDevices = 64;
 struct DeviceScratch {
-  unsigned long long *counter = nullptr;  // persistent-kernel work counter
+  unsigned long long *counter = nullptr;  // persistent-kernel work counter (+ list count in word 1)
   int sms = 0;
+  int *list = nullptr;  // pixels the analytic integrator leaves to DP45 (grow-only)
+  int64_t list_cap = 0;
 };
 std::array<DeviceScratch, kMaxDevices> g_scratch{};
 std::mutex g_scratch_mu;
@@ -120,7 +122,8 @@ int bh_kerr_scene_validate(const BH_KerrScene *s) {
   if (s->width < 0 || s->height < 0) return fail("negative image size %dx%d", s->width, s->height);
   if ((int64_t)s->width * s->height > (int64_t(1) << 31))
     return fail("image of %lld pixels exceeds 2^31", (long long)s->width * s->height);
-  if (s->integrator != BH_INTEGRATOR_RK4 && s->integrator != BH_INTEGRATOR_DP45)
+  if (s->integrator != BH_INTEGRATOR_RK4 && s->integrator != BH_INTEGRATOR_DP45 &&
+      s->integrator != BH_INTEGRATOR_ANALYTIC)
     return fail("unknown integrator %d", s->integrator);
   if (s->precision != BH_PRECISION_FP64 && s->precision != BH_PRECISION_MIXED)
     return fail("unknown precision %d", s->precision);
@@ -130,8 +133,8 @@ int bh_kerr_scene_validate(const BH_KerrScene *s) {
     return fail("max_crossings must be in [1, %d], got %d", BH_MAX_CROSSINGS, s->max_crossings);
   if (s->max_steps < 0) return fail("max_steps must be >= 0");
   if (!(s->step_coeff > 0.0) || !(s->step_rcap > 0.0)) return fail("step_coeff and step_rcap must be > 0");
-  if (s->integrator == BH_INTEGRATOR_DP45 && (!(s->rtol > 0.0) || !(s->atol > 0.0)))
-    return fail("DP45 needs rtol > 0 and atol > 0");
+  if (s->integrator != BH_INTEGRATOR_RK4 && (!(s->rtol > 0.0) || !(s->atol > 0.0)))
+    return fail("DP45 (and the analytic integrator's DP45 fallback) needs rtol > 0 and atol > 0");
   if (!(s->horizon_factor >= 1.0) || !(s->escape_factor > 0.0)) return fail("bad horizon/escape factor");
   if (!(s->disk_r_out > 0.0)) return fail("disk_r_out must be > 0");
   return 0;
@@ -193,7 +196,8 @@ int bhh_prepare_image_launch(const BH_KerrScene *scene, BhkImageParams *p, BhkLa
   if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute(SM count)");
   const int block = g_block_override ? g_block_override : 128;
   int per_sm = 0;
-  const int occ_rc = (p->precision == BH_PRECISION_MIXED)
+  const int occ_rc = (p->integrator == BH_INTEGRATOR_ANALYTIC) ? bhk_trace_image_analytic_occupancy(block, &per_sm)
+                     : (p->precision == BH_PRECISION_MIXED)
                          ? bhk_trace_image_mixed_occupancy(p->integrator, block, &per_sm)
                          : bhk_trace_image_fp64_occupancy(p->integrator, block, &per_sm);
   if (occ_rc != 0) return cuda_fail(cudaGetLastError(), "occupancy query");
@@ -216,8 +220,53 @@ int bhh_work_counter(unsigned long long **counter) {
   return 0;
 }
 
+// The analytic integrator: the closed-form kernel, then DP45 (at the scene's
+// precision) on the pixels it listed, over a persistent grid of that kernel.
+static int launch_analytic(const BhkImageParams *p, const BhkImageOut *o, unsigned long long *counter, BhkLaunch L,
+                           void *stream, int *list) {
+  int dev = 0, sms = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  if (!list) {
+    DeviceScratch *ds = nullptr;
+    if (device_scratch(&ds) != 0) return -1;
+    std::lock_guard<std::mutex> lk(g_scratch_mu);
+    if (ds->list_cap < p->n_pix) {
+      if (ds->list) cudaFree(ds->list);
+      ds->list = nullptr;
+      ds->list_cap = 0;
+      e = cudaMalloc(reinterpret_cast<void **>(&ds->list), size_t(p->n_pix) * sizeof(int));
+      if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(analytic fallback list)");
+      ds->list_cap = p->n_pix;
+    }
+    list = ds->list;
+  }
+  unsigned int *count = reinterpret_cast<unsigned int *>(counter + 1);
+  if (bhk_trace_image_analytic(p, o, list, count, L, stream) != 0)
+    return cuda_fail(cudaGetLastError(), "k_trace_image_analytic launch");
+  BhkImageParams q = *p;
+  q.integrator = BH_INTEGRATOR_DP45;
+  e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute(SM count)");
+  int per_sm = 0;
+  const int block = 128;
+  const int occ_rc = (q.precision == BH_PRECISION_MIXED) ? bhk_trace_image_mixed_occupancy(1, block, &per_sm)
+                                                         : bhk_trace_image_fp64_occupancy(1, block, &per_sm);
+  if (occ_rc != 0 || per_sm < 1) return cuda_fail(cudaGetLastError(), "occupancy query");
+  const BhkLaunch LL{int32_t(std::max<int64_t>(1, std::min<int64_t>(int64_t(sms) * per_sm, (q.n_pix + block - 1) / block))),
+                     block, 1, 0};
+  if (q.precision == BH_PRECISION_MIXED) {
+    if (bhk_trace_list_mixed(&q, o, list, count, counter, LL, stream) != 0)
+      return cuda_fail(cudaGetLastError(), "k_trace_list_mixed launch");
+    return 0;
+  }
+  if (bhk_trace_list_fp64(&q, o, list, count, counter, LL, stream) != 0) return fail("%s", bhk_last_error());
+  return 0;
+}
+
 int bhh_launch_image(const BhkImageParams *p, const BhkImageOut *o, unsigned long long *counter, BhkLaunch L,
-                     void *stream) {
+                     void *stream, int *list) {
+  if (p->integrator == BH_INTEGRATOR_ANALYTIC) return launch_analytic(p, o, counter, L, stream, list);
   if (p->precision == BH_PRECISION_MIXED) {
     if (bhk_trace_image_mixed(p, o, counter, L, stream) != 0)
       return cuda_fail(cudaGetLastError(), "k_trace_image_mixed launch");
@@ -237,7 +286,7 @@ int bh_kerr_trace_image(const BH_KerrScene *scene, const BH_KerrImageOut *out, v
   if (device_scratch(&ds) != 0) return -1;
   const BhkImageOut o{out->cls,   out->steps,     out->n_cross,   out->r_hit,     out->phi_hit,
                       out->g,     out->flux,      out->intensity, out->theta_inf, out->phi_inf, nullptr};
-  return bhh_launch_image(&p, &o, ds->counter, L, stream);
+  return bhh_launch_image(&p, &o, ds->counter, L, stream, nullptr);
 }
 
 // ---- host-buffer entry point ---------------------------------------------------

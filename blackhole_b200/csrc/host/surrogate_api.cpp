@@ -422,6 +422,7 @@ int bh_surrogate_trace_image(BH_Surrogate *s, const BH_KerrScene *scene, const B
   const int n_chunks = pol.chunks > 0 ? pol.chunks : kDefaultChunks;
   BH_KerrScene sc = *scene;
   sc.precision = BH_PRECISION_MIXED;  // the fallback integrator
+  if (sc.integrator == BH_INTEGRATOR_ANALYTIC) sc.integrator = BH_INTEGRATOR_DP45;
   BhkImageParams p;
   BhkLaunch L;
   if (bhh_prepare_image_launch(&sc, &p, &L) != 0) return -1;

@@ -148,7 +148,18 @@ enum BH_PixelClass {
 
 enum BH_Integrator {
     BH_INTEGRATOR_RK4 = 0,  /**< fixed affine step h = step_coeff * min(r, step_rcap), dsigma = h / Sigma */
-    BH_INTEGRATOR_DP45 = 1  /**< Dormand-Prince 5(4), rtol/atol on (r, cos theta, phi, p_r, p_u) */
+    BH_INTEGRATOR_DP45 = 1, /**< Dormand-Prince 5(4), rtol/atol on (r, cos theta, phi, p_r, p_u) */
+    /** No stepping: each ray in closed form (Jacobi elliptic functions of Mino time for r, the polar
+     *  angle and the azimuth; elliptic integrals in Carlson's form), FP64 whatever the precision,
+     *  the same cost per crossing in the photon-ring band as elsewhere. Single-frame calls only
+     *  (bh_kerr_trace_image*, bh_kerr_trace_image_sky). Rays it does not cover (a turning point
+     *  between r+ and the horizon cut, q_R < 0 rays that reach the equator or escape, four complex
+     *  roots with equator crossings) are traced by DP45 at the scene's precision with its rtol/atol.
+     *  steps = 0 on analytic pixels; escaped rays report theta_inf, phi_inf and the sky radiance
+     *  at exactly escape_factor * r_obs (the steppers report them after their last step's
+     *  overshoot past it). The analytic counterpart of src/physics/analytic_kerr_geodesic.h
+     *  (rAnalytic for bound orbits) and src/cuda/device_analytic_kerr.cuh, for image rays. */
+    BH_INTEGRATOR_ANALYTIC = 2
 };
 
 enum BH_Precision {
