@@ -4,7 +4,8 @@ Default workload ``c4_2048``: the a = 0.9 thin-disk scene (observer at
 r = 1000 M, 60 deg, alpha, beta in [-12, 12] M, opaque disk r_isco..30 M)
 at 2048 x 2048 pixels rendered by mixed precision plus the learned
 surrogate (bh_surrogate_trace_image: network inference on every pixel,
-exact Mino-time refinement, the mixed DP45 integrator on rejected pixels),
+exact Mino-time refinement, the closed-form tracer on rejected pixels and
+the mixed DP45 integrator on the few it does not cover),
 beside the plain FP64 integrators on the same scene: FP64 DP45 (rtol 1e-8)
 at 2048^2 and FP64 RK4 with h = 0.02 min(r, 20) (the plain method of the
 256^2 scene) timed on its 256^2 frame. One step = one render of the frame.
@@ -451,6 +452,26 @@ def run_surrogate(args, rank: int, world: int, dist):
         "accuracy_vs_fp64": accuracy([o64], [outs]),
         "render_ms": {"mean": statistics.mean(render_ms), "min": min(render_ms), "max": max(render_ms)},
     }
+    # ---- the closed-form tracer (BH_INTEGRATOR_ANALYTIC) on the same frame, FP64 ----
+    san = _abi.KerrScene.from_buffer_copy(s64)
+    san.integrator = _abi.INTEGRATOR_ANALYTIC
+    oan = kerr.alloc_image_outputs(san, device=dev, fields=list(OUT_FIELDS_USED))
+    ms_an = _timed_launches(lambda: kerr.trace_image(san, oan, stream=stream), stream, 3, 1)
+    disk_fields = [f for f in OUT_FIELDS_USED if f not in ("phi_hit", "phi_inf")]
+    oan_d = kerr.alloc_image_outputs(san, device=dev, fields=disk_fields)
+    ms_an_d = _timed_launches(lambda: kerr.trace_image(san, oan_d, stream=stream), stream, 3, 1)
+    extra["analytic"] = {
+        "value": n / (statistics.mean(ms_an) * 1e-3), "unit": UNIT, "ms_per_step": statistics.mean(ms_an),
+        "method": "every ray in closed form in Mino time (Jacobi sn/cn, Carlson R_J, Bulirsch cel), FP64, "
+                  "all outputs incl. azimuths; DP45 on the rays it does not cover",
+        "speedup_vs_fp64_plain": statistics.mean(ms64) / statistics.mean(ms_an),
+        "stepped_pixels": int((oan["steps"] > 0).sum().item()),
+        "accuracy_vs_fp64": accuracy([o64], [oan]),
+        "disk_outputs_only": {"value": n / (statistics.mean(ms_an_d) * 1e-3), "unit": UNIT,
+                              "ms_per_step": statistics.mean(ms_an_d), "fields": disk_fields,
+                              "speedup_vs_fp64_plain": statistics.mean(ms64) / statistics.mean(ms_an_d)},
+    }
+
     # ---- network inference alone: the tensor-core kernel's roofline ----
     inp = S.grid_inputs(smx, device=dev, stream=stream)
     head = torch.empty(n, 16, dtype=torch.float32, device=dev)
@@ -490,7 +511,8 @@ def run_surrogate(args, rank: int, world: int, dist):
                "d2h_bytes_per_step": sum(t.numel() * t.element_size() for t in pinned.values()),
                "api": "bh_surrogate_trace_image_host", "fields": list(fields)}
     chunks = 2  # the renderer's default chunk count (BH_SurrogatePolicy.chunks = 0)
-    launches = (1 + 2 * chunks + 1) * args.steps  # inputs, chunks x (inference, refinement), fallback tracer
+    # inputs, chunks x (inference, refinement), the closed-form and DP45 fallback tracers
+    launches = (1 + 2 * chunks + 2) * args.steps
     return dict(value=value, ms_per_step=elapsed_ms / args.steps, e2e=e2e, roofline=roofline, clocks=clocks,
                 total_steps=int(outs["steps"].sum().item()), rays_per_step=n, launches=launches, extra=extra)
 

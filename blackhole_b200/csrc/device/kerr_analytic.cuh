@@ -43,9 +43,11 @@
 #include "mino_solve.cuh"
 
 // The heavy routines are calls on the device (each keeps its working set in
-// its own frame instead of the caller's registers).
+// its own frame instead of the caller's registers), with internal linkage:
+// nvcc's host stubs of external device functions would otherwise take the
+// names of the host build of this header in the same library.
 #ifdef __CUDACC__
-#define BHA_CALL __device__ __noinline__
+#define BHA_CALL static __device__ __noinline__
 #else
 #define BHA_CALL inline
 #endif
@@ -335,12 +337,10 @@ BHM_HD double newton_root(double p2, double p1, double p0, double r) {
   return r;
 }
 
-// Real roots of x^4 + p2 x^2 + p1 x + p0 by Ferrari's factorization into
-// (x^2 + al x + be)(x^2 - al x + ga), al^2 = z the largest root of the
-// resolvent cubic z^3 + 2 p2 z^2 + (p2^2 - 4 p0) z - p1^2. Returns the number
-// of real roots (ascending in re[]); with two, (c, d) of the complex pair and
-// its squared modulus c^2 + d^2 (the constant term of its quadratic factor).
-BHA_CALL int ferrari(double p2, double p1, double p0, double re[4], double &c, double &d, double &mod2) {
+// Ferrari's factorization x^4 + p2 x^2 + p1 x + p0 = (x^2 + al x + be)(x^2 - al x + ga),
+// al^2 = z the largest root of the resolvent cubic z^3 + 2 p2 z^2 + (p2^2 - 4 p0) z - p1^2
+// (found in closed form, then polished by Newton); false if z <= 0.
+BHA_CALL bool ferrari_factor(double p2, double p1, double p0, double &al, double &be, double &ga) {
   // depressed resolvent: z = t - 2 p2 / 3, t^3 + P t + Q = 0
   const double P = -(p2 * p2) * (1.0 / 3.0) - 4.0 * p0;
   const double Q = -(2.0 / 27.0) * p2 * p2 * p2 + (8.0 / 3.0) * p2 * p0 - p1 * p1;
@@ -355,14 +355,26 @@ BHA_CALL int ferrari(double p2, double p1, double p0, double re[4], double &c, d
     t = cbrt(-0.5 * Q + sd) + cbrt(-0.5 * Q - sd);
   }
   double z = t - (2.0 / 3.0) * p2;
-  for (int it = 0; it < 3; ++it) {  // polish on the resolvent itself
+  for (int it = 0; it < 3; ++it) {
     const double f = ((z + 2.0 * p2) * z + (p2 * p2 - 4.0 * p0)) * z - p1 * p1;
     const double df = (3.0 * z + 4.0 * p2) * z + (p2 * p2 - 4.0 * p0);
     if (df != 0.0) z -= f / df;
   }
-  if (!(z > 0.0)) return -1;
-  const double al = sqrt(z);
-  const double be = 0.5 * (p2 + z - p1 / al), ga = 0.5 * (p2 + z + p1 / al);
+  if (!(z > 0.0)) return false;
+  al = sqrt(z);
+  be = 0.5 * (p2 + z - p1 / al);
+  ga = 0.5 * (p2 + z + p1 / al);
+  return true;
+}
+
+// Real roots of x^4 + p2 x^2 + p1 x + p0 from that factorization, polished
+// by Newton. Returns the number of real roots (ascending in re[]); with two,
+// (c, d) of the complex pair and its squared modulus c^2 + d^2 (the constant
+// term of its quadratic factor).
+BHA_CALL int ferrari(double p2, double p1, double p0, double re[4], double &c, double &d, double &mod2) {
+  double al, be, ga;
+  if (!ferrari_factor(p2, p1, p0, al, be, ga)) return -1;
+  const double z = al * al;
   const double d1 = z - 4.0 * be, d2 = z - 4.0 * ga;
   int n = 0;
   if (d1 >= 0.0) {

@@ -139,7 +139,32 @@ __global__ void __launch_bounds__(128, 4) k_trace_image_analytic(const __grid_co
     if (!trace_pixel(p, o, pix)) list[atomicAdd(count, 1u)] = (int)pix;
 }
 
+// The same over a list of pixels (the surrogate renderer's rejected pixels);
+// those it does not cover go on to list2.
+__global__ void __launch_bounds__(128, 4) k_trace_list_analytic(const __grid_constant__ BhkImageParams p,
+                                                                const __grid_constant__ BhkImageOut o,
+                                                                const int *__restrict__ list,
+                                                                const unsigned int *__restrict__ count,
+                                                                int *__restrict__ list2,
+                                                                unsigned int *__restrict__ count2) {
+  const unsigned int total = *count;
+  const unsigned int stride = gridDim.x * blockDim.x;
+  for (unsigned int w = blockIdx.x * blockDim.x + threadIdx.x; w < total; w += stride) {
+    const int pix = list[w];
+    if (!trace_pixel(p, o, pix)) list2[atomicAdd(count2, 1u)] = pix;
+  }
+}
+
 }  // namespace
+
+extern "C" int bhk_trace_list_analytic(const BhkImageParams *p, const BhkImageOut *o, const int *list,
+                                       const unsigned int *count, int *list2, unsigned int *count2, BhkLaunch L,
+                                       void *stream) {
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (cudaMemsetAsync(count2, 0, sizeof(unsigned int), s) != cudaSuccess) return -1;
+  k_trace_list_analytic<<<L.grid, L.block, 0, s>>>(*p, *o, list, count, list2, count2);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
 
 extern "C" int bhk_trace_image_analytic(const BhkImageParams *p, const BhkImageOut *o, int *list,
                                         unsigned int *count, BhkLaunch L, void *stream) {

@@ -46,7 +46,8 @@ struct BH_Surrogate {
   int64_t ren_pixels = 0;
   float *r_inputs = nullptr, *r_head = nullptr;
   int *r_list = nullptr;
-  unsigned int *r_counts = nullptr;  // [0] list length, [1..5] stats
+  int *r_list2 = nullptr;            // rejected pixels the closed form leaves to DP45
+  unsigned int *r_counts = nullptr;  // [0] list length, [1..5] stats, [6] list2 length
   unsigned long long *r_counter = nullptr;
   int64_t last_pixels = 0;
   // renderer concurrency: refine of chunk k on `side` while chunk k+1 is inferred
@@ -430,18 +431,20 @@ int bh_surrogate_trace_image(BH_Surrogate *s, const BH_KerrScene *scene, const B
   s->last_pixels = n;
   if (n == 0) return 0;
   if (n > s->ren_pixels) {
-    for (void *q : {static_cast<void *>(s->r_inputs), static_cast<void *>(s->r_head), static_cast<void *>(s->r_list)}) {
+    for (void *q : {static_cast<void *>(s->r_inputs), static_cast<void *>(s->r_head), static_cast<void *>(s->r_list),
+                    static_cast<void *>(s->r_list2)}) {
       if (!q) continue;
       auto it = std::find(s->allocs.begin(), s->allocs.end(), q);
       if (it != s->allocs.end()) s->allocs.erase(it);
       cudaFree(q);
     }
     s->r_inputs = s->r_head = nullptr;
-    s->r_list = nullptr;
+    s->r_list = s->r_list2 = nullptr;
     s->ren_pixels = 0;
     if (int rc = alloc(s, &s->r_inputs, static_cast<size_t>(n) * 4, "cudaMalloc(render inputs)")) return rc;
     if (int rc = alloc(s, &s->r_head, static_cast<size_t>(n) * BHS_HEAD, "cudaMalloc(render head)")) return rc;
     if (int rc = alloc(s, &s->r_list, static_cast<size_t>(n), "cudaMalloc(fallback list)")) return rc;
+    if (int rc = alloc(s, &s->r_list2, static_cast<size_t>(n), "cudaMalloc(second fallback list)")) return rc;
     s->ren_pixels = n;
   }
   if (!s->r_counts) {
@@ -478,7 +481,19 @@ int bh_surrogate_trace_image(BH_Surrogate *s, const BH_KerrScene *scene, const B
                              p0, p1, s->r_list, s->r_counts, s->r_counts + 1, s->side))
       return fail_msg("surrogate render: refine launch failed");
   }
-  if (bhk_trace_list_mixed(&p, &o, s->r_list, s->r_counts, s->r_counter, L, s->side))
+  // Rejected pixels: the closed-form tracer (O(1) per crossing, so the
+  // near-critical band costs no more than the rest), then mixed DP45 on what
+  // it does not cover.
+  int per_sm = 0;
+  if (bhk_trace_image_analytic_occupancy(128, &per_sm) != 0 || per_sm < 1)
+    return fail_msg("surrogate render: occupancy query failed");
+  int dev = 0, sms = 0;
+  if (int rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice")) return rc;
+  if (int rc = cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count")) return rc;
+  const BhkLaunch La{sms * per_sm, 128, 1, 0};
+  if (bhk_trace_list_analytic(&p, &o, s->r_list, s->r_counts, s->r_list2, s->r_counts + 6, La, s->side))
+    return fail_msg("surrogate render: closed-form fallback launch failed");
+  if (bhk_trace_list_mixed(&p, &o, s->r_list2, s->r_counts + 6, s->r_counter, L, s->side))
     return fail_msg("surrogate render: fallback tracer launch failed");
   if (int rc = cuda_check(cudaEventRecord(s->ev[kRenderChunks + 1], s->side), "cudaEventRecord")) return rc;
   return cuda_check(cudaStreamWaitEvent(st, s->ev[kRenderChunks + 1], 0), "cudaStreamWaitEvent");

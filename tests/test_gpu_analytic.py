@@ -6,7 +6,9 @@ hole several times, the integrator fallback for rays the closed form leaves
 out, the no-allocation entry point and the sky."""
 from __future__ import annotations
 
+import ctypes as C
 import math
+from pathlib import Path
 
 import numpy as np
 import pytest
@@ -176,3 +178,70 @@ def test_analytic_sky_radiance(cuda, oracle):
     assert esc.mean() > 0.3
     same = np.isclose(got["intensity"][esc], dp["intensity"][esc], rtol=1e-9)
     assert same.mean() >= 0.98
+
+
+REF_DEV = Path(__file__).resolve().parents[1] / "oracle" / "_ref" / "libbh_ref_analytic_dev.so"
+
+
+@pytest.mark.skipif(not REF_DEV.exists(), reason="reference device build absent (oracle/_ref)")
+def test_helpers_match_reference_device_functions(cuda):
+    """include/bh_analytic.h (FP64, host) against the reference's own FP32
+    device helpers (src/cuda/device_analytic_kerr.cuh, compiled unmodified):
+    d_ellpj, d_ellint_K, d_quartic_real_roots, d_kerr_r_analytic,
+    d_kerr_radial_half_period and the photon orbits, at FP32 tolerances."""
+    from blackhole_b200 import analytic as an
+
+    L = C.CDLL(str(REF_DEV))
+    vp, i = C.c_void_p, C.c_int
+    for name, args in (("ref_dev_ellpj", [i, vp, vp, vp]), ("ref_dev_ellint_k", [i, vp, vp]),
+                       ("ref_dev_roots", [i, vp, vp]), ("ref_dev_r_analytic", [i, vp, vp, C.c_float, vp]),
+                       ("ref_dev_half_period", [i, vp, vp]), ("ref_dev_critical", [i, vp, vp, vp]),
+                       ("ref_dev_photon", [i, vp, vp])):
+        getattr(L, name).argtypes = args
+    f32 = lambda x: np.ascontiguousarray(x, np.float32)  # noqa: E731
+    rng = np.random.default_rng(11)
+    n = 256
+    u, m = f32(rng.uniform(-8, 8, n)), f32(rng.uniform(1e-4, 0.98, n))
+    out = np.zeros(3 * n, np.float32)
+    assert L.ref_dev_ellpj(n, u.ctypes.data, m.ctypes.data, out.ctypes.data) == 0
+    ours = np.array([an.ellpj(float(a), float(b)) for a, b in zip(u, m)]).ravel()
+    np.testing.assert_allclose(ours, out, atol=2e-4)
+    k = f32(rng.uniform(0, 0.99, n))
+    out = np.zeros(n, np.float32)
+    assert L.ref_dev_ellint_k(n, k.ctypes.data, out.ctypes.data) == 0
+    np.testing.assert_allclose([an.ellint_k(float(x)) for x in k], out, rtol=1e-5)
+    # quartics with four well-separated real roots summing to zero, descending
+    r3 = rng.uniform(-3, 6, (n, 3))
+    roots = np.sort(np.concatenate([r3, -r3.sum(1, keepdims=True)], 1), axis=1)[:, ::-1]
+    roots = roots[np.min(-np.diff(roots, axis=1), axis=1) > 0.3][:64]
+    nq = len(roots)
+    c = np.stack([np.poly(r)[2:] for r in roots])
+    out = np.zeros(5 * nq, np.float32)
+    assert L.ref_dev_roots(nq, f32(c).ctypes.data, out.ctypes.data) == 0
+    out = out.reshape(nq, 5)
+    for q in range(nq):
+        got, nr, _ = an.radial_roots(*c[q])
+        assert nr == int(out[q, 0]) == 4
+        np.testing.assert_allclose(got.real, out[q, 1:], atol=2e-3 * max(1.0, np.abs(roots[q]).max()))
+    lam = f32(rng.uniform(0, 3, nq))
+    ro = f32(roots)
+    out = np.zeros(nq, np.float32)
+    assert L.ref_dev_r_analytic(nq, lam.ctypes.data, ro.ctypes.data, 0.0, out.ctypes.data) == 0
+    np.testing.assert_allclose([an.r_bound(float(x), r) for x, r in zip(lam, roots)], out, rtol=2e-4, atol=2e-4)
+    assert L.ref_dev_half_period(nq, ro.ctypes.data, out.ctypes.data) == 0
+    np.testing.assert_allclose([an.radial_half_period(r) for r in roots], out, rtol=2e-5)
+    # d_critical_impact_params (device_analytic_kerr.cuh:418-449) has 2 r Delta / (a Delta')
+    # in xi and drops a factor r from eta; ours is Bardeen's xi, eta as in the reference's
+    # CPU criticalImpactParams (pinned in tests/test_analytic_api.py): R = 0 there, not at the device's.
+    rph, a = f32(rng.uniform(1.2, 4.0, n)), f32(rng.uniform(0.05, 0.99, n))
+    out = np.zeros(2 * n, np.float32)
+    assert L.ref_dev_critical(n, rph.ctypes.data, a.ctypes.data, out.ctypes.data) == 0
+    r_dev = []
+    for r, s, dev in zip(rph[:16], a[:16], out.reshape(n, 2)[:16]):
+        xi, eta = an.critical_impact_params(float(r), float(s))
+        assert abs(an.radial_potential(float(r), float(s), xi, eta)) < 1e-9 * float(r) ** 4
+        r_dev.append(abs(an.radial_potential(float(r), float(s), float(dev[0]), float(dev[1]))))
+    assert max(r_dev) > 1e-2
+    assert L.ref_dev_photon(n, a.ctypes.data, out.ctypes.data) == 0
+    ours = np.array([(an.prograde_photon_orbit(float(s)), an.retrograde_photon_orbit(float(s))) for s in a]).ravel()
+    np.testing.assert_allclose(ours, out, rtol=1e-5)

@@ -44,7 +44,13 @@ def test_untrained_network_falls_back_everywhere(cuda):
     got = host(net.trace_image(s))
     st = net.last_stats()
     assert st["pixels"] == 96 * 96 and st["accepted"] == 0 and st["low_confidence"] == 96 * 96
-    ref = host(kerr.trace_image(s))
+    # every rejected pixel goes to the closed-form tracer (DP45 on those it
+    # does not cover): the render is that integrator's image, bit for bit
+    from blackhole_b200 import _abi
+
+    sa = _abi.KerrScene.from_buffer_copy(s)
+    sa.integrator = _abi.INTEGRATOR_ANALYTIC
+    ref = host(kerr.trace_image(sa))
     torch.cuda.synchronize()
     for k in ref:
         np.testing.assert_array_equal(got[k], ref[k], err_msg=k)
@@ -97,10 +103,12 @@ def test_trained_network_meets_targets(cuda, oracle):
 @pytest.mark.skipif(not WEIGHTS.exists(), reason="trained weights not shipped")
 def test_trained_network_gain_over_the_integrator(cuda):
     """Ablation: the same renderer with the trained network against the
-    method without it (an untrained network sends every pixel to the
-    integrator; the plain mixed tracer traces every pixel). The network
-    removes >= 95 % of the integration steps and renders >= 1.5x faster, at
-    the same accuracy (checked above)."""
+    methods without it: an untrained network sends every pixel to the
+    renderer's fallback (the closed-form tracer), and the plain mixed tracer
+    steps every pixel. With the network the render takes none of the mixed
+    tracer's integration steps beyond 5 % and runs >= 1.5x faster than it,
+    and faster than the fallback on every pixel, at the same accuracy
+    (checked above)."""
     from blackhole_b200 import kerr
     from blackhole_b200 import surrogate as S
 
@@ -113,9 +121,8 @@ def test_trained_network_gain_over_the_integrator(cuda):
     o_m = kerr.trace_image(s)
     torch.cuda.synchronize()
     steps_t = int(o_t["steps"].sum().item())
-    steps_b = int(o_b["steps"].sum().item())
-    assert steps_b == int(o_m["steps"].sum().item())  # no network: the integrator on every pixel
-    assert steps_t <= 0.05 * steps_b, (steps_t, steps_b)
+    steps_m = int(o_m["steps"].sum().item())
+    assert steps_t <= 0.05 * steps_m, (steps_t, steps_m)
 
     def ms(fn, reps=5):
         fn()
@@ -129,5 +136,7 @@ def test_trained_network_gain_over_the_integrator(cuda):
         return a.elapsed_time(b) / reps
 
     t_net = ms(lambda: trained.trace_image(s, o_t))
+    t_blank = ms(lambda: blank.trace_image(s, o_b))
     t_plain = ms(lambda: kerr.trace_image(s, o_m))
     assert t_plain >= 1.5 * t_net, (t_plain, t_net)
+    assert t_blank > t_net, (t_blank, t_net)
