@@ -54,8 +54,13 @@
 
 namespace bhan {
 
-using bhmino::carlson_rf;
 using bhmino::inv_sqrt;
+
+// Carlson's R_F as one shared device call: inlined at each of its call sites
+// it made the tracer's code large enough that instruction fetch, not
+// arithmetic, bounded the kernel (ncu: "no instruction" was 17 of 24 stall
+// cycles per issue); as a call the image takes 17 % less time.
+BHA_CALL double carlson_rf(double x, double y, double z) { return bhmino::carlson_rf<double>(x, y, z); }
 #ifndef __CUDACC__
 using std::isnan;
 #endif
