@@ -73,6 +73,11 @@ WORKLOADS = {
     "c2_512": dict(width=512, height=512, integrator=1, max_crossings=1, frames=[(0.94, 17.0)], rt=True),
     # smaller copies of the two scenes above, for profiler captures
     "c4_1024": dict(width=1024, height=1024, integrator=1, max_crossings=1, frames=[(0.9, 60.0)], surrogate=True),
+    # the closed-form tracer (BH_INTEGRATOR_ANALYTIC, FP64) on the C4 frame, and a
+    # 512^2 three-crossing frame for profiler captures
+    "c4_analytic": dict(width=2048, height=2048, integrator=2, max_crossings=1, frames=[(0.9, 60.0)], analytic=True),
+    "disk1_512_analytic": dict(width=512, height=512, integrator=2, max_crossings=3, frames=[(0.9, 45.0)],
+                               analytic=True),
     "c2_128": dict(width=128, height=128, integrator=1, max_crossings=1, frames=[(0.94, 17.0)], rt=True),
 }
 SURROGATE_WEIGHTS = ROOT / "blackhole_b200" / "data" / "surrogate_c4.npz"
@@ -495,7 +500,8 @@ def run_surrogate(args, rank: int, world: int, dist):
     e2e = None
     if rank == 0:
         fields = ("cls", "n_cross", "r_hit", "g", "flux", "intensity")
-        pinned = {f: torch.empty(n, dtype=torch.int32 if f in _abi.INT_FIELDS else torch.float64).pin_memory()
+        pinned = {f: torch.empty(n * (smx.max_crossings if f in _abi.PLANE_FIELDS else 1),
+                                 dtype=torch.int32 if f in _abi.INT_FIELDS else torch.float64).pin_memory()
                   for f in fields}
         o = _abi.KerrImageOut()
         for f, t in pinned.items():
@@ -515,6 +521,104 @@ def run_surrogate(args, rank: int, world: int, dist):
     launches = (1 + 2 * chunks + 2) * args.steps
     return dict(value=value, ms_per_step=elapsed_ms / args.steps, e2e=e2e, roofline=roofline, clocks=clocks,
                 total_steps=int(outs["steps"].sum().item()), rays_per_step=n, launches=launches, extra=extra)
+
+
+def run_analytic(args, rank: int, world: int, dist):
+    """The closed-form tracer: one step = one bh_kerr_trace_image of the frame
+    with integrator BH_INTEGRATOR_ANALYTIC (FP64; DP45 on the rays it does
+    not cover), the bench line's output fields; the FP64 DP45 tracer on the
+    same frame is timed beside it and is the accuracy reference."""
+    import torch
+
+    from blackhole_b200 import _abi, kerr
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    lib = _abi.load_library()
+    stream = torch.cuda.Stream(device=dev)
+    s = scenes_for(args.workload, 0)[0]
+    n = s.width * s.height
+    outs = kerr.alloc_image_outputs(s, device=dev, fields=list(OUT_FIELDS_USED))
+
+    def render():
+        kerr.trace_image(s, outs, stream=stream)
+
+    sampler = ClockSampler(dev.index if "CUDA_VISIBLE_DEVICES" not in os.environ else 0)
+    sampler.start()
+    sampler.wait_first_sample()
+    for _ in range(args.warmup):
+        render()
+    torch.cuda.synchronize(dev)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    sampler.lines.clear()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(args.steps):
+        render()
+    t1.record(stream)
+    torch.cuda.synchronize(dev)
+    clocks = sampler.stop()
+    if dist is not None:
+        dist.barrier()
+    elapsed_ms = t0.elapsed_time(t1)
+    if dist is not None:
+        t = torch.tensor([elapsed_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    ms = elapsed_ms / args.steps
+    value = n * args.steps * world / (elapsed_ms * 1e-3)
+
+    s64 = _abi.KerrScene.from_buffer_copy(s)
+    s64.integrator = _abi.INTEGRATOR_DP45
+    o64 = kerr.alloc_image_outputs(s64, device=dev, fields=list(OUT_FIELDS_USED))
+    ms64 = statistics.mean(_timed_launches(lambda: kerr.trace_image(s64, o64, stream=stream), stream, 2, 1))
+    disk_fields = [f for f in OUT_FIELDS_USED if f not in ("phi_hit", "phi_inf")]
+    od = kerr.alloc_image_outputs(s, device=dev, fields=disk_fields)
+    ms_d = statistics.mean(_timed_launches(lambda: kerr.trace_image(s, od, stream=stream), stream, 5, 2))
+    extra = {
+        "fp64_plain": {"value": n / (ms64 * 1e-3), "unit": UNIT, "ms_per_step": ms64,
+                       "method": f"FP64 DP45 rtol 1e-8 on the same {s.width}x{s.height} frame"},
+        "speedup_vs_fp64_plain": ms64 / ms,
+        "accuracy_vs_fp64": accuracy([o64], [outs]),
+        "stepped_pixels": int((outs["steps"] > 0).sum().item()),
+        "disk_outputs_only": {"value": n / (ms_d * 1e-3), "unit": UNIT, "ms_per_step": ms_d, "fields": disk_fields,
+                              "speedup_vs_fp64_plain": ms64 / ms_d},
+    }
+    # Outputs are the only HBM traffic (no inputs): the roofline below is the
+    # HBM one, far from binding; the kernel is bound by instruction fetch
+    # (profiles/k_trace_image_analytic_disk1_512.md).
+    out_bytes = sum(t.numel() * t.element_size() for t in outs.values())
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = peaks.get("hbm_gbs")
+    achieved = out_bytes / (ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak or 6650.0, "unit": "GB/s",
+                "frac": achieved / (peak or 6650.0), "traffic": None, "kernel": "k_trace_image_analytic",
+                "bytes_per_launch": out_bytes,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peak else "fallback 6.65 TB/s",
+                "note": "algorithmic bytes = the outputs written; the kernel is bound by instruction fetch, not HBM"}
+    e2e = None
+    if rank == 0:
+        fields = ("cls", "n_cross", "r_hit", "g", "flux", "intensity")
+        pinned = {f: torch.empty(n * (s.max_crossings if f in _abi.PLANE_FIELDS else 1),
+                                 dtype=torch.int32 if f in _abi.INT_FIELDS else torch.float64).pin_memory()
+                  for f in fields}
+        o = _abi.KerrImageOut()
+        for f, t in pinned.items():
+            setattr(o, f, t.data_ptr())
+        _abi.check(lib.bh_kerr_trace_image_host(C.byref(s), C.byref(o)))
+        k = max(1, min(args.steps, 3))
+        w0 = time.perf_counter()
+        for _ in range(k):
+            _abi.check(lib.bh_kerr_trace_image_host(C.byref(s), C.byref(o)))
+        w1 = time.perf_counter()
+        e2e = {"value": n * k / (w1 - w0), "unit": UNIT, "h2d_bytes_per_step": C.sizeof(_abi.KerrScene),
+               "d2h_bytes_per_step": sum(t.numel() * t.element_size() for t in pinned.values()),
+               "api": "bh_kerr_trace_image_host", "fields": list(fields)}
+    # per step: the closed-form kernel and the DP45 list tracer on what it leaves
+    return dict(value=value, ms_per_step=ms, e2e=e2e, roofline=roofline, clocks=clocks,
+                total_steps=int(outs["steps"].sum().item()), rays_per_step=n, launches=2 * args.steps, extra=extra)
 
 
 def run_rt(args, rank: int, world: int, dist):
@@ -642,6 +746,9 @@ def cpu_reference(workload: str, budget_s: float, seed: int = 7):
     lib = RefLib()
     threads = default_threads()
     scenes = scenes_for(workload, 0)
+    for s in scenes:  # the reference's CPU path steps every ray (DP45 for the closed-form workloads)
+        if s.integrator == 2:
+            s.integrator = 1
     n_frame = scenes[0].width * scenes[0].height
     rng = np.random.default_rng(seed)
     done = 0
@@ -709,7 +816,7 @@ def main():
                   "max_crossings": wl["max_crossings"], "image_plane_M": [-12, 12]}
     else:
         config = {"workload": args.workload, "frames": len(wl["frames"]), "width": wl["width"], "height": wl["height"],
-                  "integrator": "dp45" if wl["integrator"] == 1 else "rk4", "rtol": 1e-8, "atol": 1e-10,
+                  "integrator": {0: "rk4", 1: "dp45", 2: "analytic"}[wl["integrator"]], "rtol": 1e-8, "atol": 1e-10,
                   "max_crossings": wl["max_crossings"], "r_obs": 1000.0, "image_plane_M": [-12, 12]}
     config.update({"parallelism": f"replicas{world}", "launch": "one persistent launch per step (CUDA graph)",
                    "l2": "no inputs; outputs written once per step, larger than L2"})
@@ -728,8 +835,8 @@ def main():
                        "network": "192 features -> 4 x 256 SiLU -> 16, BF16 weights, FP32 accumulation",
                        "weights": "blackhole_b200/data/surrogate_c4.npz (trained on 2^26 integrator rays)",
                        "policy": {"min_confidence": 0.99, "critical_band_M": 0.05, "verify": "radial kind"},
-                       "launch": "6 launches per render on two streams: inputs, 2 x (inference, refinement), "
-                                 "integrator on the rejected pixels",
+                       "launch": "7 launches per render on two streams: inputs, 2 x (inference, refinement), "
+                                 "the closed-form tracer and DP45 on the rejected pixels",
                        "l2": f"outputs ({wl['width']}^2 pixels x 9 fields) written once per step, larger than L2"})
 
     if args.impl == "reference":
@@ -750,8 +857,14 @@ def main():
 
         dist_mod.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
         dist = dist_mod
+    if wl.get("analytic"):
+        config.update({"spin": wl["frames"][0][0], "theta_obs_deg": wl["frames"][0][1], "precision": "fp64",
+                       "method": "closed form in Mino time (BH_INTEGRATOR_ANALYTIC)",
+                       "launch": "2 launches per step: the closed-form kernel, DP45 on the rays it does not cover"})
     if wl.get("surrogate"):
         res = run_surrogate(args, rank, world, dist)
+    elif wl.get("analytic"):
+        res = run_analytic(args, rank, world, dist)
     elif wl.get("rt"):
         res = run_rt(args, rank, world, dist)
     else:
@@ -764,8 +877,9 @@ def main():
         line = {"metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None,
-                "dtype": "bf16+f32+f64" if wl.get("surrogate") else ("f64" if args.precision == "fp64" else "f32+f64"),
-                "data": "synthetic", "config": config, "precision": args.precision,
+                "dtype": "bf16+f32+f64" if wl.get("surrogate") else
+                ("f64" if args.precision == "fp64" or wl.get("analytic") else "f32+f64"),
+                "data": "synthetic", "config": config, "precision": "fp64" if wl.get("analytic") else args.precision,
                 "steps_per_s": res["total_steps"] * args.steps * world / (res["ms_per_step"] * args.steps * 1e-3),
                 **res["extra"],
                 "e2e": res["e2e"], "roofline": res["roofline"], "cpu_baseline": cb, "clocks": res["clocks"],
