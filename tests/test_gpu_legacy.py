@@ -4,7 +4,9 @@ post-processing, the lensing map, the disk texture and the geodesic paths,
 each against the CPU oracle (kerr_oracle.hpp camera/paths,
 oracle/legacy_oracle.py shading and post-processing), and the post-processing
 also against the reference's own kernels (oracle/_ref/libbh_ref_post.so, built
-from src/blender_bridge/cuda_postprocess.cu)."""
+from src/blender_bridge/cuda_postprocess.cu), and the disk geometry of the
+render against the reference's own render kernels
+(oracle/_ref/libbh_ref_render.so, built from src/cuda)."""
 from __future__ import annotations
 
 import ctypes as C
@@ -243,6 +245,60 @@ def test_postprocess_matches_reference_build(cuda, leg, w, h, threshold, strengt
     assert own.mean() > 0.75
     np.testing.assert_allclose(rb[own], ra[own], rtol=2e-5, atol=1e-6)
     np.testing.assert_allclose(rb[:, 1], ra[:, 1], rtol=2e-5, atol=1e-6)  # green is always the pixel's own
+
+
+REF_RENDER = Path(__file__).resolve().parents[1] / "oracle" / "_ref" / "libbh_ref_render.so"
+
+
+def _grow(m, k):
+    out = m.copy()
+    for dy in range(-k, k + 1):
+        for dx in range(-k, k + 1):
+            out |= np.roll(np.roll(m, dy, 0), dx, 1)
+    return out
+
+
+@pytest.mark.skipif(not REF_RENDER.exists(), reason="reference render-kernel build absent (oracle/_ref)")
+@pytest.mark.parametrize("spin,r_rs,incl", [(0.0, 15.0, 1.3), (0.0, 10.0, 1.5), (0.9, 15.0, 1.3), (0.5, 12.0, 1.45)])
+def test_disk_geometry_against_reference_render_kernel(cuda, leg, spin, r_rs, incl):
+    """Which pixels see the disk, ours against the reference's own FP32 kernel
+    (geodesicTraceFp32, src/cuda/kernels_fp32.cu:35, through its
+    bh_launch_geodesic_kernel, compiled from its source) on the same
+    BH_LaunchParams: Kerr stepping on, background and photon glow off, so that
+    both paint exactly the disk pixels (device_physics.cuh:1522-1525 black
+    background, :1899-1924 glow scaled by photon_glow_strength; disk z = 0
+    between isco and 30 rs, :606-613 and :936-937).
+
+    a = 0: the images agree except within 3 pixels of the disk's edges (the
+    reference's FP32 steps cross the plane with a coarse linear interpolation
+    at the outer rim). a != 0: the reference paints no disk below the shadow
+    (the near side of the disk, seen through the first plane crossing), while
+    the far side above it agrees; nothing it paints is absent from ours."""
+    ref_lib = C.CDLL(str(REF_RENDER))
+    ref_lib.bh_launch_geodesic_kernel.argtypes = [C.c_void_p, C.POINTER(leg.LaunchParams), C.c_int, C.c_void_p]
+    ref_lib.bh_launch_geodesic_kernel.restype = C.c_int
+    p = leg.bridge_params(spin, r_rs, incl, 0.6, 160, 120)
+    p.kerr_enabled = 1
+    p.background_enabled = 0
+    p.photon_glow_strength = 0.0
+    p.max_steps = 20000
+    p.step_size = 0.04
+    fb = torch.zeros(p.height * p.width * 4, dtype=torch.float32, device="cuda")
+    assert ref_lib.bh_launch_geodesic_kernel(C.c_void_p(fb.data_ptr()), C.byref(p), 0, None) == 0
+    torch.cuda.synchronize()
+    theirs = fb.view(p.height, p.width, 4).cpu().numpy()
+    ours = _render(leg, p).reshape(p.height, p.width, 4)
+    assert np.all(np.isfinite(theirs)) and np.all(np.isfinite(ours))
+    d_ours, d_ref = ours[..., :3].sum(-1) > 0, theirs[..., :3].sum(-1) > 0
+    diff = d_ours != d_ref
+    half = p.height // 2
+    if spin == 0.0:
+        assert d_ours.mean() > 0.5 and np.mean(~diff) >= 0.95, np.mean(~diff)
+        assert not np.any(diff & ~(_grow(d_ours, 3) & _grow(~d_ours, 3)))
+    else:
+        assert np.mean(~diff[:half]) >= 0.995, np.mean(~diff[:half])
+        assert d_ours[half:].mean() > 0.3 and not d_ref[half:].any()
+        assert np.mean(d_ref & ~d_ours) < 1e-3
 
 
 def test_bridge_environment_overrides(cuda, leg, oracle, monkeypatch):
