@@ -373,6 +373,27 @@ def _timed_launches(fn, stream, steps: int, warmup: int):
     return [a.elapsed_time(b) for a, b in out]
 
 
+LEGACY_SCENE = ("2048x2048 Blender-bridge camera (bridge defaults, fov 1.0, 600 steps of 0.08), a = 0.9, "
+                "camera at 10 rs and 60 deg from the spin axis, disk and background on")
+
+
+def time_legacy_launch(launch, steps: int = 5, warmup: int = 2) -> dict:
+    """Frames of the reference's render launch ABI, bh_launch_geodesic_kernel,
+    on one bridge-camera scene (device framebuffer, CUDA events on the
+    launching stream, which is the legacy default stream for both
+    implementations here)."""
+    import torch
+
+    from blackhole_b200 import legacy
+
+    p = legacy.bridge_params(0.9, 10.0, math.radians(60.0), 1.0, 2048, 2048)
+    fb = torch.empty(p.width * p.height * 4, dtype=torch.float32, device="cuda")
+    ts = _timed_launches(lambda: launch(p, fb), torch.cuda.current_stream(), steps, warmup)
+    ms = statistics.median(ts)
+    return {"value": p.width * p.height / (ms * 1e-3), "unit": UNIT, "ms_per_frame": ms, "frames": steps,
+            "scene": LEGACY_SCENE, "api": "bh_launch_geodesic_kernel"}
+
+
 def run_surrogate(args, rank: int, world: int, dist):
     """The learned-surrogate workload: one step = one bh_surrogate_trace_image
     render of the 2048^2 a = 0.9 disk frame."""
@@ -765,6 +786,36 @@ def cpu_reference(workload: str, budget_s: float, seed: int = 7):
                       f"{el:.1f} s wall on {threads} threads (oracle/_ref: reference kerrPotentials)"}
 
 
+def reference_gpu_kernel() -> dict:
+    """The reference's own FP32 render kernel (geodesicTraceFp32, variant 0 of
+    its bh_launch_geodesic_kernel; oracle/_ref/libbh_ref_render.so, compiled
+    from its source for sm_100a) on the bridge-camera scene, for context: FP32
+    fixed-step stepping and art-directed shading, not this metric's method."""
+    lib_path = ROOT / "oracle" / "_ref" / "libbh_ref_render.so"
+    try:
+        import torch
+
+        if not torch.cuda.is_available():
+            return {"unavailable": "no CUDA device"}
+        if not lib_path.exists():
+            return {"unavailable": "oracle/_ref/libbh_ref_render.so not built (reference sources absent at build)"}
+        from blackhole_b200 import legacy
+
+        ref = C.CDLL(str(lib_path))
+        ref.bh_launch_geodesic_kernel.argtypes = [C.c_void_p, C.POINTER(legacy.LaunchParams), C.c_int, C.c_void_p]
+        ref.bh_launch_geodesic_kernel.restype = C.c_int
+
+        def launch(p, fb):
+            if ref.bh_launch_geodesic_kernel(C.c_void_p(fb.data_ptr()), C.byref(p), 0, None) != 0:
+                raise RuntimeError("reference bh_launch_geodesic_kernel failed")
+
+        out = time_legacy_launch(launch)
+        out["kernel"] = "geodesicTraceFp32 (reference build, FP32)"
+        return out
+    except Exception as e:  # context only: never fail the reference line over it
+        return {"unavailable": f"{type(e).__name__}: {e}"}
+
+
 def cpu_reference_rt(inp: dict, budget_s: float, seed: int = 7):
     """Time the CPU restatement of the transfer (oracle rt_oracle.hpp: FP64
     DP45 ray, the reference's synchrotron / Planck / rteStep physics) on a
@@ -848,6 +899,8 @@ def main():
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config, "impl": "reference",
                 "cpu_baseline": cb,
                 "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        if args.workload == "c4_2048":
+            line["gpu_kernel_context"] = reference_gpu_kernel()
         print(json.dumps(line))
         return
 
@@ -870,6 +923,12 @@ def main():
     else:
         res = run_ours(args, rank, world, dist)
     if rank == 0:
+        if world == 1 and args.workload == "c4_2048":
+            from blackhole_b200 import legacy
+
+            lr = time_legacy_launch(lambda p, fb: legacy.launch(p, fb, -1))
+            lr["kernel"] = "k_trace_camera_mixed + shading (mixed DP45)"
+            res["extra"]["legacy_render"] = lr
         cb = None
         if world == 1 and args.cpu_budget > 0:
             cb = cpu_reference_rt(res["cpu_inputs"], args.cpu_budget) if wl.get("rt") else \
