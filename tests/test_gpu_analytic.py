@@ -45,7 +45,10 @@ def _wrap(x):
     return np.abs(np.angle(np.exp(1j * x)))
 
 
-def _compare(got, ref, maxc, r_tol=1e-8, ang_tol=1e-8, inf_tol=1e-2):
+def _compare(got, ref, maxc, r_tol=1e-8, ang_tol=1e-8, inf_tol=1e-2, polar=None):
+    """``polar``: pixels whose rays pass over the pole (angular momentum
+    |lambda| ~ 1e-15 on an image column through alpha = 0): phi jumps by pi
+    across lambda = 0 there and is compared to 1e-7 instead."""
     ok = ref["cls"] != 3
     same = ok & (got["cls"] == ref["cls"])
     assert same.sum() >= 0.999 * ok.sum(), (same.sum(), ok.sum())
@@ -56,10 +59,15 @@ def _compare(got, ref, maxc, r_tol=1e-8, ang_tol=1e-8, inf_tol=1e-2):
             continue
         np.testing.assert_allclose(got["r_hit"][k][m], ref["r_hit"][k][m], rtol=r_tol)
         np.testing.assert_allclose(got["g"][k][m], ref["g"][k][m], rtol=r_tol)
-        assert _wrap(got["phi_hit"][k][m] - ref["phi_hit"][k][m]).max() < ang_tol
+        dphi = _wrap(got["phi_hit"][k][m] - ref["phi_hit"][k][m])
+        tight = np.ones_like(dphi, bool) if polar is None else ~polar[m]
+        assert dphi[tight].max(initial=0.0) < ang_tol
+        assert dphi.max() < 1e-7
     hit = same & (ref["n_cross"] > 0)
-    np.testing.assert_allclose(got["flux"][hit], ref["flux"][hit], rtol=r_tol, atol=1e-300)
-    np.testing.assert_allclose(got["intensity"][same], ref["intensity"][same], rtol=r_tol, atol=1e-300)
+    # absolute floor at r_tol of the frame's peak: the flux vanishes at the ISCO,
+    # where its relative error is r's times r / (r - r_isco)
+    for f, m in (("flux", hit), ("intensity", same)):
+        np.testing.assert_allclose(got[f][m], ref[f][m], rtol=r_tol, atol=r_tol * np.abs(ref[f][m]).max(initial=0.0))
     esc = same & (ref["cls"] == 2)
     if esc.any():
         assert np.abs(got["theta_inf"][esc] - ref["theta_inf"][esc]).max() < inf_tol
@@ -76,6 +84,42 @@ def test_analytic_matches_oracle(cuda, oracle, spin, incl, form):
     same = _compare(got, ref, 3)
     assert (got["steps"] == 0).mean() > 0.99  # all but the fallback pixels solved in closed form
     assert (ref["n_cross"][same] >= 2).any()
+
+
+@pytest.mark.parametrize("spin,incl", [(0.998, 89.0), (-0.7, 30.0)])
+def test_analytic_extreme_observers(cuda, oracle, spin, incl):
+    """Near-extremal spin seen almost edge-on (the observer next to the
+    equator, where the polar motion starts close to its crossing), and a
+    retrograde hole, on a ragged 37 x 19 frame. Its middle column has
+    |alpha| ~ 1e-15: those rays pass within ~1e-16 rad of the pole, where the
+    azimuth is conditioned like 1/|lambda|; the closed form agrees with the
+    oracle to ~2e-8 there (sqrt of the FP64 epsilon) and to ~1e-11 elsewhere."""
+    s = _scene(spin=spin, incl=incl, width=37, height=19)
+    got = _gpu(s)
+    ref = oracle.trace_pixels(s)
+    alpha = s.alpha_min + (np.arange(37 * 19) % 37 + 0.5) * (s.alpha_max - s.alpha_min) / 37
+    _compare(got, ref, 3, polar=np.abs(alpha) < 1e-9)
+    assert (got["steps"] == 0).mean() > 0.95
+
+
+def test_analytic_single_pixel_and_partial_outputs(cuda, oracle):
+    """A 1 x 1 frame through the image centre's neighbour, and a frame that
+    asks for a subset of the outputs (the others NULL): the fields given are
+    the full trace's, bit for bit."""
+    one = _scene(n=1, alpha_min=-3.0, alpha_max=-2.9, beta_min=0.4, beta_max=0.5)
+    got = _gpu(one)
+    ref = oracle.trace_pixels(one)
+    _compare(got, ref, 3)
+    s = _abi.KerrScene.from_buffer_copy(_scene(n=40))
+    s.integrator = ANALYTIC
+    full = kerr.trace_image(s)
+    part = {"cls": torch.full((1600,), -7, dtype=torch.int32, device="cuda"),
+            "g": torch.full((3, 1600), -7.0, dtype=torch.float64, device="cuda")}
+    kerr.trace_image(s, part)
+    torch.cuda.synchronize()
+    assert torch.equal(part["cls"], full["cls"])
+    hit = full["n_cross"] > 0
+    assert torch.equal(part["g"][0][hit], full["g"][0][hit])
 
 
 def test_analytic_escape_direction_at_escape_radius(cuda, oracle):
