@@ -292,6 +292,18 @@ BHA_CALL double ellip_q_sc(double n, double s, double c, double m1, double &qc) 
   if (isnan(qc)) qc = ellip_qc(n, m1);
   return 2.0 * qc - q_part(n, s, -c, m1);
 }
+// The same with the complement nc = 1 - n given (1 - n s^2 = c^2 + nc s^2 with
+// no cancellation): the polar motion's n = z+ tends to 1 as lambda -> 0, and
+// 1 - z+ ~ lambda^2 drops below FP64 resolution when formed from z+.
+BHM_HD double ellip_qc_nc(double nc, double m1) { return bulirsch_cel(sqrt(m1), nc, 0.0, 1.0); }
+BHM_HD double q_part_nc(double nc, double s, double c, double m1) {
+  return s * s * s * carlson_rj(c * c, c * c + m1 * s * s, 1.0, c * c + nc * s * s) * (1.0 / 3.0);
+}
+BHA_CALL double ellip_q_sc_nc(double nc, double s, double c, double m1, double &qc) {
+  if (c >= 0.0) return q_part_nc(nc, s, c, m1);
+  if (isnan(qc)) qc = ellip_qc_nc(nc, m1);
+  return 2.0 * qc - q_part_nc(nc, s, -c, m1);
+}
 // Both poles at once (the same amplitude, characteristics n1, n2; c >= 0).
 BHA_CALL void ellip_q2_sc(double n1, double n2, double s, double c, double m1, double &q1, double &q2) {
   const double x = c * c, y = c * c + m1 * s * s, s2 = s * s, s3 = s2 * s * (1.0 / 3.0);
@@ -661,6 +673,7 @@ BHA_CALL void j_eval_escape(const RadSol &q, JPole &jp, JPole &jm, double &vp, d
 struct PolSol {
   bool crosses;
   double zp, w, mm, sz;  // U = (z+ - u^2)(a^2 u^2 + w), mm = a^2 z+, sz = sqrt(z+)
+  double zc;             // 1 - z+, formed without cancellation
   double m1;             // complementary parameter of -mm / w
   double sw;             // sqrt(w)
   double phi_start;      // Phi at the observer [Mino time]
@@ -677,6 +690,7 @@ BHA_CALL PolSol polar(double a2, double qTh, double lam, double u0, double pu0) 
   const double b2 = a2 - qTh;
   const double sq = sqrt(b2 * b2 + 4.0 * a2 * c0);
   t.zp = (b2 > 0.0) ? (b2 + sq) / (2.0 * a2) : 2.0 * c0 / (sq - b2);
+  t.zc = 2.0 * lam * lam / (a2 + qTh + sq);  // (a^2 + qTh)^2 - sq^2 = 4 a^2 lambda^2
   t.w = c0 / t.zp;
   t.mm = a2 * t.zp;
   t.sz = sqrt(t.zp);
@@ -699,8 +713,8 @@ BHA_CALL PolSol polar(double a2, double qTh, double lam, double u0, double pu0) 
 }
 
 BHM_HD void polar_q0(PolSol &t) {
-  if (isnan(t.q0)) t.q0 = ellip_q_sc(t.zp, t.s0, t.c0, t.m1, t.qc);
-  if (isnan(t.qc)) t.qc = ellip_qc(t.zp, t.m1);
+  if (isnan(t.q0)) t.q0 = ellip_q_sc_nc(t.zc, t.s0, t.c0, t.m1, t.qc);
+  if (isnan(t.qc)) t.qc = ellip_qc_nc(t.zc, t.m1);
 }
 
 // lambda int_0^tau dtau / (1 - u^2) at an equatorial crossing (chi = j pi,
@@ -722,7 +736,7 @@ BHA_CALL void polar_at(PolSol &t, double lam, double tau, double &u, double &pu,
   u = sg * t.sz * sa;
   pu = sg * t.sz * ca * sqrt(t.w + t.mm * sa * sa);
   polar_q0(t);
-  const double q = 2.0 * j * t.qc + ellip_q_sc(t.zp, sa, ca, t.m1, t.qc);
+  const double q = 2.0 * j * t.qc + ellip_q_sc_nc(t.zc, sa, ca, t.m1, t.qc);
   phi_th = lam * (tau + t.zp / t.sw * (q - t.q0));
 }
 

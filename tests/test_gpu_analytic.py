@@ -47,8 +47,10 @@ def _wrap(x):
 
 def _compare(got, ref, maxc, r_tol=1e-8, ang_tol=1e-8, inf_tol=1e-2, polar=None):
     """``polar``: pixels whose rays pass over the pole (angular momentum
-    |lambda| ~ 1e-15 on an image column through alpha = 0): phi jumps by pi
-    across lambda = 0 there and is compared to 1e-7 instead."""
+    |lambda| ~ 1e-15 on an image column through alpha = 0). Passing the pole
+    at an angular distance ~|lambda| turns the azimuth by pi within a Mino-time
+    width ~|lambda|: the closed form has that turn, the oracle's stepper
+    steps over it, so there phi is compared modulo pi."""
     ok = ref["cls"] != 3
     same = ok & (got["cls"] == ref["cls"])
     assert same.sum() >= 0.999 * ok.sum(), (same.sum(), ok.sum())
@@ -60,9 +62,9 @@ def _compare(got, ref, maxc, r_tol=1e-8, ang_tol=1e-8, inf_tol=1e-2, polar=None)
         np.testing.assert_allclose(got["r_hit"][k][m], ref["r_hit"][k][m], rtol=r_tol)
         np.testing.assert_allclose(got["g"][k][m], ref["g"][k][m], rtol=r_tol)
         dphi = _wrap(got["phi_hit"][k][m] - ref["phi_hit"][k][m])
-        tight = np.ones_like(dphi, bool) if polar is None else ~polar[m]
-        assert dphi[tight].max(initial=0.0) < ang_tol
-        assert dphi.max() < 1e-7
+        if polar is not None:
+            dphi = np.where(polar[m], np.minimum(dphi, np.abs(dphi - np.pi)), dphi)
+        assert dphi.max() < ang_tol
     hit = same & (ref["n_cross"] > 0)
     # absolute floor at r_tol of the frame's peak: the flux vanishes at the ISCO,
     # where its relative error is r's times r / (r - r_isco)
@@ -71,7 +73,10 @@ def _compare(got, ref, maxc, r_tol=1e-8, ang_tol=1e-8, inf_tol=1e-2, polar=None)
     esc = same & (ref["cls"] == 2)
     if esc.any():
         assert np.abs(got["theta_inf"][esc] - ref["theta_inf"][esc]).max() < inf_tol
-        assert _wrap(got["phi_inf"][esc] - ref["phi_inf"][esc]).max() < inf_tol
+        dinf = _wrap(got["phi_inf"][esc] - ref["phi_inf"][esc])
+        if polar is not None:
+            dinf = np.where(polar[esc], np.minimum(dinf, np.abs(dinf - np.pi)), dinf)
+        assert dinf.max() < inf_tol
     assert np.all(got["steps"][same & (got["steps"] == 0)] == 0)
     return same
 
@@ -91,9 +96,9 @@ def test_analytic_extreme_observers(cuda, oracle, spin, incl):
     """Near-extremal spin seen almost edge-on (the observer next to the
     equator, where the polar motion starts close to its crossing), and a
     retrograde hole, on a ragged 37 x 19 frame. Its middle column has
-    |alpha| ~ 1e-15: those rays pass within ~1e-16 rad of the pole, where the
-    azimuth is conditioned like 1/|lambda|; the closed form agrees with the
-    oracle to ~2e-8 there (sqrt of the FP64 epsilon) and to ~1e-11 elsewhere."""
+    |alpha| ~ 1e-15: those rays pass within ~1e-16 rad of the pole (see
+    _compare); modulo that turn the closed form agrees with the oracle to
+    ~1e-11 there as elsewhere."""
     s = _scene(spin=spin, incl=incl, width=37, height=19)
     got = _gpu(s)
     ref = oracle.trace_pixels(s)
