@@ -84,9 +84,27 @@ SURROGATE_WEIGHTS = ROOT / "blackhole_b200" / "data" / "surrogate_c4.npz"
 # The sky of escaping rays in the disk16 workload: 6 x 512 x 512 FP16 cubemap,
 # seeded uniform noise plus 10^4 point stars (bh_sky_generate).
 SKY_SIZE, SKY_STARS, SKY_SEED = 512, 10_000, 20261203
-# MACs per ray of the network (192x256 + 3 x 256x256 + 256x16), 2 FLOPs each.
-SURROGATE_FLOPS_PER_RAY = 2.0 * (192 * 256 + 3 * 256 * 256 + 256 * 16)
-OUT_FIELDS_USED = ("cls", "steps", "n_cross", "r_hit", "phi_hit", "g", "intensity", "theta_inf", "phi_inf")
+# Algorithmic MACs per ray of the network, 2 FLOPs each: 134 input features
+# (128 Fourier, 4 raw inputs, lambda, eta) x 256, 3 x 256 x 256, 256 x 16
+# heads. The kernel executes the input layer on 192 zero-padded columns
+# (three 64-column TMA boxes): SURROGATE_MMA_FLOPS_PER_RAY.
+SURROGATE_FLOPS_PER_RAY = 2.0 * (134 * 256 + 3 * 256 * 256 + 256 * 16)
+SURROGATE_MMA_FLOPS_PER_RAY = 2.0 * (192 * 256 + 3 * 256 * 256 + 256 * 16)
+OUT_FIELDS_USED = ("cls", "steps", "n_cross", "r_hit", "phi_hit", "g", "flux", "intensity", "theta_inf", "phi_inf")
+
+
+def fma_probe():
+    """The bench's FMA-pipe peak probe (blackhole_b200/lib/libbh_bench_probe.so,
+    built beside the tracer library but not part of it)."""
+    lib = C.CDLL(str(ROOT / "blackhole_b200" / "lib" / "libbh_bench_probe.so"))
+    lib.bh_bench_fma_peak.restype = C.c_int
+    lib.bh_bench_fma_peak.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
+    return lib
+
+
+def _check_probe(rc: int) -> None:
+    if rc != 0:
+        raise RuntimeError("bh_bench_fma_peak failed")
 
 
 def batch_frames(n: int = 4096, seed: int = 20261203):
@@ -244,14 +262,37 @@ def time_precision(args, precision: str, dev, stream, dist):
                 clocks=clocks, frame_ms=frame_ms, launch_cfg=tuned, batch=batch)
 
 
-def accuracy(ref_outs, test_outs) -> dict:
-    """Class agreement and |dg|/g of ``test`` against ``ref`` over all frames:
-    g compared at the last recorded crossing of pixels whose class and
-    crossing count agree."""
+def _stats(x, unit: str) -> dict:
+    """Median, 99.9th percentile and maximum of a 1-D tensor of errors."""
+    import torch
+
+    if x.numel() == 0:
+        return {"median": None, "p999": None, "max": None, "n": 0, "unit": unit}
+    xs = x.double()
+    q = torch.quantile(xs[:16_000_000], torch.tensor([0.5, 0.999], dtype=torch.float64, device=xs.device)).tolist()
+    return {"median": q[0], "p999": q[1], "max": float(xs.max().item()), "n": int(xs.numel()), "unit": unit}
+
+
+def _wrap_abs(d):
+    """|d| reduced modulo 2 pi into [0, pi] (azimuths are angles)."""
+    import torch
+
+    return torch.remainder(d + math.pi, 2.0 * math.pi).sub(math.pi).abs()
+
+
+def accuracy(ref_outs, test_outs, reference: str = "this run's FP64 path (bit-identical to the CPU oracle)") -> dict:
+    """Errors of ``test`` against ``ref`` over all frames. Class agreement over
+    every pixel; the other fields on pixels whose class (and, for disk
+    fields, crossing count) agree: r_hit and g relative at every crossing,
+    phi_hit in radians modulo 2 pi, flux and intensity absolute in units of
+    the frame's peak (the flux vanishes at the ISCO, so a relative error
+    there says nothing), theta_inf and phi_inf in radians on escaped pixels.
+    The legacy keys dg_over_g_* are g at the last recorded crossing."""
     import torch
 
     agree = total = 0
     dgs = []
+    errs = {k: [] for k in ("r_hit", "g", "phi_hit", "flux", "intensity", "theta_inf", "phi_inf")}
     for a, b in zip(ref_outs, test_outs):
         same_cls = a["cls"] == b["cls"]
         agree += int(same_cls.sum().item())
@@ -262,12 +303,33 @@ def accuracy(ref_outs, test_outs) -> dict:
         ga = a["g"][k, idx]
         gb = b["g"][k, idx]
         dgs.append((gb - ga).abs() / ga.abs())
+        maxc = a["r_hit"].shape[0] if "r_hit" in a else 0
+        for c in range(maxc):
+            m = same & (a["n_cross"] > c)
+            if "r_hit" in b:
+                errs["r_hit"].append(((b["r_hit"][c][m] - a["r_hit"][c][m]).abs() / a["r_hit"][c][m]))
+            if "g" in b:
+                errs["g"].append(((b["g"][c][m] - a["g"][c][m]).abs() / a["g"][c][m].abs()))
+            if "phi_hit" in a and "phi_hit" in b:
+                errs["phi_hit"].append(_wrap_abs(b["phi_hit"][c][m] - a["phi_hit"][c][m]))
+        for f, m in (("flux", same), ("intensity", same_cls)):
+            if f in a and f in b:
+                peak = float(a[f].abs().max().item()) or 1.0
+                errs[f].append((b[f][m] - a[f][m]).abs() / peak)
+        esc = same_cls & (a["cls"] == 2)
+        if "theta_inf" in a and "theta_inf" in b:
+            errs["theta_inf"].append((b["theta_inf"][esc] - a["theta_inf"][esc]).abs())
+        if "phi_inf" in a and "phi_inf" in b:
+            errs["phi_inf"].append(_wrap_abs(b["phi_inf"][esc] - a["phi_inf"][esc]))
     dg = torch.cat(dgs)
     q = torch.quantile(dg[: 16_000_000].float(), torch.tensor([0.5, 0.999], device=dg.device)).tolist() \
         if dg.numel() else [None, None]
+    units = {"r_hit": "relative", "g": "relative", "phi_hit": "rad (mod 2 pi)", "flux": "of the frame's peak",
+             "intensity": "of the frame's peak", "theta_inf": "rad", "phi_inf": "rad (mod 2 pi)"}
+    fields = {f: _stats(torch.cat(v), units[f]) for f, v in errs.items() if v}
     return {"class_agreement": agree / total, "dg_over_g_median": q[0], "dg_over_g_p999": q[1],
             "dg_over_g_max": float(dg.max().item()) if dg.numel() else None, "pixels_compared": int(dg.numel()),
-            "reference": "this run's FP64 path (bit-identical to the CPU oracle)"}
+            "fields": fields, "reference": reference}
 
 
 def run_ours(args, rank: int, world: int, dist):
@@ -337,14 +399,14 @@ def run_ours(args, rank: int, world: int, dist):
     # ---- roofline of the headline tracing kernel ----
     fp64 = args.precision == "fp64"
     peak = C.c_double(0.0)
-    _abi.check(lib.bh_measure_fma_peak(1 if fp64 else 0, 5, C.byref(peak)))
+    _check_probe(fma_probe().bh_bench_fma_peak(1 if fp64 else 0, 5, C.byref(peak)))
     mean_launch_s = statistics.mean(head["launch_ms"]) * 1e-3
     flops_per_launch = FLOPS_PER_STEP[integ] * head["total_steps"]
     achieved = flops_per_launch / mean_launch_s / 1e12
     kname = "k_trace_batch_fp64" if fp64 else "k_trace_batch_mixed"
     roofline = {"bound": "fp64" if fp64 else "fp32", "achieved": achieved, "peak": peak.value,
                 "unit": "TFLOP/s", "frac": achieved / peak.value if peak.value else None, "traffic": None,
-                "peak_source": "measured FMA-pipe probe (bh_measure_fma_peak), FMA = 2 FLOPs",
+                "peak_source": "this repository's own FMA-pipe probe (bh_bench_fma_peak, lib/libbh_bench_probe.so; MEASURED_PEAKS.json has no FP32/FP64 figure), FMA = 2 FLOPs",
                 "flops_per_step": FLOPS_PER_STEP[integ], "steps_per_launch": head["total_steps"],
                 "kernel": f"{kname}<{1 if integ == 'dp45' else 0}>",
                 "launch_ms_mean": statistics.mean(head["launch_ms"]),
@@ -462,10 +524,22 @@ def run_surrogate(args, rank: int, world: int, dist):
     msc0 = _timed_launches(lambda: kerr.trace_image(c0, oc0, stream=stream), stream, 2, 1)
     fp64_dp45 = n / (statistics.mean(ms64) * 1e-3)
     fp64_rk4 = 256 * 256 / (statistics.mean(msc0) * 1e-3)
+    # ---- the closed-form tracer (BH_INTEGRATOR_ANALYTIC) on the same frame, FP64 ----
+    san = _abi.KerrScene.from_buffer_copy(s64)
+    san.integrator = _abi.INTEGRATOR_ANALYTIC
+    oan = kerr.alloc_image_outputs(san, device=dev, fields=list(OUT_FIELDS_USED))
+    ms_an = _timed_launches(lambda: kerr.trace_image(san, oan, stream=stream), stream, 3, 1)
+    disk_fields = [f for f in OUT_FIELDS_USED if f not in ("phi_hit", "phi_inf")]
+    oan_d = kerr.alloc_image_outputs(san, device=dev, fields=disk_fields)
+    ms_an_d = _timed_launches(lambda: kerr.trace_image(san, oan_d, stream=stream), stream, 3, 1)
+    # ---- ablation at equal outputs: the same render asked for the disk fields only ----
+    outs_d = kerr.alloc_image_outputs(smx, device=dev, fields=disk_fields)
+    ms_sd = _timed_launches(lambda: net.trace_image(smx, outs_d, stream=stream), stream, 3, 1)
+    steps64 = int(o64["steps"].sum().item())
     extra = {
         "fp64_plain": {"value": fp64_dp45, "unit": UNIT, "ms_per_step": statistics.mean(ms64),
                        "method": f"FP64 DP45 rtol 1e-8 on the same {smx.width}x{smx.height} frame",
-                       "steps_per_ray": float(o64["steps"].double().mean().item())},
+                       "steps_per_ray": steps64 / n},
         "fp64_plain_rk4": {"value": fp64_rk4, "unit": UNIT, "ms_per_step": statistics.mean(msc0),
                            "method": "FP64 RK4 h = 0.02 min(r, 20), the plain method of the 256^2 frame of this "
                                      "scene (rays/s measured on that frame)",
@@ -476,16 +550,14 @@ def run_surrogate(args, rank: int, world: int, dist):
         "speedup_vs_fp64_rk4": value / fp64_rk4,
         "surrogate_stats": stats,
         "accuracy_vs_fp64": accuracy([o64], [outs]),
+        "accuracy_vs_closed_form": accuracy(
+            [oan], [outs], reference="this run's closed-form FP64 tracer: exact at the escape radius, where the "
+                                     "DP45 stepper reports escape angles after its last step's overshoot"),
         "render_ms": {"mean": statistics.mean(render_ms), "min": min(render_ms), "max": max(render_ms)},
+        "steps_per_s_note": "FP64 DP45 accepted steps of the same frame per second of render: the integration "
+                            "the render stands in for (its own integrator steps, on rejected pixels: "
+                            f"{int(outs['steps'].sum().item())} per render)",
     }
-    # ---- the closed-form tracer (BH_INTEGRATOR_ANALYTIC) on the same frame, FP64 ----
-    san = _abi.KerrScene.from_buffer_copy(s64)
-    san.integrator = _abi.INTEGRATOR_ANALYTIC
-    oan = kerr.alloc_image_outputs(san, device=dev, fields=list(OUT_FIELDS_USED))
-    ms_an = _timed_launches(lambda: kerr.trace_image(san, oan, stream=stream), stream, 3, 1)
-    disk_fields = [f for f in OUT_FIELDS_USED if f not in ("phi_hit", "phi_inf")]
-    oan_d = kerr.alloc_image_outputs(san, device=dev, fields=disk_fields)
-    ms_an_d = _timed_launches(lambda: kerr.trace_image(san, oan_d, stream=stream), stream, 3, 1)
     extra["analytic"] = {
         "value": n / (statistics.mean(ms_an) * 1e-3), "unit": UNIT, "ms_per_step": statistics.mean(ms_an),
         "method": "every ray in closed form in Mino time (Jacobi sn/cn, Carlson R_J, Bulirsch cel), FP64, "
@@ -496,6 +568,14 @@ def run_surrogate(args, rank: int, world: int, dist):
         "disk_outputs_only": {"value": n / (statistics.mean(ms_an_d) * 1e-3), "unit": UNIT,
                               "ms_per_step": statistics.mean(ms_an_d), "fields": disk_fields,
                               "speedup_vs_fp64_plain": statistics.mean(ms64) / statistics.mean(ms_an_d)},
+    }
+    extra["ablation_equal_outputs"] = {
+        "all_fields": {"fields": list(OUT_FIELDS_USED), "surrogate_ms": statistics.mean(render_ms),
+                       "closed_form_ms": statistics.mean(ms_an), "mixed_dp45_ms": statistics.mean(msmx)},
+        "disk_fields": {"fields": disk_fields, "surrogate_ms": statistics.mean(ms_sd),
+                        "closed_form_ms": statistics.mean(ms_an_d)},
+        "note": "the renderer without a trained network sends every pixel to its fallback, the closed-form "
+                "tracer; both renders give every field from an exact solve (accuracy keys above)",
     }
 
     # ---- network inference alone: the tensor-core kernel's roofline ----
@@ -510,7 +590,8 @@ def run_surrogate(args, rank: int, world: int, dist):
                 "traffic": INFER_DRAM_BYTES_2048 if (smx.width, smx.height) == (2048, 2048) else None,
                 "traffic_unit": "bytes per launch (dram read + write, ncu)",
                 "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst, of measured)" if peak else "fallback 1.59 PF",
-                "kernel": "k_mlp_infer", "flops_per_ray": SURROGATE_FLOPS_PER_RAY, "rays_per_launch": n,
+                "kernel": "k_mlp_infer", "flops_per_ray": SURROGATE_FLOPS_PER_RAY,
+                "mma_flops_per_ray_executed": SURROGATE_MMA_FLOPS_PER_RAY, "rays_per_launch": n,
                 "launch_ms_mean": statistics.mean(fwd_ms),
                 "note": "network inference timed alone on the frame's inputs; a render also runs the refinement "
                         "kernel (FP64 set-up, FP32 quadrature) concurrently and the integrator on rejected pixels"}
@@ -520,7 +601,7 @@ def run_surrogate(args, rank: int, world: int, dist):
     # ---- end to end through the host-buffer C entry point (pinned host memory) ----
     e2e = None
     if rank == 0:
-        fields = ("cls", "n_cross", "r_hit", "g", "flux", "intensity")
+        fields = OUT_FIELDS_USED  # the headline render's outputs, all copied back
         pinned = {f: torch.empty(n * (smx.max_crossings if f in _abi.PLANE_FIELDS else 1),
                                  dtype=torch.int32 if f in _abi.INT_FIELDS else torch.float64).pin_memory()
                   for f in fields}
@@ -541,7 +622,7 @@ def run_surrogate(args, rank: int, world: int, dist):
     # inputs, chunks x (inference, refinement), the closed-form and DP45 fallback tracers
     launches = (1 + 2 * chunks + 2) * args.steps
     return dict(value=value, ms_per_step=elapsed_ms / args.steps, e2e=e2e, roofline=roofline, clocks=clocks,
-                total_steps=int(outs["steps"].sum().item()), rays_per_step=n, launches=launches, extra=extra)
+                total_steps=steps64, rays_per_step=n, launches=launches, extra=extra)
 
 
 def run_analytic(args, rank: int, world: int, dist):
@@ -715,11 +796,11 @@ def run_rt(args, rank: int, world: int, dist):
     from blackhole_b200 import _abi
 
     peak = C.c_double(0.0)
-    _abi.check(_abi.load_library().bh_measure_fma_peak(1 if prec == 0 else 0, 5, C.byref(peak)))
+    _check_probe(fma_probe().bh_bench_fma_peak(1 if prec == 0 else 0, 5, C.byref(peak)))
     achieved = FLOPS_PER_STEP["rt"] * steps / (statistics.mean(ms) * 1e-3) / 1e12
     roofline = {"bound": "fp64" if prec == 0 else "fp32", "achieved": achieved, "peak": peak.value,
                 "unit": "TFLOP/s", "frac": achieved / peak.value if peak.value else None, "traffic": None,
-                "peak_source": "measured FMA-pipe probe (bh_measure_fma_peak), FMA = 2 FLOPs",
+                "peak_source": "this repository's own FMA-pipe probe (bh_bench_fma_peak, lib/libbh_bench_probe.so; MEASURED_PEAKS.json has no FP32/FP64 figure), FMA = 2 FLOPs",
                 "flops_per_step": FLOPS_PER_STEP["rt"], "steps_per_launch": steps,
                 "kernel": "k_trace_rt_fp64" if prec == 0 else "k_trace_rt_mixed",
                 "launch_ms_mean": statistics.mean(ms),
@@ -888,7 +969,7 @@ def main():
                        "policy": {"min_confidence": 0.99, "critical_band_M": 0.05, "verify": "radial kind"},
                        "launch": "7 launches per render on two streams: inputs, 2 x (inference, refinement), "
                                  "the closed-form tracer and DP45 on the rejected pixels",
-                       "l2": f"outputs ({wl['width']}^2 pixels x 9 fields) written once per step, larger than L2"})
+                       "l2": f"outputs ({wl['width']}^2 pixels x 10 fields) written once per step, larger than L2"})
 
     if args.impl == "reference":
         if rank != 0:

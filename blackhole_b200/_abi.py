@@ -242,8 +242,10 @@ def _declare(lib: C.CDLL) -> None:
     lib.bh_kerr_trace_image_sky.argtypes = [C.POINTER(KerrScene), C.POINTER(KerrImageOut), C.POINTER(SkyCubemap), vp]
     lib.bh_kerr_batch_set_sky.restype = C.c_int
     lib.bh_kerr_batch_set_sky.argtypes = [vp, C.POINTER(SkyCubemap)]
-    lib.bh_measure_fma_peak.restype = C.c_int
-    lib.bh_measure_fma_peak.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
+    lib.bh_debug_device_allocations.restype = C.c_int64
+    lib.bh_debug_device_allocations.argtypes = []
+    lib.bh_debug_fail_device_allocation.restype = C.c_int
+    lib.bh_debug_fail_device_allocation.argtypes = [C.c_int64]
     # include/bh_surrogate.h
     lib.bh_surrogate_param_count.restype = i64
     lib.bh_surrogate_param_count.argtypes = []
@@ -264,6 +266,12 @@ def _declare(lib: C.CDLL) -> None:
     lib.bh_surrogate_train_step.argtypes = [vp, vp, vp, i64, C.POINTER(AdamConfig), vp, vp]
     lib.bh_surrogate_device_error.restype = C.c_int
     lib.bh_surrogate_device_error.argtypes = [vp]
+    lib.bh_surrogate_get_state.restype = C.c_int
+    lib.bh_surrogate_get_state.argtypes = [vp, vp, vp, C.c_int64, C.POINTER(C.c_int64)]
+    lib.bh_surrogate_set_state.restype = C.c_int
+    lib.bh_surrogate_set_state.argtypes = [vp, vp, vp, C.c_int64, C.c_int64]
+    lib.bh_surrogate_set_wait_limit.restype = C.c_int
+    lib.bh_surrogate_set_wait_limit.argtypes = [vp, C.c_int64]
     lib.bh_surrogate_make_targets.restype = C.c_int
     lib.bh_surrogate_make_targets.argtypes = [C.POINTER(KerrImageOut), i64, C.c_int, vp, vp]
     lib.bh_surrogate_grid_inputs.restype = C.c_int

@@ -1,11 +1,11 @@
-// probe.cu - FMA-throughput probe giving the measured FP64 / FP32 pipe peak
-// that the tracer kernels' roofline fractions divide by.
+// fma_probe.cu - FMA-throughput probe giving the measured FP64 / FP32 pipe
+// peak that bench.py divides the tracer kernels' FLOP rates by. A measuring
+// tool of the bench, built into its own library (lib/libbh_bench_probe.so),
+// not part of the tracer library.
 //
 // Each thread runs 8 independent FMA chains for `iters` iterations; the grid
 // covers every SM at full occupancy. FLOPs = 2 * 8 * iters * threads.
 #include <cuda_runtime.h>
-
-#include "launch.h"
 
 namespace {
 
@@ -29,7 +29,11 @@ __global__ void __launch_bounds__(256) k_fma_probe(T *out, int iters, T x, T y) 
 
 }  // namespace
 
-extern "C" int bhk_fma_probe(int fp64, int iters, int repeats, double *tflops) {
+// Best of `repeats` launches (after one warm-up), in TFLOP/s (FMA = 2 FLOPs).
+extern "C" int bh_bench_fma_peak(int fp64, int repeats, double *tflops) {
+  const int iters = 1 << 14;
+  if (!tflops) return -1;
+  if (repeats < 1) repeats = 1;
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

@@ -91,53 +91,13 @@ BHM_HD double carlson_rc(double x, double y) {
   return f * g * inv_sqrt(x);
 }
 
-// R_C(1, 1 + e) (e > -1): atan(sqrt e) / sqrt e, atanh(sqrt -e) / sqrt -e, or
-// its series for |e| < 1e-3.
-BHM_HD double carlson_rc1(double e) {
-  if (fabs(e) < 1e-3) return 1.0 - e * (1.0 / 3.0 - e * (0.2 - e * (1.0 / 7.0 - e * (1.0 / 9.0 - e * (1.0 / 11.0)))));
-  if (e > 0.0) {
-    const double se = sqrt(e);
-    return atan(se) / se;
-  }
-  const double se = sqrt(-e);
-  return atanh(se) / se;
-}
+// R_C(1, 1 + e) (e > -1), shared with the surrogate's refinement (mino_solve.cuh).
+BHM_HD double carlson_rc1(double e) { return bhmino::rc1<double>(e); }
 
-// The fifth-order expansion of R_J about the mean of its arguments.
-BHM_HD double rj_series(double X, double Y, double Z, double P) {
-  const double E2 = X * Y + X * Z + Y * Z - 3.0 * P * P;
-  const double E3 = X * Y * Z + 2.0 * E2 * P + 4.0 * P * P * P;
-  const double E4 = (2.0 * X * Y * Z + E2 * P + 3.0 * P * P * P) * P;
-  const double E5 = X * Y * Z * P * P;
-  return 1.0 - (3.0 / 14.0) * E2 + E3 * (1.0 / 6.0) + (9.0 / 88.0) * E2 * E2 - (3.0 / 22.0) * E4 -
-         (9.0 / 52.0) * E2 * E3 + (3.0 / 26.0) * E5;
-}
-
-// R_J(x, y, z, p) for p > 0 in Carlson's 1995 form: R_J = 4^-n A_n^-3/2 S +
-// 6 sum_m 4^-m R_C(1, 1 + e_m) / d_m, d_m = (sqrt p_m + sqrt x_m)(sqrt p_m + sqrt y_m)
-// (sqrt p_m + sqrt z_m), e_m = 4^-3m delta / d_m^2, delta = (p - x)(p - y)(p - z):
-// e_m falls by 64 per step, so all but the first terms take the series.
-BHA_CALL double carlson_rj_pos(double x, double y, double z, double p) {
-  const double delta = (p - x) * (p - y) * (p - z);
-  double sum = 0.0, fac = 1.0, f3 = 1.0;
-  for (int it = 0; it < 60; ++it) {
-    const double sx = sqrt(x), sy = sqrt(y), sz = sqrt(z), sp = sqrt(p);
-    const double lam = sx * sy + sy * sz + sz * sx;
-    const double d = (sp + sx) * (sp + sy) * (sp + sz);
-    sum += fac * carlson_rc1(f3 * delta / (d * d)) / d;
-    fac *= 0.25;
-    f3 *= 1.0 / 64.0;
-    x = 0.25 * (x + lam);
-    y = 0.25 * (y + lam);
-    z = 0.25 * (z + lam);
-    p = 0.25 * (p + lam);
-    const double A = (x + y + z + 2.0 * p) * 0.2;
-    const double X = (A - x) / A, Y = (A - y) / A, Z = (A - z) / A, P = (A - p) / A;
-    if (fmax(fmax(fabs(X), fabs(Y)), fmax(fabs(Z), fabs(P))) < 1e-3)
-      return 6.0 * sum + fac * rj_series(X, Y, Z, P) * inv_sqrt(A) / A;
-  }
-  return NAN;
-}
+// R_J(x, y, z, p) for p > 0 in Carlson's 1995 form (mino_solve.cuh), as one
+// shared device call.
+BHA_CALL double carlson_rj_pos(double x, double y, double z, double p) { return bhmino::rj_pos<double>(x, y, z, p); }
+BHM_HD double rj_series(double X, double Y, double Z, double P) { return bhmino::rj_series<double>(X, Y, Z, P); }
 
 // R_J for any p != 0 (x, y, z >= 0, at most one zero); p < 0 gives the
 // Cauchy principal value via an R_J with positive fourth argument.
@@ -240,41 +200,9 @@ BHM_HD void sncndn_neg(double u, double m1, double &sn, double &cn, double &dn) 
   dn = 1.0 / d;
 }
 
-// Bulirsch's complete integral cel(kc, p, a, b) = int_0^(pi/2) (a cos^2 + b sin^2) /
-// ((cos^2 + p sin^2) sqrt(cos^2 + kc^2 sin^2)) dphi (R. Bulirsch, Numer. Math. 13
-// (1969) 305-315), a Gauss-type iteration with quadratic convergence; p < 0
-// gives the Cauchy principal value.
-BHA_CALL double bulirsch_cel(double kc, double p, double a, double b) {
-  kc = fabs(kc);
-  double e = kc, em = 1.0;
-  if (p > 0.0) {
-    p = sqrt(p);
-    b /= p;
-  } else {
-    double f = kc * kc, q = 1.0 - f;
-    const double g = 1.0 - p;
-    f -= p;
-    q *= (b - a * p);
-    p = sqrt(f / g);
-    a = (a - b) / g;
-    b = -q / (g * g * p) + a * p;
-  }
-  for (int it = 0; it < 40; ++it) {
-    const double f = a;
-    a += b / p;
-    double g = e / p;
-    b += f * g;
-    b += b;
-    p = g + p;
-    g = em;
-    em += kc;
-    if (fabs(g - kc) <= g * 1e-15) break;
-    kc = sqrt(e);
-    kc += kc;
-    e = kc * em;
-  }
-  return 1.5707963267948966 * (b + a * em) / (em * (em + p));
-}
+// Bulirsch's complete integral cel(kc, p, a, b) (mino_solve.cuh; p < 0 gives
+// the Cauchy principal value), as one shared device call.
+BHA_CALL double bulirsch_cel(double kc, double p, double a, double b) { return bhmino::cel<double>(kc, p, a, b); }
 
 // The complete Q(n; pi/2 | m) = int_0^(pi/2) sin^2 / ((1 - n sin^2) dn) = cel(sqrt m1, 1 - n, 0, 1).
 BHM_HD double ellip_qc(double n, double m1) { return bulirsch_cel(sqrt(m1), 1.0 - n, 0.0, 1.0); }
@@ -678,7 +606,7 @@ struct PolSol {
   double sw;             // sqrt(w)
   double phi_start;      // Phi at the observer [Mino time]
   double tau1, period;   // first crossing, time between crossings
-  double s0, c0;         // chi at the observer: sin, cos (chi0 in (-pi/2, pi])
+  double s0, c0;         // chi at the observer: sin, cos (chi0 in (-pi/2, 3 pi/2); cos has the sign of du/dtau)
   double q0, qc;         // Q(z+; chi0) and the complete Q(z+) (NaN until needed)
 };
 
@@ -703,7 +631,8 @@ BHA_CALL PolSol polar(double a2, double qTh, double lam, double u0, double pu0) 
   const double phi_x = s0 * carlson_rf(t.w * c2, t.w + t.mm * s0 * s0, t.w);
   const double K = bhmino::quarter_period<double>(t.w, t.mm);
   t.phi_start = (pu0 >= 0.0) ? phi_x : 2.0 * K - phi_x;
-  t.tau1 = ((pu0 * u0) < 0.0) ? phi_x : 2.0 * K - phi_x;
+  // |Phi(chi0)| to the next crossing when moving toward the equator, else over the turning point
+  t.tau1 = ((pu0 * u0) < 0.0) ? fabs(phi_x) : 2.0 * K - fabs(phi_x);
   t.period = 2.0 * K;
   t.s0 = s0;
   t.c0 = (pu0 >= 0.0 ? 1.0 : -1.0) * sqrt(c2);  // dchi/dtau > 0: cos chi has the sign of du/dtau
@@ -719,7 +648,18 @@ BHM_HD void polar_q0(PolSol &t) {
 
 // lambda int_0^tau dtau / (1 - u^2) at an equatorial crossing (chi = j pi,
 // Q(z+; j pi) = 2 j Q(pi/2)): lambda (tau + (z+ / sqrt(w)) (2 j Q_c - Q(chi0))).
+// With 1 - z+ == 0 (lambda == 0, or lambda^2 below the smallest double) the
+// integral is its limit lambda -> 0 from the side of lambda's sign: a turn by
+// copysign(pi, lambda) at each pass over the pole (chi = pi/2 + j pi), so
+// lambda = +0 and -0 continue their two sides, which agree modulo 2 pi.
+BHM_HD double pole_turns(const PolSol &t, double lam, double tau) {
+  const double K = 0.5 * t.period;
+  const double passes = floor((t.phi_start + tau - K) / t.period) - floor((t.phi_start - K) / t.period);
+  return copysign(3.141592653589793, lam) * passes;
+}
+
 BHA_CALL double phi_theta_crossing(PolSol &t, double lam, double tau) {
+  if (!(t.zc > 0.0)) return pole_turns(t, lam, tau);
   polar_q0(t);
   const double j = rint((t.phi_start + tau) / t.period);
   return lam * (tau + t.zp / t.sw * (2.0 * j * t.qc - t.q0));
@@ -735,6 +675,10 @@ BHA_CALL void polar_at(PolSol &t, double lam, double tau, double &u, double &pu,
   const double sg = fmod(j, 2.0) != 0.0 ? -1.0 : 1.0;
   u = sg * t.sz * sa;
   pu = sg * t.sz * ca * sqrt(t.w + t.mm * sa * sa);
+  if (!(t.zc > 0.0)) {
+    phi_th = pole_turns(t, lam, tau);
+    return;
+  }
   polar_q0(t);
   const double q = 2.0 * j * t.qc + ellip_q_sc_nc(t.zc, sa, ca, t.m1, t.qc);
   phi_th = lam * (tau + t.zp / t.sw * (q - t.q0));

@@ -226,7 +226,6 @@ int bhk_trace_list_analytic(const BhkImageParams *p, const BhkImageOut *o, const
 int bhk_trace_list_fp64(const BhkImageParams *p, const BhkImageOut *o, const int *list, const unsigned int *count,
                         unsigned long long *counter, BhkLaunch L, void *stream);
 
-int bhk_fma_probe(int fp64, int iters, int repeats, double *tflops);
 
 // Last CUDA error string of the device layer (thread-local).
 const char *bhk_last_error(void);

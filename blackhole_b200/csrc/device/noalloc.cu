@@ -16,7 +16,6 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
-#include <mutex>
 
 #include "../../../include/bh_kerr.h"
 #include "launch.h"
@@ -25,30 +24,21 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[BH_NOALLOC_SCRA
 
 namespace {
 
-constexpr int kMaxDevices = 64;
-void *g_scratch_addr[kMaxDevices] = {};
-std::mutex g_scratch_mu;
-
-// Device address of g_noalloc_scratch on the current device. Looked up once
-// per device with that device current; in host code the array's name is only
-// a host-side stand-in and must never be handed to a kernel.
+// Device address of g_noalloc_scratch on the current device, looked up on
+// every call with that device current (cudaGetSymbolAddress allocates
+// nothing; once the module is loaded it is a table lookup). An address kept
+// from an earlier call would dangle after cudaDeviceReset, which reloads the
+// module elsewhere. In host code the array's name is only a host-side
+// stand-in and must never be handed to a kernel.
 int scratch_address(void **out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return bhh_fail(cudaGetErrorString(e));
-  if (dev < 0 || dev >= kMaxDevices) return bhh_fail("device ordinal out of range");
-  std::lock_guard<std::mutex> lk(g_scratch_mu);
-  if (!g_scratch_addr[dev]) {
-    void *p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) {
-      char msg[256];
-      std::snprintf(msg, sizeof(msg), "cudaGetSymbolAddress(no-allocation scratch): %s", cudaGetErrorString(e));
-      return bhh_fail(msg);
-    }
-    g_scratch_addr[dev] = p;
+  void *p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p) {
+    char msg[256];
+    std::snprintf(msg, sizeof(msg), "cudaGetSymbolAddress(no-allocation scratch): %s", cudaGetErrorString(e));
+    return bhh_fail(msg);
   }
-  *out = g_scratch_addr[dev];
+  *out = p;
   return 0;
 }
 

@@ -25,7 +25,11 @@ namespace {
 constexpr int kBM = 128;
 constexpr int kBK = 64;
 constexpr int kStages = 4;
-constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s per wait, then an error code
+// Waits on other warps' progress run out after the caller's limit (default
+// 2 s; bh_surrogate_set_wait_limit) and record an error code. Work this
+// thread itself started (TMA loads, MMAs) is then drained with a fixed limit
+// before TMEM is freed and the CTA exits: it completes on its own.
+constexpr uint64_t kDrainNs = 1000000000ull;
 
 enum : int { kErrProducer = 11, kErrMma = 12, kErrDone = 13 };
 
@@ -61,6 +65,25 @@ __device__ __forceinline__ float silu_grad(float y) {
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
   const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
   return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+__device__ __forceinline__ uint32_t pack_f16(float lo, float hi) {
+  uint32_t r;
+  asm("cvt.rn.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+  return r;
+}
+
+// SiLU of two pre-activations given as halves hy = y / 2 (FP32), returned as
+// packed FP16: hy (1 + tanh hy) = y sigmoid(y), with one tanh.approx.f16x2
+// (one MUFU operation for both) and one f16x2 FMA. The activation is the next
+// layer's FP16 operand, so nothing is unpacked; FP16 keeps 11 significant
+// bits, as many as the MUFU tanh delivers.
+__device__ __forceinline__ uint32_t silu_f16x2(float hy_lo, float hy_hi) {
+  const uint32_t h = pack_f16(hy_lo, hy_hi);
+  uint32_t t, r;
+  asm("tanh.approx.f16x2 %0, %1;" : "=r"(t) : "r"(h));
+  asm("fma.rn.f16x2 %0, %1, %2, %2;" : "=r"(r) : "r"(t), "r"(h));
+  return r;
 }
 
 __device__ __forceinline__ void store_bf16x16(__nv_bfloat16* dst, const float (&h)[16]) {
@@ -170,7 +193,7 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 template <int BN, class Epi>
 __global__ void __launch_bounds__(128, 1)
   k_gemm_bf16(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, int K,
-        int kchunks_per_split, Epi epi, int* err) {
+        int kchunks_per_split, Epi epi, int* err, uint64_t wait_ns) {
   using Cfg = GemmCfg<BN>;
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = umma::smem_u32(smem_raw);
@@ -212,9 +235,10 @@ __global__ void __launch_bounds__(128, 1)
   const uint32_t tmem = *tmem_slot;
 
   if (warp == 0 && lane == 0) {
+    int issued = 0;
     for (int i = 0; i < nch; ++i) {
       const int s = i % kStages;
-      if (i >= kStages && !umma::mbar_wait(empty(s), ((i / kStages) - 1) & 1, kWaitNs)) {
+      if (i >= kStages && !umma::mbar_wait(empty(s), ((i / kStages) - 1) & 1, wait_ns)) {
         atomicExch(err, kErrProducer);
         break;
       }
@@ -222,12 +246,16 @@ __global__ void __launch_bounds__(128, 1)
       const int kx = (c0 + i) * kBK;
       umma::tma_load_2d(sA(s), &ta, full(s), kx, m0);
       umma::tma_load_2d(sB(s), &tb, full(s), kx, n0);
+      issued = i + 1;
     }
+    // the last load issued on each stage has landed before the CTA may exit
+    for (int i = max(0, issued - kStages); i < issued; ++i)
+      umma::mbar_wait(full(i % kStages), (i / kStages) & 1, kDrainNs);
   } else if (warp == 1 && lane == 0) {
     constexpr uint32_t idesc = umma::idesc_bf16_f32(kBM, BN);
     for (int i = 0; i < nch; ++i) {
       const int s = i % kStages;
-      if (!umma::mbar_wait(full(s), (i / kStages) & 1, kWaitNs)) {
+      if (!umma::mbar_wait(full(s), (i / kStages) & 1, wait_ns)) {
         atomicExch(err, kErrMma);
         break;
       }
@@ -243,10 +271,10 @@ __global__ void __launch_bounds__(128, 1)
   }
   __syncwarp();
 
-  bool ok = umma::mbar_wait(done, 0, kWaitNs);
+  bool ok = umma::mbar_wait(done, 0, wait_ns);
   if (!ok) {
     atomicExch(err, kErrDone);
-    ok = umma::mbar_wait(done, 0, kWaitNs);  // let tensor-core work in flight drain before TMEM is freed
+    umma::mbar_wait(done, 0, kDrainNs);  // let tensor-core work in flight drain before TMEM is freed
   }
   umma::tc_fence_after();
   const int64_t row = (int64_t)m0 + warp * 32 + lane;
@@ -422,7 +450,12 @@ __global__ void k_loss(const float* __restrict__ out, const float* __restrict__ 
 
 // ---- fused inference -----------------------------------------------------------
 //
-// One persistent CTA per SM runs the whole network on pairs of 128-row tiles.
+// One persistent CTA per SM runs the whole network on pairs of 128-row tiles,
+// in FP16 (weights and activations; FP32 accumulation): the network is
+// trained in BF16, and FP16's 11 significant bits evaluate it more closely,
+// while letting SiLU run as tanh.approx.f16x2 -- one MUFU operation per two
+// activations, which halves the epilogue's bound (at one tanh per element
+// the MUFU pipe alone took as long as the layer's MMAs).
 // Warp 0 streams weight K-chunks by TMA through a 3-stage ring (each chunk
 // is loaded once per tile), warp 1 issues the tcgen05 MMAs, warps 2-9 and
 // 10-17 are the epilogues of tile slots 0 and 1 (two warps per TMEM lane
@@ -450,7 +483,8 @@ struct InferArgs {
   int64_t n;
   int64_t pairs;
   int* err;
-  float bias[kBiasCount];  // layers 0..3 (256 each), then the head (16)
+  uint64_t wait_ns;  // limit of each wait on another warp's progress
+  float bias[kBiasCount];  // layers 0..3 (256 each, halved: b / 2), then the head (16, as is)
 };
 
 __device__ __forceinline__ int layer_chunks(int l) { return (l == 0 ? BHS_FEATURES : BHS_HIDDEN) / kBK; }
@@ -472,12 +506,13 @@ __global__ void __launch_bounds__(kInfThreads, 1)
   const uint32_t act0 = raw + pad;
   const uint32_t ring0 = act0 + 2u * kActBytes;
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + pad + 2 * kActBytes + kInfRing * kWChunk);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kInfRing + 4);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kInfRing + 5);
   const uint32_t b0 = umma::smem_u32(bars);
   auto full = [&](int i) { return b0 + 8u * i; };
   auto empty = [&](int i) { return b0 + 8u * (kInfRing + i); };
   auto act_ready = [&](int s) { return b0 + 8u * (2 * kInfRing + s); };
   auto acc_full = [&](int s) { return b0 + 8u * (2 * kInfRing + 2 + s); };
+  const uint32_t drained = b0 + 8u * (2 * kInfRing + 4);  // every MMA issued has completed
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
   if (threadIdx.x == 0) {
@@ -489,6 +524,7 @@ __global__ void __launch_bounds__(kInfThreads, 1)
       umma::mbar_init(act_ready(s), kEpiThreads);
       umma::mbar_init(acc_full(s), 1);
     }
+    umma::mbar_init(drained, 1);
     umma::fence_mbar_init();
     umma::tma_prefetch_desc(&w0);
     umma::tma_prefetch_desc(&w1);
@@ -516,7 +552,7 @@ __global__ void __launch_bounds__(kInfThreads, 1)
           for (int s = 0; ok && s < 2; ++s)
             for (int c = 0; c < layer_chunks(l); ++c, ++it) {
               const int st = (int)(it % kInfRing);
-              if (it >= (uint32_t)kInfRing && !umma::mbar_wait(empty(st), ((it / kInfRing) - 1) & 1, kWaitNs)) {
+              if (it >= (uint32_t)kInfRing && !umma::mbar_wait(empty(st), ((it / kInfRing) - 1) & 1, A.wait_ns)) {
                 atomicExch(A.err, kErrProducer);
                 ok = false;
                 break;
@@ -525,6 +561,9 @@ __global__ void __launch_bounds__(kInfThreads, 1)
               umma::tma_load_2d(ring0 + (uint32_t)st * kWChunk, maps[l], full(st), c * kBK, 0);
             }
         }
+      // the last load issued on each ring stage has landed before the CTA may exit
+      for (uint32_t i = it > (uint32_t)kInfRing ? it - kInfRing : 0u; i < it; ++i)
+        umma::mbar_wait(full((int)(i % kInfRing)), (i / kInfRing) & 1, kDrainNs);
     }
   } else if (warp == 1) {
     if (lane == 0) {  // MMA issuer
@@ -533,18 +572,18 @@ __global__ void __launch_bounds__(kInfThreads, 1)
       for (int64_t p = blockIdx.x; ok && p < A.pairs; p += gridDim.x)
         for (int l = 0; ok && l < BHS_LAYERS; ++l)
           for (int s = 0; ok && s < 2; ++s) {
-            if (!umma::mbar_wait(act_ready(s), ph[s], kWaitNs)) {
+            if (!umma::mbar_wait(act_ready(s), ph[s], A.wait_ns)) {
               atomicExch(A.err, kErrMma);
               ok = false;
               break;
             }
             ph[s] ^= 1u;
             umma::tc_fence_after();
-            const uint32_t idesc = umma::idesc_bf16_f32(kBM, l == BHS_LAYERS - 1 ? BHS_HEAD : BHS_HIDDEN);
+            const uint32_t idesc = umma::idesc_f16_f32(kBM, l == BHS_LAYERS - 1 ? BHS_HEAD : BHS_HIDDEN);
             const uint32_t d = tmem + (uint32_t)s * 256u;
             for (int c = 0; c < layer_chunks(l); ++c, ++it) {
               const int st = (int)(it % kInfRing);
-              if (!umma::mbar_wait(full(st), (it / kInfRing) & 1, kWaitNs)) {
+              if (!umma::mbar_wait(full(st), (it / kInfRing) & 1, A.wait_ns)) {
                 atomicExch(A.err, kErrMma);
                 ok = false;
                 break;
@@ -559,6 +598,9 @@ __global__ void __launch_bounds__(kInfThreads, 1)
             }
             umma::mma_commit(acc_full(s));
           }
+      // every MMA issued has completed (and stopped writing TMEM) before TMEM is freed
+      umma::mma_commit(drained);
+      umma::mbar_wait(drained, 0, kDrainNs);
     }
   } else {  // epilogue of slot s: TMEM lane quarter q (warp % 4), column half hf
     const int e = warp - 2;
@@ -584,15 +626,15 @@ __global__ void __launch_bounds__(kInfThreads, 1)
 #pragma unroll
           for (int uu = 0; uu < 4; ++uu) {
             const int u = 4 * d + uu;
-            st_unit(act + (uint32_t)(u >> 3) * kActChunk, r, u & 7, pack_bf16(z * v[8 * uu], z * v[8 * uu + 1]),
-                    pack_bf16(z * v[8 * uu + 2], z * v[8 * uu + 3]), pack_bf16(z * v[8 * uu + 4], z * v[8 * uu + 5]),
-                    pack_bf16(z * v[8 * uu + 6], z * v[8 * uu + 7]));
+            st_unit(act + (uint32_t)(u >> 3) * kActChunk, r, u & 7, pack_f16(z * v[8 * uu], z * v[8 * uu + 1]),
+                    pack_f16(z * v[8 * uu + 2], z * v[8 * uu + 3]), pack_f16(z * v[8 * uu + 4], z * v[8 * uu + 5]),
+                    pack_f16(z * v[8 * uu + 6], z * v[8 * uu + 7]));
           }
         }
         if (hf == 1) {
           // unit 16: columns 128..135 (scaled inputs, lambda, eta, two zeros); units 17..23: zero
-          st_unit(act + 2u * kActChunk, r, 0, pack_bf16(z * x[0], z * x[1]), pack_bf16(z * x[2], z * x[3]),
-                  pack_bf16(z * lam, z * eta), 0u);
+          st_unit(act + 2u * kActChunk, r, 0, pack_f16(z * x[0], z * x[1]), pack_f16(z * x[2], z * x[3]),
+                  pack_f16(z * lam, z * eta), 0u);
 #pragma unroll
           for (int u = 17; u < BHS_FEATURES / 8; ++u) st_unit(act + 2u * kActChunk, r, u & 7, 0u, 0u, 0u, 0u);
         }
@@ -601,7 +643,7 @@ __global__ void __launch_bounds__(kInfThreads, 1)
       umma::mbar_arrive(act_ready(s));
       bool ok = true;
       for (int l = 0; l < BHS_LAYERS - 1; ++l) {
-        ok = __all_sync(0xffffffffu, umma::mbar_wait(acc_full(s), ph, kWaitNs));
+        ok = __all_sync(0xffffffffu, umma::mbar_wait(acc_full(s), ph, A.wait_ns));
         ph ^= 1u;
         if (!ok) break;
         umma::tc_fence_after();
@@ -618,9 +660,9 @@ __global__ void __launch_bounds__(kInfThreads, 1)
             const int j = j0 + h;
             uint32_t pk[16];
 #pragma unroll
-            for (int i = 0; i < 16; ++i)
-              pk[i] = pack_bf16(silu(v[32 * h + 2 * i] + b[32 * j + 2 * i]),
-                                silu(v[32 * h + 2 * i + 1] + b[32 * j + 2 * i + 1]));
+            for (int i = 0; i < 16; ++i)  // b: halved biases, so hy = acc / 2 + b / 2
+              pk[i] = silu_f16x2(fmaf(v[32 * h + 2 * i], 0.5f, b[32 * j + 2 * i]),
+                                 fmaf(v[32 * h + 2 * i + 1], 0.5f, b[32 * j + 2 * i + 1]));
             const uint32_t cb = act + (uint32_t)(j >> 1) * kActChunk;
 #pragma unroll
             for (int uu = 0; uu < 4; ++uu)
@@ -631,7 +673,7 @@ __global__ void __launch_bounds__(kInfThreads, 1)
         umma::tc_fence_before();
         umma::mbar_arrive(act_ready(s));
       }
-      if (ok) ok = __all_sync(0xffffffffu, umma::mbar_wait(acc_full(s), ph, kWaitNs));
+      if (ok) ok = __all_sync(0xffffffffu, umma::mbar_wait(acc_full(s), ph, A.wait_ns));
       ph ^= 1u;
       if (!ok) {
         if (lane == 0) atomicExch(A.err, kErrDone);
@@ -754,6 +796,16 @@ __global__ void k_adam(float* __restrict__ w, const float* __restrict__ g, float
   }
 }
 
+// FP16 copies of the weights for inference, K-major [N][K] like the BF16 ones.
+__global__ void k_refresh_f16(const float* __restrict__ w, int64_t n, LayerTable t, MutPtr5 wh) {
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
+    int l = BHS_LAYERS - 1;
+    while (l > 0 && p < t.w_off[l]) --l;
+    const int64_t q = p - t.w_off[l];
+    if (q < (int64_t)t.n[l] * t.k[l]) static_cast<__half*>(wh.p[l])[q] = __float2half_rn(w[p]);
+  }
+}
+
 __global__ void k_refresh_bf16(const float* __restrict__ w, int64_t n, LayerTable t, MutPtr5 wb, MutPtr5 wt) {
   for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x)
     write_bf16_weight(t, wb, wt, p, w[p]);
@@ -826,8 +878,9 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
-// K-major BF16 matrix [rows][ld] (K valid columns), box {64, box_rows}, 128-byte swizzle.
-bool make_map(CUtensorMap* m, const void* base, int64_t rows, int K, int ld, int box_rows) {
+// K-major 16-bit matrix [rows][ld] (K valid columns), box {64, box_rows}, 128-byte swizzle.
+bool make_map(CUtensorMap* m, const void* base, int64_t rows, int K, int ld, int box_rows,
+              CUtensorMapDataType type = CU_TENSOR_MAP_DATA_TYPE_BFLOAT16) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) return false;
   if ((reinterpret_cast<uintptr_t>(base) & 15u) != 0 || (ld * 2) % 16 != 0) return false;
@@ -835,7 +888,7 @@ bool make_map(CUtensorMap* m, const void* base, int64_t rows, int K, int ld, int
   const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
   const cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)box_rows};
   const cuuint32_t es[2] = {1, 1};
-  return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, es,
+  return fn(m, type, 2, const_cast<void*>(base), dims, strides, box, es,
        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
@@ -859,7 +912,7 @@ int launch_tile(const BhsGemm* g, const Epi& epi, int* err, cudaStream_t st) {
   const int kcps = g->kchunks_per_split > 0 ? g->kchunks_per_split : total;
   const int splits = (total + kcps - 1) / kcps;
   const dim3 grid((unsigned)((g->M + kBM - 1) / kBM), (unsigned)(g->N / BN), (unsigned)splits);
-  k_gemm_bf16<BN, Epi><<<grid, 128, Cfg::kSmem, st>>>(ta, tb, g->K, kcps, epi, err);
+  k_gemm_bf16<BN, Epi><<<grid, 128, Cfg::kSmem, st>>>(ta, tb, g->K, kcps, epi, err, g->wait_ns);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
@@ -889,12 +942,13 @@ int blocks_for(int64_t n, int threads) { return (int)((n + threads - 1) / thread
 
 }  // namespace
 
-extern "C" int bhs_launch_infer(const __nv_bfloat16* const* wb, const float* host_bias, const float* inputs,
-                                int64_t n, float* head, int* d_err, cudaStream_t stream) {
+extern "C" int bhs_launch_infer(const __half* const* wh, const float* host_bias, const float* inputs,
+                                int64_t n, float* head, int* d_err, uint64_t wait_ns, cudaStream_t stream) {
   if (n <= 0) return 0;
   CUtensorMap m[BHS_LAYERS];
   for (int l = 0; l < BHS_LAYERS; ++l)
-    if (!make_map(&m[l], wb[l], bhs_layer_n(l), bhs_layer_k(l), bhs_layer_k(l), bhs_layer_n(l))) {
+    if (!make_map(&m[l], wh[l], bhs_layer_n(l), bhs_layer_k(l), bhs_layer_k(l), bhs_layer_n(l),
+                  CU_TENSOR_MAP_DATA_TYPE_FLOAT16)) {
       std::fprintf(stderr, "blackhole_b200: tensor map encoding failed\n");
       return -1;
     }
@@ -913,8 +967,9 @@ extern "C" int bhs_launch_infer(const __nv_bfloat16* const* wb, const float* hos
   a.n = n;
   const int64_t tiles = (n + kBM - 1) / kBM;
   a.pairs = (tiles + 1) / 2;
-  for (int i = 0; i < kBiasCount; ++i) a.bias[i] = host_bias[i];
+  for (int i = 0; i < kBiasCount; ++i) a.bias[i] = i < 4 * BHS_HIDDEN ? 0.5f * host_bias[i] : host_bias[i];
   a.err = d_err;
+  a.wait_ns = wait_ns;
   const int grid = (int)std::min<int64_t>(sms, a.pairs);
   k_mlp_infer<<<grid, kInfThreads, kInfSmem, stream>>>(m[0], m[1], m[2], m[3], m[4], a);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
@@ -986,6 +1041,13 @@ extern "C" int bhs_launch_refresh_bf16(const float* params, __nv_bfloat16* const
     t.p[l] = wt[l];
   }
   k_refresh_bf16<<<592, 256, 0, stream>>>(params, bhs_param_count(), make_table(), b, t);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+extern "C" int bhs_launch_refresh_f16(const float* params, __half* const* wh, cudaStream_t stream) {
+  MutPtr5 h{};
+  for (int l = 0; l < BHS_LAYERS; ++l) h.p[l] = wh[l];
+  k_refresh_f16<<<592, 256, 0, stream>>>(params, bhs_param_count(), make_table(), h);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

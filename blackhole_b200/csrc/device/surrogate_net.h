@@ -17,6 +17,7 @@
 
 #include <cstdint>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #define BHS_FEATURES 192
@@ -67,16 +68,21 @@ typedef struct BhsGemm {
   void* out_t;            // BF16 transposed copy [N][ld_t] (optional)
   float* y_out;           // HIDDEN: pre-activation (optional)
   int64_t ld_t;
+  uint64_t wait_ns;       // limit of each wait on another warp (>= 1)
 } BhsGemm;
 
 int bhs_launch_gemm(const BhsGemm* g, int* d_err, cudaStream_t stream);
 
 // Fused inference of n rows (features, 4 hidden layers, head) in one
-// persistent launch: head [n][16] = network(inputs [n][4]). host_bias: the
-// 4 x 256 hidden biases then the 16 head biases (host memory, copied into
-// the launch's parameters).
-int bhs_launch_infer(const __nv_bfloat16* const* wb, const float* host_bias, const float* inputs, int64_t n,
-                     float* head, int* d_err, cudaStream_t stream);
+// persistent launch: head [n][16] = network(inputs [n][4]), FP16 weights wh
+// (bhs_launch_refresh_f16) and activations, FP32 accumulation. host_bias:
+// the 4 x 256 hidden biases then the 16 head biases (host memory, copied
+// into the launch's parameters).
+int bhs_launch_infer(const __half* const* wh, const float* host_bias, const float* inputs, int64_t n,
+                     float* head, int* d_err, uint64_t wait_ns, cudaStream_t stream);
+
+// FP16 inference weights W_l [N][K] from the master parameters.
+int bhs_launch_refresh_f16(const float* params, __half* const* wh, cudaStream_t stream);
 
 // Features of n rays from inputs [n][4] = (alpha, beta, spin, cos theta_obs).
 int bhs_launch_features(const float* inputs, int64_t n, __nv_bfloat16* F, __nv_bfloat16* FT, int64_t ld_t,

@@ -10,12 +10,17 @@
 //   3. radial potential of a form not handled, or the
 //      exact solve does not converge                  -> integrator
 //   4. the exact solve disagrees with the network's
-//      class                                          -> integrator
+//      class (verify 1, 2; with verify 3 the solved
+//      class stands)                                  -> integrator
 // Accepted disk pixels get r_hit from the Mino-time solve seeded with the
 // network's radius (FP32 quadrature and elliptic integrals by default, all
 // FP64 on request), and g, flux and intensity from r_hit exactly as the
 // tracer computes them; escaped pixels get theta_inf from the exact polar
-// motion at the escape radius; phi_hit and phi_inf are the network's.
+// motion at the escape radius. When the caller asks for azimuths, phi_hit
+// and phi_inf are solved too: the radial part on the Mino-time quadrature's
+// own nodes, the polar part in closed form (R_J, cel), so no output of an
+// accepted pixel is the network's. Escaped rays whose polar motion stays on
+// one side of the equator go to the integrator.
 #include <cuda_runtime.h>
 
 #include "image_fp64.cuh"
@@ -36,7 +41,7 @@ __device__ __forceinline__ void warp_count(unsigned *stats, int slot, bool pred)
   if ((threadIdx.x & 31u) == 0 && m) atomicAdd(stats + slot, (unsigned)__popc(m));
 }
 
-template <bool FAST>
+template <bool FAST, bool PHI>
 __global__ void __launch_bounds__(128) k_surrogate_refine(const __grid_constant__ BhkImageParams p,
                                                           const __grid_constant__ BhkImageOut o,
                                                           const float *__restrict__ head, float min_conf,
@@ -69,7 +74,8 @@ __global__ void __launch_bounds__(128) k_surrogate_refine(const __grid_constant_
     if (!(conf >= min_conf)) {
       reason = 1;
     } else {
-      const bhmino::Radial q = bhmino::radial_motion(p.a2, p.a2 - a * lam, C, p.r_obs, p.r_plus, p.r_hor, p.r_esc);
+      bhmino::Radial q = bhmino::radial_motion(p.a2, p.a2 - a * lam, C, p.r_obs, p.r_plus, p.r_hor, p.r_esc);
+      if (PHI) bhmino::set_azimuth(q, a, lam);
       const double d = bhmino::critical_distance(q.r_min, q.R_min, a, lam, p.form == 1, p.sin_o, p.cos_o, alpha,
                                                  beta);
       if (q.kind < 0) {
@@ -78,52 +84,53 @@ __global__ void __launch_bounds__(128) k_surrogate_refine(const __grid_constant_
         reason = 2;
       } else {
         int cls = q.kind == 1 ? 2 : 0;  // radial kind: escapes or falls in
+        const bool search = nn_cls == 1 || verify >= 2;
+        bhmino::Polar th{};
+        if (search || cls == 2)
+          th = FAST ? bhmino::polar_motion<float>(p.a2, qTh, lam, p.cos_o, pu0, PHI)
+                    : bhmino::polar_motion<double>(p.a2, qTh, lam, p.cos_o, pu0, PHI);
         int nhit = 0;
-        double rh[3] = {0.0, 0.0, 0.0};
         bool solved = true;
         bhmino::Crossings c{};
         c.v_last = q.v_obs;
         c.t_last = 0.0;
-        if (nn_cls == 1 || verify >= 2) {
+        c.p_last = 0.0;
+        if (search) {
           const double r_seed = (double)__expf(h[3] + 2.0f);
-          c = bhmino::crossings<16, FAST>(q, p.a2, lam, qTh, p.r_in, p.r_out, p.cos_o, pu0, r_seed, p.max_cross,
-                                          kPanel<FAST>);
+          c = bhmino::crossings<FAST, PHI>(q, th, p.r_in, p.r_out, r_seed, p.max_cross, kPanel<FAST>);
           solved = c.status == 0;
           nhit = c.n_hits;
-          for (int k = 0; k < 3; ++k) rh[k] = c.r[k];
           if (nhit >= p.max_cross) cls = 1;
         }
         const int opaque_cls = nhit > 0 ? 1 : cls;
         if (!solved) {
           reason = 3;
-        } else if (verify >= 1 && opaque_cls != nn_cls) {
-          reason = 4;
+        } else if (verify <= 2 && opaque_cls != nn_cls) {
+          reason = 4;  // verify 3: the solved class stands
         } else if (nhit > 0 && cls == 2) {
-          reason = 4;  // passed the disk and escaped: the network has no escape direction for it
+          reason = 4;  // passed the disk and escaped: left to the integrator
+        } else if (cls == 2 && !th.crosses) {
+          reason = 3;  // polar motion on one side of the equator (vortical): left to the integrator
         } else {
           double th_inf = 0.0, ph_inf = 0.0;
           if (cls == 2) {
-            const bhmino::ThetaMotion tm = bhmino::theta_motion(p.a2, qTh, lam, p.cos_o, pu0);
-            if (tm.crosses) {
-              const double te = bhmino::tau_end<16, FAST>(q, c.v_last, c.t_last, kPanel<FAST>);
-              const double u = FAST ? bhmino::u_at<float>(p.a2, qTh, lam, p.cos_o, pu0, te)
-                                    : bhmino::u_at<double>(p.a2, qTh, lam, p.cos_o, pu0, te);
-              th_inf = acos(fmin(1.0, fmax(-1.0, u)));
-            } else {
-              th_inf = acos(fmin(1.0, fmax(-1.0, (double)h[10])));
-            }
-            ph_inf = (double)atan2f(h[12], h[11]);
+            const bhmino::TauPhi te = bhmino::tau_end<FAST, PHI>(q, c.v_last, c.t_last, c.p_last, kPanel<FAST>);
+            double phth = 0.0;
+            const double u = FAST ? bhmino::polar_at<float>(th, lam, te.t, PHI, phth)
+                                  : bhmino::polar_at<double>(th, lam, te.t, PHI, phth);
+            th_inf = acos(fmin(1.0, fmax(-1.0, u)));
+            if (PHI) ph_inf = -(te.ph + phth);
           }
           double inten = 0.0;
           for (int k = 0; k < p.max_cross; ++k) {
             const long long off = (long long)k * p.n_pix + pix;
             double r = 0.0, g = 0.0, ph = 0.0;
             if (k < nhit) {
-              r = rh[k];
+              r = c.r[k];
               g = bhk::disk_g(r, a, lam);
               const double qq = p.r_in / r;
               inten += g * g * g * g * qq * qq * qq;
-              ph = (double)((k == 0) ? atan2f(h[5], h[4]) : ((k == 1) ? atan2f(h[8], h[7]) : 0.0f));
+              if (PHI) ph = -(c.phr[k] + bhmino::phi_theta_crossing(th, lam, c.tau[k]));
             }
             if (o.r_hit) o.r_hit[off] = r;
             if (o.g) o.g[off] = g;
@@ -132,7 +139,7 @@ __global__ void __launch_bounds__(128) k_surrogate_refine(const __grid_constant_
           if (o.cls) o.cls[pix] = cls;
           if (o.steps) o.steps[pix] = 0;
           if (o.n_cross) o.n_cross[pix] = nhit;
-          if (o.flux) o.flux[pix] = nhit > 0 ? bhk::nt_flux(rh[0], p.nt_isco, p.nt_flux_peak) : 0.0;
+          if (o.flux) o.flux[pix] = nhit > 0 ? bhk::nt_flux(c.r[0], p.nt_isco, p.nt_flux_peak) : 0.0;
           if (o.intensity) o.intensity[pix] = inten;
           if (o.theta_inf) o.theta_inf[pix] = th_inf;
           if (o.phi_inf) o.phi_inf[pix] = ph_inf;
@@ -159,12 +166,22 @@ extern "C" int bhk_surrogate_refine(const BhkImageParams *p, const BhkImageOut *
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   p1 = p1 < p->n_pix ? p1 : p->n_pix;
   if (p1 <= p0) return 0;
-  const long long blocks = (p1 - p0 + 127) / 128;
-  if (refine_fp64)
-    k_surrogate_refine<false>
-        <<<(unsigned)blocks, 128, 0, s>>>(*p, *o, head, min_conf, band, verify, list, count, stats, p0, p1);
-  else
-    k_surrogate_refine<true>
-        <<<(unsigned)blocks, 128, 0, s>>>(*p, *o, head, min_conf, band, verify, list, count, stats, p0, p1);
+  const unsigned blocks = (unsigned)((p1 - p0 + 127) / 128);
+  const bool phi = o->phi_hit != nullptr || o->phi_inf != nullptr;
+  if (refine_fp64) {
+    if (phi)
+      k_surrogate_refine<false, true><<<blocks, 128, 0, s>>>(*p, *o, head, min_conf, band, verify, list, count,
+                                                             stats, p0, p1);
+    else
+      k_surrogate_refine<false, false><<<blocks, 128, 0, s>>>(*p, *o, head, min_conf, band, verify, list, count,
+                                                              stats, p0, p1);
+  } else {
+    if (phi)
+      k_surrogate_refine<true, true><<<blocks, 128, 0, s>>>(*p, *o, head, min_conf, band, verify, list, count,
+                                                            stats, p0, p1);
+    else
+      k_surrogate_refine<true, false><<<blocks, 128, 0, s>>>(*p, *o, head, min_conf, band, verify, list, count,
+                                                             stats, p0, p1);
+  }
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

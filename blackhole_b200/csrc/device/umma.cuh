@@ -1,6 +1,7 @@
 // Blackwell (sm_100a) tensor-core primitives in inline PTX: mbarriers, TMA
-// tile loads, TMEM allocation, tcgen05.mma (kind::f16, BF16 x BF16 -> FP32)
-// and tcgen05.ld. Used by the surrogate network's GEMM kernels.
+// tile loads, TMEM allocation, tcgen05.mma (kind::f16: BF16 x BF16 or
+// FP16 x FP16 -> FP32) and tcgen05.ld. Used by the surrogate network's GEMM
+// and inference kernels.
 //
 // Operand layout used throughout: K-major tiles of 64 BF16 (128 bytes) per
 // row, 128-byte swizzle, 8-row atoms of 1024 bytes -- exactly what a TMA
@@ -167,7 +168,13 @@ __host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N) {
       (static_cast<uint32_t>(M >> 4) << 24);
 }
 
-// D[tmem] (+)= A[smem] * B[smem]^T, M = 128, one K = 16 slice. Issued by one thread.
+// The same for A = B = FP16 (format 0 in bits [7,10) and [10,13)).
+__host__ __device__ constexpr uint32_t idesc_f16_f32(int M, int N) {
+  return (1u << 4) | (static_cast<uint32_t>(N >> 3) << 17) | (static_cast<uint32_t>(M >> 4) << 24);
+}
+
+// D[tmem] (+)= A[smem] * B[smem]^T, M = 128, one K = 16 slice (A and B both
+// BF16 or both FP16, as the instruction descriptor says). Issued by one thread.
 __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
                      uint32_t accumulate) {
   asm volatile(

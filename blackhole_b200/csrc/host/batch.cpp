@@ -17,6 +17,7 @@
 
 #include "../../../include/bh_kerr.h"
 #include "../device/launch.h"
+#include "dalloc.hpp"
 
 struct BH_KerrBatch {
   int device = -1;
@@ -146,7 +147,7 @@ BH_KerrBatch *bh_kerr_batch_create(const BH_KerrScene *scenes, const BH_KerrImag
   const size_t o_start = o_end + align256(sizeof(unsigned long long) * n);
   const size_t o_counter = o_start + 256;
   const size_t total = o_counter + 256;
-  if (cuda_check(cudaMalloc(&b->dev, total), "cudaMalloc(batch)")) return nullptr;
+  if (cuda_check(bhh_malloc(&b->dev, total), "cudaMalloc(batch)")) return nullptr;
   char *base = static_cast<char *>(b->dev);
   b->d.frames = reinterpret_cast<const BhkFrame *>(base + o_frames);
   b->d.prefix = reinterpret_cast<const long long *>(base + o_prefix);

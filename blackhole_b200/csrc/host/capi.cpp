@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -20,6 +21,7 @@
 #include "../../../include/bh_kerr.h"
 #include "../device/launch.h"
 #include "scene_math.hpp"
+#include "dalloc.hpp"
 
 namespace {
 
@@ -56,7 +58,7 @@ int device_scratch(DeviceScratch **out) {
   std::lock_guard<std::mutex> lk(g_scratch_mu);
   DeviceScratch &s = g_scratch[dev];
   if (!s.counter) {
-    e = cudaMalloc(reinterpret_cast<void **>(&s.counter), 256);
+    e = bhh_malloc((&s.counter), 256);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(work counter)");
     e = cudaDeviceGetAttribute(&s.sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute(SM count)");
@@ -212,6 +214,12 @@ int bhh_prepare_image_launch(const BH_KerrScene *scene, BhkImageParams *p, BhkLa
 // Records an error message from the device layer (noalloc.cu).
 int bhh_fail(const char *msg) { return fail("%s", msg); }
 
+// ---- device allocations -------------------------------------------------------
+namespace {
+std::atomic<int64_t> g_device_allocs{0};  // successful bhh_malloc calls
+std::atomic<int64_t> g_fail_in{0};        // > 0: the g_fail_in-th allocation from now fails
+}  // namespace
+
 // The current device's persistent-kernel work counter.
 int bhh_work_counter(unsigned long long **counter) {
   DeviceScratch *ds = nullptr;
@@ -235,7 +243,7 @@ static int launch_analytic(const BhkImageParams *p, const BhkImageOut *o, unsign
       if (ds->list) cudaFree(ds->list);
       ds->list = nullptr;
       ds->list_cap = 0;
-      e = cudaMalloc(reinterpret_cast<void **>(&ds->list), size_t(p->n_pix) * sizeof(int));
+      e = bhh_malloc((&ds->list), size_t(p->n_pix) * sizeof(int));
       if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(analytic fallback list)");
       ds->list_cap = p->n_pix;
     }
@@ -315,7 +323,7 @@ int ensure_host_buffers(size_t bytes) {
     if (g_hb.dev) cudaFree(g_hb.dev);
     g_hb.dev = nullptr;
     g_hb.bytes = 0;
-    e = cudaMalloc(&g_hb.dev, bytes);
+    e = bhh_malloc(&g_hb.dev, bytes);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(output buffers)");
     g_hb.bytes = bytes;
   }
@@ -357,13 +365,6 @@ int bh_kerr_trace_image_host(const BH_KerrScene *scene, const BH_KerrImageOut *h
   }
   cudaError_t e = cudaStreamSynchronize(g_hb.stream);
   if (e != cudaSuccess) return cuda_fail(e, "bh_kerr_trace_image_host");
-  return 0;
-}
-
-int bh_measure_fma_peak(int fp64, int repeats, double *tflops) {
-  if (!tflops) return fail("tflops is NULL");
-  if (repeats < 1) repeats = 1;
-  if (bhk_fma_probe(fp64, 1 << 14, repeats, tflops) != 0) return cuda_fail(cudaGetLastError(), "FMA probe");
   return 0;
 }
 
@@ -421,3 +422,21 @@ int bh_kerr_trace_rays(int64_t n, BH_KerrStateSoA s, BH_KerrConstsSoA c, const B
 }
 
 }  // extern "C"
+
+cudaError_t bhh_malloc(void **p, size_t bytes) {
+  int64_t k = g_fail_in.load();
+  while (k > 0 && !g_fail_in.compare_exchange_weak(k, k - 1)) {
+  }
+  if (k == 1) return cudaErrorMemoryAllocation;  // injected: as if the device were out of memory
+  const cudaError_t e = cudaMalloc(p, bytes);
+  if (e == cudaSuccess) g_device_allocs.fetch_add(1);
+  return e;
+}
+
+extern "C" int64_t bh_debug_device_allocations(void) { return g_device_allocs.load(); }
+
+extern "C" int bh_debug_fail_device_allocation(int64_t nth) {
+  if (nth < 0) return fail("bh_debug_fail_device_allocation: nth must be >= 0, got %lld", (long long)nth);
+  g_fail_in.store(nth);
+  return 0;
+}

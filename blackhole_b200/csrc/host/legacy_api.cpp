@@ -18,6 +18,7 @@
 #include "../../../include/bh_legacy.h"
 #include "../device/launch.h"
 #include "scene_math.hpp"
+#include "dalloc.hpp"
 
 namespace {
 
@@ -127,7 +128,7 @@ int scratch(int64_t n, Scratch **out) {
     s.cap = 0;
     const size_t b_cls = up256(size_t(n) * 4), b_d = up256(size_t(n) * 8), b_dir = up256(size_t(n) * 12);
     char *p = nullptr;
-    if (int rc = cuda_check(cudaMalloc(reinterpret_cast<void **>(&p), b_cls + 3 * b_d + b_dir + 256),
+    if (int rc = cuda_check(bhh_malloc((&p), b_cls + 3 * b_d + b_dir + 256),
                             "cudaMalloc(legacy scratch)"))
       return rc;
     s.base = p;
@@ -418,7 +419,7 @@ int postprocess_locked(float *fb, int w, int h, float threshold, float strength,
     if (sc->post) cudaFree(sc->post);
     sc->post = nullptr;
     sc->post_cap = 0;
-    if (int rc = cuda_check(cudaMalloc(reinterpret_cast<void **>(&sc->post), size_t(need) * 4),
+    if (int rc = cuda_check(bhh_malloc((&sc->post), size_t(need) * 4),
                             "cudaMalloc(postprocess scratch)"))
       return rc;
     sc->post_cap = need;
@@ -437,7 +438,7 @@ int render_to_host(const BH_LaunchParams *lp, float *out_rgba) {
   if (!(lp->width > 0 && lp->height > 0)) return fail_msg("bridge: image size %dx%d", lp->width, lp->height);
   const size_t bytes = size_t(lp->width) * size_t(lp->height) * 16;
   void *fb = nullptr;
-  if (int rc = cuda_check(cudaMalloc(&fb, bytes), "cudaMalloc(bridge framebuffer)")) return rc;
+  if (int rc = cuda_check(bhh_malloc(&fb, bytes), "cudaMalloc(bridge framebuffer)")) return rc;
   int rc = render(fb, lp, BH_KERNEL_FP32_BASELINE, nullptr);
   if (rc == 0) {
     std::lock_guard<std::mutex> lock(g_mu);
@@ -492,7 +493,7 @@ BH_CudaBackend *bhCudaInit(unsigned int /*gl_texture*/, int width, int height) {
   auto *b = new BhCudaBackend;
   if (cuda_check(cudaGetDevice(&b->device), "cudaGetDevice") ||
       cuda_check(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "cudaStreamCreate") ||
-      cuda_check(cudaMalloc(&b->fb, size_t(width) * size_t(height) * 16), "cudaMalloc(framebuffer)")) {
+      cuda_check(bhh_malloc(&b->fb, size_t(width) * size_t(height) * 16), "cudaMalloc(framebuffer)")) {
     bhCudaShutdown(b);
     return nullptr;
   }
@@ -518,7 +519,7 @@ int bhCudaResize(BH_CudaBackend *b, unsigned int /*gl_texture*/, int width, int 
   cudaFree(b->fb);
   b->fb = nullptr;
   b->width = b->height = 0;
-  if (int rc = cuda_check(cudaMalloc(&b->fb, size_t(width) * size_t(height) * 16), "cudaMalloc(framebuffer)"))
+  if (int rc = cuda_check(bhh_malloc(&b->fb, size_t(width) * size_t(height) * 16), "cudaMalloc(framebuffer)"))
     return rc;
   b->width = width;
   b->height = height;
@@ -642,7 +643,7 @@ int bhbCudaRenderLensingMap(double aStar, double observerRRg, double inclination
   o.g = sc->g;
   const size_t bytes = size_t(n) * 16;
   void *fb = nullptr;
-  if (int rc = cuda_check(cudaMalloc(&fb, bytes), "cudaMalloc(lensing map)")) return rc;
+  if (int rc = cuda_check(bhh_malloc(&fb, bytes), "cudaMalloc(lensing map)")) return rc;
   int rc = 0;
   if (bhk_trace_image_mixed(&p, &o, sc->counter, L, nullptr) != 0 ||
       bhk_legacy_lensing(n, sc->cls, sc->r_hit, sc->g, static_cast<float *>(fb), nullptr) != 0)
@@ -665,7 +666,7 @@ int bhbCudaRenderDiskTexture(const BhbDiskParams *params, int width, int height,
   std::lock_guard<std::mutex> lock(g_mu);
   Scratch *sc = nullptr;
   if (scratch(0, &sc) != 0) return -1;  // colour table
-  if (int rc = cuda_check(cudaMalloc(&fb, bytes), "cudaMalloc(disk texture)")) return rc;
+  if (int rc = cuda_check(bhh_malloc(&fb, bytes), "cudaMalloc(disk texture)")) return rc;
   int rc = 0;
   if (bhk_legacy_disk_texture(s.spin, k.r_in, params->rOutRg, k.nt_flux_peak, params->inclinationRad,
                               kDiskPeakTemperature, width, height, static_cast<float *>(fb), nullptr) != 0)
@@ -701,7 +702,7 @@ int bhbCudaTraceGeodesics(double aStar, double observerRRg, double inclinationRa
   const int64_t n = p.n_pix;
   const size_t b_xyz = size_t(n) * size_t(maxSteps) * 12, b_cnt = size_t(n) * 4;
   char *d = nullptr;
-  if (int rc = cuda_check(cudaMalloc(reinterpret_cast<void **>(&d), b_xyz + b_cnt + 256), "cudaMalloc(geodesic paths)"))
+  if (int rc = cuda_check(bhh_malloc((&d), b_xyz + b_cnt + 256), "cudaMalloc(geodesic paths)"))
     return rc;
   int32_t *cnt = reinterpret_cast<int32_t *>(d + ((b_xyz + 255) & ~size_t(255)));
   int rc = 0;

@@ -9,6 +9,7 @@
 #include "../../../include/bh_rt.h"
 #include "../device/launch.h"
 #include "../device/sky.cuh"
+#include "dalloc.hpp"
 
 namespace {
 
@@ -64,7 +65,7 @@ int bh_grmhd_synthetic(const BH_GrmhdGrid *g, const BH_TorusParams *t, void *str
     modes[4 * m + 3] = 6.283185307179586 * u.next();
   }
   double *d_modes = nullptr;
-  if (cudaMalloc(reinterpret_cast<void **>(&d_modes), modes.size() * sizeof(double)) != cudaSuccess)
+  if (bhh_malloc((&d_modes), modes.size() * sizeof(double)) != cudaSuccess)
     return bhh_fail("bh_grmhd_synthetic: cudaMalloc failed");
   cudaMemcpy(d_modes, modes.data(), modes.size() * sizeof(double), cudaMemcpyHostToDevice);
   const int rc = bhk_grmhd_fill(static_cast<float *>(const_cast<void *>(g->cells)), g->n_r, g->n_theta, g->n_phi,

@@ -10,6 +10,7 @@
 #include "../../../include/bh_kerr.h"
 #include "../device/launch.h"
 #include "../device/sky.cuh"
+#include "dalloc.hpp"
 
 namespace {
 
@@ -51,8 +52,8 @@ int bh_sky_generate(void* texels, int32_t size, int32_t n_stars, uint64_t seed, 
   float* d_val = nullptr;
   const int m = (int)idx.size();
   if (m > 0) {
-    if (cudaMalloc(reinterpret_cast<void**>(&d_idx), m * sizeof(long long)) != cudaSuccess ||
-        cudaMalloc(reinterpret_cast<void**>(&d_val), m * sizeof(float)) != cudaSuccess) {
+    if (bhh_malloc((&d_idx), m * sizeof(long long)) != cudaSuccess ||
+        bhh_malloc((&d_val), m * sizeof(float)) != cudaSuccess) {
       cudaFree(d_idx);
       return fail_msg("bh_sky_generate: cudaMalloc failed");
     }

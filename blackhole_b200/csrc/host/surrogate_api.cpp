@@ -18,11 +18,13 @@
 #include "../../../include/bh_surrogate.h"
 #include "../device/launch.h"
 #include "../device/surrogate_net.h"
+#include "dalloc.hpp"
 
 using bf16 = __nv_bfloat16;
 
 constexpr int kRenderChunks = 8;   // most chunks a render splits into
 constexpr int kDefaultChunks = 2;
+constexpr uint64_t kDefaultWaitNs = 2000000000ull;  // 2 s per bounded device wait
 
 struct BH_Surrogate {
   int device = -1;
@@ -32,6 +34,7 @@ struct BH_Surrogate {
   std::vector<void *> allocs;
   float *w = nullptr, *m = nullptr, *v = nullptr, *grad = nullptr;
   bf16 *wb[BHS_LAYERS] = {}, *wt[BHS_LAYERS] = {};
+  __half *wh[BHS_LAYERS] = {};  // FP16 inference copies, refreshed with the host biases
   // training activations, batch-major [B][.] and transposed [.][B]
   bf16 *F = nullptr, *FT = nullptr;
   bf16 *h[4] = {}, *ht[4] = {};
@@ -60,6 +63,8 @@ struct BH_Surrogate {
   // host copy of the biases for the fused inference launch
   std::vector<float> host_bias;
   bool bias_stale = true;
+  // limit of each bounded device wait on another warp's progress
+  uint64_t wait_ns = kDefaultWaitNs;
 };
 
 namespace {
@@ -84,7 +89,7 @@ int cuda_check(cudaError_t e, const char *what) {
 template <class T>
 int alloc(BH_Surrogate *s, T **p, size_t count, const char *what) {
   void *q = nullptr;
-  if (int rc = cuda_check(cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T)), what)) return rc;
+  if (int rc = cuda_check(bhh_malloc(&q, std::max<size_t>(count, 1) * sizeof(T)), what)) return rc;
   s->allocs.push_back(q);
   *p = static_cast<T *>(q);
   return 0;
@@ -126,7 +131,9 @@ int refresh(BH_Surrogate *s, cudaStream_t st) {
   return 0;
 }
 
-int gemm(BH_Surrogate *s, const BhsGemm &g, cudaStream_t st, const char *what) {
+int gemm(BH_Surrogate *s, const BhsGemm &g0, cudaStream_t st, const char *what) {
+  BhsGemm g = g0;
+  g.wait_ns = s->wait_ns;
   if (bhs_launch_gemm(&g, s->err, st) != 0)
     return fail_msg("surrogate: GEMM launch failed (%s: M=%lld N=%d K=%d)", what, static_cast<long long>(g.M), g.N,
                     g.K);
@@ -256,7 +263,8 @@ BH_Surrogate *bh_surrogate_create(int64_t max_batch, uint64_t seed) {
     return bad();
   for (int l = 0; l < BHS_LAYERS; ++l) {
     const size_t nk = static_cast<size_t>(bhs_layer_n(l)) * bhs_layer_k(l);
-    if (alloc(s, &s->wb[l], nk, "cudaMalloc(bf16 weights)")) return bad();
+    if (alloc(s, &s->wb[l], nk, "cudaMalloc(bf16 weights)") || alloc(s, &s->wh[l], nk, "cudaMalloc(f16 weights)"))
+      return bad();
     const size_t tsz = l == BHS_LAYERS - 1 ? static_cast<size_t>(BHS_HIDDEN) * BHS_HEAD_PAD : nk;
     if (alloc(s, &s->wt[l], tsz, "cudaMalloc(bf16 weights^T)")) return bad();
   }
@@ -312,6 +320,28 @@ int bh_surrogate_set_params(BH_Surrogate *s, const float *host, int64_t n) {
   return cuda_check(cudaDeviceSynchronize(), "set_params");
 }
 
+int bh_surrogate_get_state(const BH_Surrogate *s, float *m, float *v, int64_t n, int64_t *step) {
+  if (!s || !m || !v || !step || n != s->n_params)
+    return fail_msg("surrogate: get_state needs two arrays of %lld values and a step pointer",
+                    s ? static_cast<long long>(s->n_params) : 0LL);
+  const size_t b = static_cast<size_t>(n) * sizeof(float);
+  if (int rc = cuda_check(cudaMemcpy(m, s->m, b, cudaMemcpyDeviceToHost), "cudaMemcpy(adam m)")) return rc;
+  if (int rc = cuda_check(cudaMemcpy(v, s->v, b, cudaMemcpyDeviceToHost), "cudaMemcpy(adam v)")) return rc;
+  *step = s->step;
+  return 0;
+}
+
+int bh_surrogate_set_state(BH_Surrogate *s, const float *m, const float *v, int64_t n, int64_t step) {
+  if (!s || !m || !v || n != s->n_params || step < 0)
+    return fail_msg("surrogate: set_state needs two arrays of %lld values and step >= 0",
+                    s ? static_cast<long long>(s->n_params) : 0LL);
+  const size_t b = static_cast<size_t>(n) * sizeof(float);
+  if (int rc = cuda_check(cudaMemcpy(s->m, m, b, cudaMemcpyHostToDevice), "cudaMemcpy(adam m)")) return rc;
+  if (int rc = cuda_check(cudaMemcpy(s->v, v, b, cudaMemcpyHostToDevice), "cudaMemcpy(adam v)")) return rc;
+  s->step = step;
+  return 0;
+}
+
 int bh_surrogate_features(const float *inputs, int64_t n, void *features, void *stream) {
   if (n < 0 || (n > 0 && (!inputs || !features))) return fail_msg("surrogate: bad feature arguments");
   if (bhs_launch_features(inputs, n, static_cast<bf16 *>(features), nullptr, 0, static_cast<cudaStream_t>(stream)))
@@ -322,7 +352,9 @@ int bh_surrogate_features(const float *inputs, int64_t n, void *features, void *
 int bh_surrogate_forward(BH_Surrogate *s, const float *inputs, int64_t n, float *head, void *stream) {
   if (!s || n < 0 || (n > 0 && (!inputs || !head))) return fail_msg("surrogate: bad forward arguments");
   if (n == 0) return 0;
-  if (s->bias_stale) {  // after training steps: fetch the biases once (synchronous)
+  if (s->bias_stale) {  // after training steps: fetch the biases once (synchronous), refresh the FP16 weights
+    if (bhs_launch_refresh_f16(s->w, s->wh, static_cast<cudaStream_t>(stream)) != 0)
+      return fail_msg("surrogate: FP16 weight refresh launch failed");
     s->host_bias.resize(4 * BHS_HIDDEN + BHS_HEAD);
     for (int l = 0; l < BHS_LAYERS; ++l)
       if (int rc = cuda_check(cudaMemcpy(s->host_bias.data() + l * BHS_HIDDEN, s->w + bhs_bias_offset(l),
@@ -331,7 +363,8 @@ int bh_surrogate_forward(BH_Surrogate *s, const float *inputs, int64_t n, float 
         return rc;
     s->bias_stale = false;
   }
-  if (bhs_launch_infer(s->wb, s->host_bias.data(), inputs, n, head, s->err, static_cast<cudaStream_t>(stream)) != 0)
+  if (bhs_launch_infer(s->wh, s->host_bias.data(), inputs, n, head, s->err, s->wait_ns,
+                       static_cast<cudaStream_t>(stream)) != 0)
     return fail_msg("surrogate: fused inference launch failed");
   return 0;
 }
@@ -362,6 +395,12 @@ int bh_surrogate_train_step(BH_Surrogate *s, const float *inputs, const float *t
                       st) != 0)
     return fail_msg("surrogate: Adam launch failed");
   s->bias_stale = true;
+  return 0;
+}
+
+int bh_surrogate_set_wait_limit(BH_Surrogate *s, int64_t ns) {
+  if (!s || ns < 0) return fail_msg("surrogate: set_wait_limit needs a handle and ns >= 0");
+  s->wait_ns = ns == 0 ? kDefaultWaitNs : static_cast<uint64_t>(ns);
   return 0;
 }
 
@@ -416,9 +455,9 @@ int bh_surrogate_trace_image(BH_Surrogate *s, const BH_KerrScene *scene, const B
   BH_SurrogatePolicy pol;
   bh_surrogate_policy_defaults(&pol);
   if (policy) pol = *policy;
-  if (!(pol.min_confidence >= 0.0f && pol.min_confidence <= 1.0f) || pol.verify < 1 || pol.verify > 2 ||
+  if (!(pol.min_confidence >= 0.0f && pol.min_confidence <= 1.0f) || pol.verify < 1 || pol.verify > 3 ||
       !(pol.critical_band >= 0.0) || pol.chunks < 0 || pol.chunks > kRenderChunks)
-    return fail_msg("surrogate render: policy needs min_confidence in [0, 1], verify 1 or 2, critical_band >= 0, "
+    return fail_msg("surrogate render: policy needs min_confidence in [0, 1], verify 1, 2 or 3, critical_band >= 0, "
                     "chunks in [0, %d]", kRenderChunks);
   const int n_chunks = pol.chunks > 0 ? pol.chunks : kDefaultChunks;
   BH_KerrScene sc = *scene;
@@ -447,10 +486,8 @@ int bh_surrogate_trace_image(BH_Surrogate *s, const BH_KerrScene *scene, const B
     if (int rc = alloc(s, &s->r_list2, static_cast<size_t>(n), "cudaMalloc(second fallback list)")) return rc;
     s->ren_pixels = n;
   }
-  if (!s->r_counts) {
-    if (int rc = alloc(s, &s->r_counts, 8, "cudaMalloc(render counters)")) return rc;
-    if (int rc = alloc(s, &s->r_counter, 1, "cudaMalloc(work counter)")) return rc;
-  }
+  if (!s->r_counts && alloc(s, &s->r_counts, 8, "cudaMalloc(render counters)")) return -1;
+  if (!s->r_counter && alloc(s, &s->r_counter, 1, "cudaMalloc(work counter)")) return -1;
   auto st = static_cast<cudaStream_t>(stream);
   const double da = (sc.alpha_max - sc.alpha_min) / sc.width, db = (sc.beta_max - sc.beta_min) / sc.height;
   if (bhs_launch_grid_inputs(sc.spin, std::cos(sc.theta_obs), sc.alpha_min, da, sc.beta_min, db, sc.width, n,
@@ -541,7 +578,17 @@ int bh_surrogate_trace_image_host(BH_Surrogate *s, const BH_KerrScene *scene, co
       if (int rc = cuda_check(cudaMemcpyAsync(host[i], d[i], bytes[i], cudaMemcpyDeviceToHost, s->host_stream),
                               "cudaMemcpyAsync(D2H)"))
         return rc;
-  return cuda_check(cudaStreamSynchronize(s->host_stream), "bh_surrogate_trace_image_host");
+  if (int rc = cuda_check(cudaStreamSynchronize(s->host_stream), "bh_surrogate_trace_image_host")) return rc;
+  // a bounded wait of the network's kernels that ran out leaves its pixels undefined
+  int code = 0;
+  if (int rc = cuda_check(cudaMemcpy(&code, s->err, sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy(error flag)"))
+    return rc;
+  if (code) {
+    cudaMemset(s->err, 0, sizeof(int));
+    return fail_msg("bh_surrogate_trace_image_host: a bounded device wait of the network ran out (code %d); "
+                    "the outputs are not valid", code);
+  }
+  return 0;
 }
 
 int bh_surrogate_last_stats(BH_Surrogate *s, BH_SurrogateStats *out) {
@@ -566,11 +613,12 @@ int bh_bf16_gemm(const void *A, const void *B, int64_t M, int N, int K, float *C
   if (!(N == 16 || N == 192 || (N > 0 && N % 256 == 0))) return fail_msg("bf16 gemm: N must be 16, 192 or k*256");
   static int *err = nullptr;
   if (!err) {
-    if (int rc = cuda_check(cudaMalloc(&err, sizeof(int)), "cudaMalloc(error flag)")) return rc;
+    if (int rc = cuda_check(bhh_malloc(&err, sizeof(int)), "cudaMalloc(error flag)")) return rc;
     cudaMemset(err, 0, sizeof(int));
   }
   BhsGemm g = make_gemm(A, K, B, K, M, N, K, BHS_EPI_F32);
   g.out = C;
+  g.wait_ns = kDefaultWaitNs;
   if (bhs_launch_gemm(&g, err, static_cast<cudaStream_t>(stream)) != 0) return fail_msg("bf16 gemm: launch failed");
   return 0;
 }

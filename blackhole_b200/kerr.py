@@ -117,8 +117,8 @@ def trace_image(s: KerrScene, outs: dict[str, torch.Tensor] | None = None, strea
     return outs
 
 
-def trace_image_host(s: KerrScene, fields=None) -> dict[str, np.ndarray]:
-    """Trace into host (numpy) arrays through bh_kerr_trace_image_host."""
+def host_image_outputs(s: KerrScene, fields=None):
+    """Zeroed host (numpy) output arrays of a scene and their BH_KerrImageOut."""
     n = s.width * s.height
     mc = s.max_crossings
     dt = {"cls": np.int32, "steps": np.int32, "n_cross": np.int32}
@@ -127,7 +127,13 @@ def trace_image_host(s: KerrScene, fields=None) -> dict[str, np.ndarray]:
     for k in fields:
         shape = (mc, n) if k in _abi.PLANE_FIELDS else (n,)
         outs[k] = np.zeros(shape, dt.get(k, np.float64))
-    check(_abi.load_library().bh_kerr_trace_image_host(C.byref(s), C.byref(_out_struct(outs))))
+    return outs, _out_struct(outs)
+
+
+def trace_image_host(s: KerrScene, fields=None) -> dict[str, np.ndarray]:
+    """Trace into host (numpy) arrays through bh_kerr_trace_image_host."""
+    outs, o = host_image_outputs(s, fields)
+    check(_abi.load_library().bh_kerr_trace_image_host(C.byref(s), C.byref(o)))
     return outs
 
 

@@ -129,11 +129,54 @@ class Surrogate:
         assert p.size == self.n_params
         check(self._lib.bh_surrogate_set_params(self._h, p.ctypes.data, self.n_params))
 
-    def save(self, path):
-        np.savez_compressed(path, params=self.get_params())
+    def get_state(self):
+        """Adam moments (m, v) and step count."""
+        m = np.empty(self.n_params, np.float32)
+        v = np.empty(self.n_params, np.float32)
+        step = C.c_int64(0)
+        check(self._lib.bh_surrogate_get_state(self._h, m.ctypes.data, v.ctypes.data, self.n_params, C.byref(step)))
+        return m, v, int(step.value)
+
+    def set_state(self, m: np.ndarray, v: np.ndarray, step: int):
+        m = np.ascontiguousarray(m, np.float32)
+        v = np.ascontiguousarray(v, np.float32)
+        check(self._lib.bh_surrogate_set_state(self._h, m.ctypes.data, v.ctypes.data, self.n_params, int(step)))
+
+    def save(self, path, manifest: dict | None = None):
+        """Checkpoint: parameters and Adam state in ``path`` (.npz), and beside
+        it ``path`` + ``.json``, a manifest of what made it (``manifest``:
+        seed, training and data configuration; added here: the network's
+        shapes, the SHA-256 of the parameters, the data configuration's hash,
+        the git commit of the source tree when there is one)."""
+        import hashlib
+        import json
+        import subprocess
+        from pathlib import Path
+
+        params = self.get_params()
+        m, v, step = self.get_state()
+        np.savez_compressed(path, params=params, adam_m=m, adam_v=v, adam_step=np.int64(step))
+        man = dict(manifest or {})
+        man.update({
+            "format": "blackhole_b200 surrogate checkpoint 1",
+            "param_count": int(self.n_params), "layer_k": list(LAYER_K), "layer_n": list(LAYER_N),
+            "params_sha256": hashlib.sha256(params.tobytes()).hexdigest(), "adam_step": step,
+        })
+        if "data" in man:
+            man["data_hash"] = hashlib.sha256(json.dumps(man["data"], sort_keys=True).encode()).hexdigest()
+        try:
+            man["git_commit"] = subprocess.run(["git", "rev-parse", "HEAD"], capture_output=True, text=True,
+                                               cwd=Path(__file__).resolve().parent, check=True).stdout.strip()
+        except (OSError, subprocess.CalledProcessError):
+            man["git_commit"] = None
+        Path(str(path) + ".json").write_text(json.dumps(man, indent=1, sort_keys=True) + "\n")
 
     def load(self, path):
-        self.set_params(np.load(path)["params"])
+        """Parameters, and the Adam state when the checkpoint carries it."""
+        z = np.load(path)
+        self.set_params(z["params"])
+        if "adam_m" in z:
+            self.set_state(z["adam_m"], z["adam_v"], int(z["adam_step"]))
 
     def forward(self, inputs: torch.Tensor, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
         inputs = inputs.contiguous()
@@ -169,6 +212,21 @@ class Surrogate:
         check(self._lib.bh_surrogate_trace_image(self._h, C.byref(scene), C.byref(o), C.byref(pol),
                                                  _stream(stream)))
         return outs
+
+    def trace_image_host(self, scene, fields=None, min_confidence: float = 0.99, verify: int = 1,
+                         critical_band: float = 0.05, refine_fp64: bool = False, chunks: int = 0) -> dict:
+        """The same render into host (numpy) buffers through
+        bh_surrogate_trace_image_host; raises on -1 with the library's message."""
+        from .kerr import host_image_outputs
+
+        arrs, o = host_image_outputs(scene, fields)
+        pol = _abi.SurrogatePolicy(min_confidence, verify, critical_band, int(refine_fp64), int(chunks))
+        check(self._lib.bh_surrogate_trace_image_host(self._h, C.byref(scene), C.byref(o), C.byref(pol)))
+        return arrs
+
+    def set_wait_limit(self, ns: int) -> None:
+        """Limit of each bounded wait of the network's kernels (0: the default, 2 s)."""
+        check(self._lib.bh_surrogate_set_wait_limit(self._h, int(ns)))
 
     def last_stats(self) -> dict:
         st = _abi.SurrogateStats()

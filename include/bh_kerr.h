@@ -267,15 +267,18 @@ int bh_kerr_trace_image_host(const BH_KerrScene *scene, const BH_KerrImageOut *o
  * and the device copies of the outputs live in one fixed device array of
  * BH_NOALLOC_SCRATCH_BYTES. A call whose requested outputs (each rounded up
  * to 256 bytes) plus 256 bytes exceed that size is rejected with -1 and a
- * message; with every field and one disk crossing that is about 490,000
- * pixels (700 x 700).
+ * message; with BH_INTEGRATOR_ANALYTIC the list of pixels the closed form
+ * leaves to DP45 takes 4 more bytes per pixel (rounded up to 256). With
+ * every field and one disk crossing that allows about 490,000 pixels
+ * (700 x 700), 465,000 (680 x 680) with the closed form.
  *
  * stream: cudaStream_t to run on (NULL = legacy default stream); the call
  * returns after that stream has finished the copies. It creates no stream
  * and calls no cudaMalloc, cudaFree or allocating library routine.
- * The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress, which also loads the library's device code); make
- * that first call before any stream capture. Every call shares the array
+ * Every call looks up the array's device address on the current device
+ * (cudaGetSymbolAddress; it allocates nothing). The first call on a device
+ * also loads the library's device code there: make that first call before
+ * any stream capture. Every call shares the array
  * and overwrites the previous call's contents: calls whose GPU work overlaps
  * race and must be serialised by the caller.
  */
@@ -378,12 +381,23 @@ int bh_kerr_trace_image_sky(const BH_KerrScene *scene, const BH_KerrImageOut *ou
 /** Attach a sky to every frame of a batch (NULL detaches). */
 int bh_kerr_batch_set_sky(BH_KerrBatch *batch, const BH_SkyCubemap *sky);
 
+/* ---------------------------------------------------------------------------
+ * 5. Diagnostics of device allocation (no counterpart in the reference, whose
+ *    renderer reports a failed allocation only by returning -1 and asks its
+ *    caller to re-initialise, src/cuda/cuda_render_manager.h:155-199)
+ * ------------------------------------------------------------------------- */
+
+/** Device allocations (cudaMalloc) the library has made in this process. */
+int64_t bh_debug_device_allocations(void);
+
 /**
- * Measured FMA-pipe peak of the current device in TFLOP/s (fp64 != 0: FP64,
- * else FP32): best of `repeats` launches of independent FMA chains covering
- * every SM. The roofline figures of the tracer divide by this number.
+ * Make the library's nth device allocation from now fail as if the device
+ * were out of memory (nth = 1: the next one; 0: off). The entry point that
+ * makes it returns -1 with a message naming the allocation and leaves its
+ * cached buffers consistent, so the next call allocates afresh. For tests of
+ * the error paths; a process uses it from one thread at a time.
  */
-int bh_measure_fma_peak(int fp64, int repeats, double *tflops);
+int bh_debug_fail_device_allocation(int64_t nth);
 
 #ifdef __cplusplus
 }

@@ -56,6 +56,12 @@ void bh_surrogate_destroy(BH_Surrogate* s); /* NULL-safe */
 int bh_surrogate_get_params(const BH_Surrogate* s, float* host_params, int64_t n);
 int bh_surrogate_set_params(BH_Surrogate* s, const float* host_params, int64_t n);
 
+/* Adam state (first and second moments, bh_surrogate_param_count() values
+ * each, and the step count) for checkpoints; set_params resets it, so
+ * restore it after the parameters. */
+int bh_surrogate_get_state(const BH_Surrogate* s, float* adam_m, float* adam_v, int64_t n, int64_t* step);
+int bh_surrogate_set_state(BH_Surrogate* s, const float* adam_m, const float* adam_v, int64_t n, int64_t step);
+
 /* Input features (BF16 [n][192]) of n rows; diagnostic. */
 int bh_surrogate_features(const float* inputs, int64_t n, void* features_bf16, void* stream);
 
@@ -74,8 +80,17 @@ int bh_surrogate_train_step(BH_Surrogate* s, const float* inputs, const float* t
                             const BH_AdamConfig* adam, float* loss4, void* stream);
 
 /* Synchronise the device and return the first kernel error code recorded by
- * a bounded wait since the last call (0 = none). */
+ * a bounded wait since the last call (0 = none), then clear it. */
 int bh_surrogate_device_error(BH_Surrogate* s);
+
+/* Limit of each wait of the network's tensor-core kernels on another warp's
+ * progress (an mbarrier phase), in ns; 0 restores the default of 2 s. A wait
+ * that runs out records an error code (bh_surrogate_device_error), lets the
+ * work its own thread started finish, frees its tensor memory and returns,
+ * so the context stays usable. The reference has no counterpart; its
+ * renderer's contract on a failure is an error return after which the caller
+ * re-initialises (src/cuda/cuda_render_manager.h:155-199). */
+int bh_surrogate_set_wait_limit(BH_Surrogate* s, int64_t ns);
 
 /* Training targets from integrator outputs (device planes as written by
  * bh_kerr_trace_image with the given max_crossings). */
@@ -89,7 +104,11 @@ int bh_surrogate_grid_inputs(const BH_KerrScene* scene, float* inputs, void* str
 typedef struct BH_SurrogatePolicy {
     float min_confidence;  /* softmax class probability below this -> integrator (0.99) */
     int32_t verify;        /* 1: check the radial kind of captured/escaped predictions;
-                              2: run the exact crossing search on every pixel */
+                              2: run the exact crossing search on every pixel, and send a
+                                 pixel whose solved class contradicts the network's to the
+                                 integrator;
+                              3: as 2, but the solved class stands (the network only seeds
+                                 the Newton iteration of the solve) */
     double critical_band;  /* first-order image-plane distance to the critical curve, M,
                               below which a pixel goes to the integrator (0.05) */
     int32_t refine_fp64;   /* 0: Mino-time quadrature in FP32 (r_hit to ~4e-6); 1: all FP64 (~1e-8) */
@@ -110,16 +129,22 @@ void bh_surrogate_policy_defaults(BH_SurrogatePolicy* policy);
 
 /* Render a scene through the surrogate: network inference on every pixel,
  * exact Mino-time refinement of accepted disk hits (r_hit, g, flux,
- * intensity) and of escaped pixels' theta_inf, and the mixed-precision
- * integrator (the scene's integrator) on every pixel the policy rejects.
- * Outputs as bh_kerr_trace_image; for accepted pixels steps = 0 and phi_hit,
- * phi_inf are the network's. Asynchronous on `stream`; no host sync. */
+ * intensity, phi_hit) and of escaped pixels' theta_inf and phi_inf, and the
+ * closed-form tracer (DP45 at the scene's precision on the rays it does not
+ * cover) on every pixel the policy rejects. Outputs as bh_kerr_trace_image;
+ * for accepted pixels steps = 0. No output field is the network's own
+ * answer: it decides the class (checked per `verify`) and seeds the solve.
+ * The azimuths are solved only when out->phi_hit or out->phi_inf is given.
+ * Asynchronous on `stream`; no host sync. */
 int bh_surrogate_trace_image(BH_Surrogate* s, const BH_KerrScene* scene, const BH_KerrImageOut* out,
                              const BH_SurrogatePolicy* policy, void* stream);
 
 /* The same with HOST output buffers (BH_KerrImageOut of host pointers, NULL =
  * not wanted): grow-only device buffers owned by the network, one
- * device-to-host copy per requested field, returns when the copies are done. */
+ * device-to-host copy per requested field, returns when the copies are done.
+ * Returns -1 with a message when an allocation fails or when a bounded wait
+ * of the network's kernels ran out (the outputs are then not valid); the
+ * next call starts afresh. */
 int bh_surrogate_trace_image_host(BH_Surrogate* s, const BH_KerrScene* scene, const BH_KerrImageOut* out_host,
                                   const BH_SurrogatePolicy* policy);
 

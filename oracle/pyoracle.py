@@ -27,7 +27,9 @@ _vp, _i32, _i64, _f64 = C.c_void_p, C.c_int32, C.c_int64, C.c_double
 
 
 def build(quiet: bool = True) -> None:
-    """Run oracle/Makefile (builds _ref too when the reference sources exist)."""
+    """Run oracle/Makefile for the restatement (_build). The libraries of
+    oracle/_ref are built from the reference's sources by __graft_entry__.build()
+    (make REF_SRC=...) and only loaded here when present."""
     subprocess.run(["make", "-s", "-C", str(HERE)], check=True,
                    stdout=subprocess.DEVNULL if quiet else None)
 

@@ -11,7 +11,9 @@ differences of its own loss.
 ``emulate=True`` rounds to BF16 at the points where the GPU stores BF16:
 weights, features, hidden activations H, the loss gradient w.r.t. the head
 and the back-propagated dY; everything else is exact float64 (the GPU
-accumulates in FP32).
+accumulates in FP32). ``emulate="f16"`` rounds the same points of the
+forward pass to FP16 instead, as the fused inference kernel stores them
+(training runs in BF16; inference evaluates the trained network in FP16).
 """
 from __future__ import annotations
 
@@ -28,6 +30,11 @@ def bf16(x) -> np.ndarray:
     u = f.view(np.uint32).astype(np.uint64)
     u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
     return u.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def f16(x) -> np.ndarray:
+    """Round to the nearest FP16 (ties to even), returned as float64."""
+    return np.asarray(x, np.float64).astype(np.float16).astype(np.float64)
 
 
 def features(inputs: np.ndarray) -> np.ndarray:
@@ -74,7 +81,10 @@ def silu_grad(y):
 def forward(params, F, emulate=True):
     """Head outputs and the cache the backward pass needs."""
     Ws, bs = unpack(params)
-    r = bf16 if emulate else (lambda v: np.asarray(v, np.float64))
+    if emulate == "f16":
+        r = f16
+    else:
+        r = bf16 if emulate else (lambda v: np.asarray(v, np.float64))
     Wq = [r(W) for W in Ws]
     X = r(F)
     cache = {"X": [X], "Y": []}

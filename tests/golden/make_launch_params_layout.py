@@ -4,8 +4,8 @@ Compiles a small C program against the reference's own header
 (src/cuda/kernel_launch.h, a plain C header) with the host C compiler and
 writes sizeof and every field's offset to launch_params_layout.json, the
 fixture tests/test_legacy_layout.py checks include/bh_legacy.h against.
-Run from the repository root with the reference checked out at REF
-(default /root/reference):  python tests/golden/make_launch_params_layout.py
+Run from the repository root with the reference checkout given as REF:
+    REF=<reference checkout> python tests/golden/make_launch_params_layout.py
 """
 import json
 import os
@@ -15,7 +15,9 @@ import sys
 import tempfile
 from pathlib import Path
 
-REF = Path(os.environ.get("REF", "/root/reference"))
+if not os.environ.get("REF"):
+    sys.exit("set REF to the reference checkout (the directory holding src/cuda/kernel_launch.h)")
+REF = Path(os.environ["REF"])
 HERE = Path(__file__).resolve().parent
 
 

@@ -81,8 +81,11 @@ def _compare(got, ref, maxc, r_tol=1e-8, ang_tol=1e-8, inf_tol=1e-2, polar=None)
     return same
 
 
-@pytest.mark.parametrize("spin,incl,form", [(0.9, 60.0, 1), (0.5, 80.0, 0), (0.99, 17.0, 1), (0.0, 45.0, 1)])
+@pytest.mark.parametrize("spin,incl,form", [(0.9, 60.0, 1), (0.5, 80.0, 0), (0.99, 17.0, 1), (0.0, 45.0, 1),
+                                            (0.9, 120.0, 1), (0.5, 150.0, 0)])
 def test_analytic_matches_oracle(cuda, oracle, spin, incl, form):
+    """Observers above and below the equator (120 and 150 deg: the polar
+    motion starts at cos theta_obs < 0)."""
     s = _scene(spin=spin, incl=incl, form=form)
     got = _gpu(s)
     ref = oracle.trace_pixels(s)
@@ -105,6 +108,27 @@ def test_analytic_extreme_observers(cuda, oracle, spin, incl):
     alpha = s.alpha_min + (np.arange(37 * 19) % 37 + 0.5) * (s.alpha_max - s.alpha_min) / 37
     _compare(got, ref, 3, polar=np.abs(alpha) < 1e-9)
     assert (got["steps"] == 0).mean() > 0.95
+
+
+def test_analytic_pole_passing_rays(cuda, oracle):
+    """Columns at alpha = +-1e-5 (|lambda| ~ 9e-6): those rays pass the pole at
+    an angular distance the oracle's DP45 (rtol 1e-11) resolves, so it follows
+    the azimuth's turn by pi and phi is compared without any modulo-pi
+    relaxation. The column at alpha = +0 (lambda = -0) gets the limit of the
+    lambda < 0 side, a turn by copysign(pi, lambda) per pass over the pole:
+    the same outputs as the column at alpha = 1e-12 to 1e-9."""
+    for a0 in (1e-5, -1e-5):
+        s = _scene(width=1, height=48, alpha_min=a0 - 0.5, alpha_max=a0 + 0.5)
+        _compare(_gpu(s), oracle.trace_pixels(s), 3)
+    z = _gpu(_scene(width=1, height=48, alpha_min=-0.5, alpha_max=0.5))  # alpha = +0 exactly
+    e = _gpu(_scene(width=1, height=48, alpha_min=1e-12 - 0.5, alpha_max=1e-12 + 0.5))
+    np.testing.assert_array_equal(z["cls"], e["cls"])
+    np.testing.assert_array_equal(z["n_cross"], e["n_cross"])
+    assert (z["n_cross"] > 0).sum() >= 10 and (z["cls"] == 2).sum() >= 4
+    for f in ("r_hit", "phi_hit", "g"):
+        np.testing.assert_allclose(z[f], e[f], rtol=0, atol=1e-9, err_msg=f)
+    for f in ("theta_inf", "phi_inf"):
+        np.testing.assert_allclose(z[f], e[f], rtol=0, atol=1e-9, err_msg=f)
 
 
 def test_analytic_single_pixel_and_partial_outputs(cuda, oracle):

@@ -62,18 +62,28 @@ def test_noalloc_matches_allocating_entry_point_twice(cuda, lib, integrator, max
             np.testing.assert_array_equal(got[k], ref[k], err_msg=f"{k} (call {attempt + 1})")
 
 
-def test_noalloc_second_call_allocates_no_device_memory(cuda, lib):
+@pytest.mark.parametrize("integrator", [1, 2])
+def test_noalloc_calls_allocate_no_device_memory(cuda, lib, integrator):
+    """The library counts every device allocation it makes
+    (bh_debug_device_allocations): neither a first nor a second call of the
+    no-allocation entry point adds one, with a stepping or the closed-form
+    integrator (whose fallback list also lives in the fixed array). The
+    device's free memory, a secondary check that other processes can
+    disturb, stays the same across the second call."""
     import torch
 
     from blackhole_b200 import _abi
 
-    s = _abi.default_scene(width=80, height=72, integrator=1, max_crossings=2)
+    s = _abi.default_scene(width=80, height=72, integrator=integrator, max_crossings=2)
+    before = lib.bh_debug_device_allocations()
     call(lib, "bh_kerr_trace_image_host_noalloc", s, host_arrays(s), None)
+    assert lib.bh_debug_device_allocations() == before
     torch.cuda.synchronize()
     free_before, _ = torch.cuda.mem_get_info()
     got = call(lib, "bh_kerr_trace_image_host_noalloc", s, host_arrays(s), None)
     torch.cuda.synchronize()
     free_after, _ = torch.cuda.mem_get_info()
+    assert lib.bh_debug_device_allocations() == before
     assert free_after == free_before
     assert (got["cls"] >= 0).all()
 
