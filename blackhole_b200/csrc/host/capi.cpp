@@ -307,7 +307,7 @@ struct HostCallBuffers {
 };
 thread_local HostCallBuffers g_hb;
 
-int ensure_host_buffers(size_t bytes) {
+static int ensure_host_buffers(size_t bytes) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");

@@ -134,6 +134,26 @@ int bh_kerr_trace_rays(int64_t n, BH_KerrStateSoA initial, BH_KerrConstsSoA cons
                        double *out_theta, double *out_phi, double *out_redshift,
                        void *stream);
 
+/**
+ * The same three calls with HOST arrays (every pointer above in host memory,
+ * outputs NULL = not wanted): the library stages them through device buffers
+ * of the calling thread and returns when the results are back. These serve
+ * callers of the reference's scalar C++ API (include/bh_physics_compat.hpp)
+ * that hold their states in host memory.
+ */
+int bh_kerr_potentials_host(int64_t n, const double *r, const double *theta,
+                            double mass, double a, BH_KerrConstsSoA consts,
+                            double *out_r_pot, double *out_dr_pot,
+                            double *out_theta_pot, double *out_dtheta_pot);
+int bh_kerr_step_mino_host(int64_t n, BH_KerrStateSoA state, double mass, double a,
+                           BH_KerrConstsSoA consts, const double *dlam,
+                           double dlam_scalar);
+int bh_kerr_trace_rays_host(int64_t n, BH_KerrStateSoA initial, BH_KerrConstsSoA consts,
+                            const BH_KerrRaytracerParams *params,
+                            int32_t *out_status, int32_t *out_steps,
+                            double *out_total_distance, double *out_r,
+                            double *out_theta, double *out_phi, double *out_redshift);
+
 /* ---------------------------------------------------------------------------
  * 2. Image-plane tracer (geometric units G = c = M = 1)
  * ------------------------------------------------------------------------- */
