@@ -44,6 +44,10 @@ typedef struct BhkImageOut {
   // mixed tracer only: unit direction of motion of escaped rays, [3][n]
   // Cartesian (x, y, z) with x toward the observer's azimuth (zero if not escaped)
   float *esc_dir;
+  // mixed camera tracer only: the ray's closest approach to the hole, [3][n]:
+  // r [M], cos(theta) and phi (from the camera's azimuth) there; the camera's
+  // own position if the ray never came closer
+  float *closest;
 } BhkImageOut;
 
 typedef struct BhkLaunch {
@@ -199,6 +203,28 @@ typedef struct BhkShade {
   float cphi, sphi;      // camera azimuth (rotates escape directions into the world frame)
   unsigned long long tex_emissivity, tex_spectral, tex_galaxy, tex_equirect;
 } BhkShade;
+// The reference renderer's own look (legacy_look.cu): lengths in the
+// caller's world unit (m of them per M), textures as CUDA texture objects
+// (0 = not registered).
+typedef struct BhkLook {
+  int64_t n;
+  float m;                       // world units per M (rs / 2)
+  float rs, isco, spin;          // world units; spin a / M as the caller gave it
+  double r_esc;                  // escape radius [M]
+  float cam_pos[3], cam_right[3];
+  float cphi, sphi;              // camera azimuth: tracer frame -> world
+  int32_t redshift_enabled, use_luts, background_enabled, pad;
+  float adisk_lit, doppler_strength, bg_intensity, time_sec, glow_strength;
+  float bg_yaw, bg_pitch, bg_filter;
+  float bg_layers[12], bg_lod_bias[3];
+  float lut_r_min, lut_r_max, z_r_min, z_r_max, spec_r_min, spec_r_max;  // [rs]
+  float grmhd_r_min, grmhd_r_max, grmhd_alpha;
+  unsigned long long tex_emissivity, tex_redshift, tex_spectral, tex_galaxy, tex_grmhd, tex_grmhd_right,
+      tex_equirect;
+} BhkLook;
+int bhk_legacy_look(const BhkLook *L, const int32_t *cls, const double *r_hit, const double *phi_hit,
+                    const double *theta_inf, const double *phi_inf, const float *closest, float *rgba, void *stream);
+
 int bhk_legacy_set_blackbody(const float *rgb_table, int n, float log2_t0, float log2_t1);
 int bhk_legacy_shade(const BhkShade *s, const int32_t *cls, const double *r_hit, const double *g, const double *flux,
                      const float *esc_dir, float *rgba, void *stream);

@@ -46,6 +46,7 @@ struct RayMx {
   int steps;
   int attempts;
   int ncross;
+  float cl_r, cl_u, cl_psi;  // closest approach so far (camera rays only)
 };
 
 __device__ __forceinline__ void split(double v, float &hi, float &lo) {
@@ -267,6 +268,12 @@ __device__ __forceinline__ void finish(const BhkImageParams &p, const BhkImageOu
 // projection is idempotent on a projected state -- so accepted and rejected
 // lanes of a warp never diverge. k0 = rhs(y0); k1 = rhs(y1) when the caller
 // has it (DP45's FSAL stage), else NULL and evaluated only at a crossing.
+// TRACK: also keep the ray's closest approach (camera rays): the smallest r
+// of the step ends, and inside a step where p_r turns from negative to
+// positive the radial turning point, with p_r linear over the step: at the
+// fraction s = -p_r0 / (p_r1 - p_r0) of it, r = r0 + p_r0 s h / 2, u and psi
+// interpolated linearly.
+template <bool TRACK = false>
 __device__ __forceinline__ bool accept(const BhkImageParams &p, const BhkImageOut &o, RayMx &R, const Yf &d,
                                        bool acc, float h, const Yf &k0, const Yf *k1) {
   const Yf y0 = R.y;
@@ -277,6 +284,23 @@ __device__ __forceinline__ bool accept(const BhkImageParams &p, const BhkImageOu
   R.y.pr += acc ? d.pr : 0.0f;
   R.y.pu += acc ? d.pu : 0.0f;
   R.steps += acc ? 1 : 0;
+  if (TRACK && acc) {
+    const float r1 = R.y.r + R.lo.r;
+    if (r1 < R.cl_r) {
+      R.cl_r = r1;
+      R.cl_u = R.y.u;
+      R.cl_psi = R.y.phi;
+    }
+    if (y0.pr < 0.0f && R.y.pr >= 0.0f) {
+      const float s = -y0.pr / (R.y.pr - y0.pr);
+      const float r_tp = (y0.r + lo0.r) + 0.5f * y0.pr * s * h;
+      if (r_tp < R.cl_r) {
+        R.cl_r = r_tp;
+        R.cl_u = y0.u + s * (R.y.u - y0.u);
+        R.cl_psi = y0.phi + s * (R.y.phi - y0.phi);
+      }
+    }
+  }
   bool stop = false;
   if (acc && (y0.u + lo0.u) * (R.y.u + R.lo.u) < 0.0f) {
     const Yf kk = k1 ? *k1 : rhs(R.y, R.c);
@@ -294,7 +318,7 @@ __device__ __forceinline__ bool accept(const BhkImageParams &p, const BhkImageOu
   return stop;
 }
 
-template <int INTEG>
+template <int INTEG, bool TRACK = false>
 __device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOut &o, RayMx &R) {
   const float r_hor = R.r_hor, r_esc = R.r_esc;
   if (INTEG == 0) {
@@ -305,7 +329,7 @@ __device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOu
     const float h = __fdividef(hh, fmaf(R.c.a2 * R.y.u, R.y.u, R.y.r * R.y.r));
     const Yf k0 = rhs(R.y, R.c);
     const Yf d = rk4_inc(R.y, h, R.c, k0);
-    return accept(p, o, R, d, true, h, k0, nullptr) ? 1 : -1;
+    return accept<TRACK>(p, o, R, d, true, h, k0, nullptr) ? 1 : -1;
   } else {
     const long long max_attempts = 4LL * p.max_steps + 64;
     if (R.steps >= p.max_steps || R.attempts >= max_attempts) return 3;
@@ -315,7 +339,7 @@ __device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOu
     const DPf d = dp45(R.y, R.h, R.c, R.k1, R.rtol, R.atol, true);
     const bool acc = d.err <= 1.0f;
     const float h = R.h;
-    const bool stop = accept(p, o, R, d.d, acc, h, R.k1, &d.k7);
+    const bool stop = accept<TRACK>(p, o, R, d.d, acc, h, R.k1, &d.k7);
     R.k1 = acc ? d.k7 : R.k1;
     R.k1.r = R.y.pr;  // projection moved only the momenta
     R.k1.u = R.y.pu;
@@ -339,6 +363,24 @@ struct CameraSrc {
   __device__ __forceinline__ void pixel_done(int) const {}
 };
 
+// Sources whose rays keep their closest approach (for the reference look of
+// the render launch ABI): the camera's.
+template <class Src>
+struct tracks_closest {
+  static constexpr bool value = false;
+};
+template <>
+struct tracks_closest<CameraSrc> {
+  static constexpr bool value = true;
+};
+
+__device__ __forceinline__ void write_closest(const BhkImageParams &p, const BhkImageOut &o, const RayMx &R) {
+  if (!o.closest) return;
+  o.closest[R.pix] = R.cl_r;
+  o.closest[p.n_pix + R.pix] = R.cl_u;
+  o.closest[2 * p.n_pix + R.pix] = (float)phi_of_psi((double)R.cl_psi, (double)R.cl_r, p);
+}
+
 // A ray's initial state: image-plane pixels for every source but the camera.
 template <class Src>
 __device__ __forceinline__ void init_from(const Src &src, int f, long long pix, RayMx &R) {
@@ -346,6 +388,9 @@ __device__ __forceinline__ void init_from(const Src &src, int f, long long pix, 
 }
 __device__ __forceinline__ void init_from(const CameraSrc &src, int, long long pix, RayMx &R) {
   init_ray_camera(src.p, src.cam, pix, R);
+  R.cl_r = R.y.r + R.lo.r;
+  R.cl_u = R.y.u;
+  R.cl_psi = 0.0f;
 }
 
 // The persistent loop shared by the single-frame and batch kernels (see
@@ -382,8 +427,9 @@ __device__ __forceinline__ void trace_loop(const Src &src, unsigned long long *_
     for (int k = 0; k < refill; ++k) {
       if (active) {
         const BhkImageParams &P = src.params(R.f);
-        const int cls = iterate<INTEG>(P, src.out(R.f), R);
+        const int cls = iterate<INTEG, tracks_closest<Src>::value>(P, src.out(R.f), R);
         if (cls >= 0) {
+          if (tracks_closest<Src>::value) write_closest(P, src.out(R.f), R);
           finish(P, src.out(R.f), R, cls);
           src.pixel_done(R.f);
           active = false;

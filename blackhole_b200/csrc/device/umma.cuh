@@ -56,8 +56,30 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
   return ok != 0;
 }
 
+// Non-blocking test of the same phase (returns at once).
+__device__ __forceinline__ bool mbar_test_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+    "{\n\t.reg .pred p;\n\t"
+    "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+    "selp.u32 %0, 1, 0, p;\n\t}"
+    : "=r"(ok)
+    : "r"(bar), "r"(parity)
+    : "memory");
+  return ok != 0;
+}
+
 // Wait for the phase with the given parity to complete; false after limit_ns.
+// try_wait may suspend the thread for a while by itself, so a limit below a
+// microsecond polls with test_wait and reads the clock after every test.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, uint64_t limit_ns) {
+  if (limit_ns < 1000) {
+    const uint64_t t0 = globaltimer();
+    for (;;) {
+      if (mbar_test_wait(bar, parity)) return true;
+      if (globaltimer() - t0 > limit_ns) return false;
+    }
+  }
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = globaltimer();
   for (;;) {

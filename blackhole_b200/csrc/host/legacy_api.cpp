@@ -98,7 +98,9 @@ struct Scratch {
   int64_t cap = 0;
   int32_t *cls = nullptr;
   double *r_hit = nullptr, *g = nullptr, *flux = nullptr;
+  double *phi_hit = nullptr, *theta_inf = nullptr, *phi_inf = nullptr;
   float *esc_dir = nullptr;
+  float *closest = nullptr;
   unsigned long long *counter = nullptr;
   float *post = nullptr;  // bloom planes and composite of bhb_cuda_postprocess
   int64_t post_cap = 0;
@@ -128,20 +130,38 @@ int scratch(int64_t n, Scratch **out) {
     s.cap = 0;
     const size_t b_cls = up256(size_t(n) * 4), b_d = up256(size_t(n) * 8), b_dir = up256(size_t(n) * 12);
     char *p = nullptr;
-    if (int rc = cuda_check(bhh_malloc((&p), b_cls + 3 * b_d + b_dir + 256),
+    if (int rc = cuda_check(bhh_malloc((&p), b_cls + 6 * b_d + 2 * b_dir + 256),
                             "cudaMalloc(legacy scratch)"))
       return rc;
     s.base = p;
     s.cls = reinterpret_cast<int32_t *>(p);
-    s.r_hit = reinterpret_cast<double *>(p + b_cls);
-    s.g = reinterpret_cast<double *>(p + b_cls + b_d);
-    s.flux = reinterpret_cast<double *>(p + b_cls + 2 * b_d);
-    s.esc_dir = reinterpret_cast<float *>(p + b_cls + 3 * b_d);
-    s.counter = reinterpret_cast<unsigned long long *>(p + b_cls + 3 * b_d + b_dir);
+    double *d = reinterpret_cast<double *>(p + b_cls);
+    const size_t nd = b_d / 8;
+    s.r_hit = d;
+    s.g = d + nd;
+    s.flux = d + 2 * nd;
+    s.phi_hit = d + 3 * nd;
+    s.theta_inf = d + 4 * nd;
+    s.phi_inf = d + 5 * nd;
+    s.esc_dir = reinterpret_cast<float *>(p + b_cls + 6 * b_d);
+    s.closest = reinterpret_cast<float *>(p + b_cls + 6 * b_d + b_dir);
+    s.counter = reinterpret_cast<unsigned long long *>(p + b_cls + 6 * b_d + 2 * b_dir);
     s.cap = n;
   }
   *out = &s;
   return 0;
+}
+
+// ---- shading: the reference's look (default) or physical -----------------------
+
+int g_shading = -1;  // BH_SHADING_*, -1 until first read from BLACKHOLE_SHADING
+
+int shading_mode() {
+  if (g_shading < 0) {
+    const char *v = std::getenv("BLACKHOLE_SHADING");
+    g_shading = (v && std::strcmp(v, "physical") == 0) ? BH_SHADING_PHYSICAL : BH_SHADING_REFERENCE;
+  }
+  return g_shading;
 }
 
 // ---- BH_LaunchParams -> camera and tracer parameters --------------------------
@@ -233,14 +253,70 @@ int render(void *fb, const BH_LaunchParams *lp, int variant, cudaStream_t st) {
   if (scratch(n, &sc) != 0) return -1;
   BhkLaunch L;
   if (launch_shape(*sc, n, &L) != 0) return -1;
+  const bool look = shading_mode() == BH_SHADING_REFERENCE;
   BhkImageOut o{};
   o.cls = sc->cls;
   o.r_hit = sc->r_hit;
-  o.g = sc->g;
-  o.flux = sc->flux;
-  o.esc_dir = sc->esc_dir;
+  if (look) {
+    o.phi_hit = sc->phi_hit;
+    o.theta_inf = sc->theta_inf;
+    o.phi_inf = sc->phi_inf;
+    o.closest = sc->closest;
+  } else {
+    o.g = sc->g;
+    o.flux = sc->flux;
+    o.esc_dir = sc->esc_dir;
+  }
   if (bhk_trace_camera_mixed(&job.p, &job.cam, &o, sc->counter, L, st) != 0)
     return cuda_check(cudaGetLastError(), "k_trace_camera_mixed launch");
+  if (look) {
+    BhkLook lk{};
+    lk.n = n;
+    lk.m = 0.5f * lp->rs;
+    lk.rs = lp->rs;
+    lk.isco = lp->isco;
+    lk.spin = lp->spin;
+    lk.r_esc = job.p.r_esc;
+    for (int k = 0; k < 3; ++k) {
+      lk.cam_pos[k] = lp->cam_pos[k];
+      lk.cam_right[k] = lp->cam_basis[k];
+    }
+    lk.cphi = float(job.cam.cphi);
+    lk.sphi = float(job.cam.sphi);
+    lk.redshift_enabled = lp->redshift_enabled;
+    lk.use_luts = lp->use_luts;
+    lk.background_enabled = lp->background_enabled;
+    lk.adisk_lit = lp->adisk_lit;
+    lk.doppler_strength = lp->doppler_strength;
+    lk.bg_intensity = lp->background_intensity;
+    lk.time_sec = lp->time_sec;
+    lk.glow_strength = lp->photon_glow_strength;
+    lk.bg_yaw = lp->background_yaw_rad;
+    lk.bg_pitch = lp->background_pitch_rad;
+    lk.bg_filter = lp->background_filter_radius;
+    for (int k = 0; k < 12; ++k) lk.bg_layers[k] = lp->background_layer_params[k];
+    for (int k = 0; k < 3; ++k) lk.bg_lod_bias[k] = lp->background_layer_lod_bias[k];
+    lk.lut_r_min = lp->lut_radius_min;
+    lk.lut_r_max = lp->lut_radius_max;
+    lk.z_r_min = lp->redshift_radius_min;
+    lk.z_r_max = lp->redshift_radius_max;
+    lk.spec_r_min = lp->spectral_radius_min;
+    lk.spec_r_max = lp->spectral_radius_max;
+    lk.grmhd_r_min = lp->grmhd_r_min;
+    lk.grmhd_r_max = lp->grmhd_r_max;
+    lk.grmhd_alpha = lp->grmhd_alpha;
+    lk.tex_emissivity = g_lut[0];
+    lk.tex_redshift = g_lut[1];
+    lk.tex_spectral = g_lut[2];
+    lk.tex_galaxy = g_lut[4];
+    lk.tex_grmhd = g_lut[5];
+    lk.tex_grmhd_right = g_lut[7];
+    lk.tex_equirect = g_equirect;
+    if (bhk_legacy_look(&lk, sc->cls, sc->r_hit, sc->phi_hit, sc->theta_inf, sc->phi_inf, sc->closest,
+                        static_cast<float *>(fb), st) != 0)
+      return cuda_check(cudaGetLastError(), "k_legacy_look launch");
+    return 0;
+  }
   BhkShade sh{};
   sh.n = n;
   sh.width = lp->width;
@@ -461,6 +537,20 @@ int bh_launch_geodesic_kernel(void *framebuffer, const BH_LaunchParams *params, 
 }
 
 int bh_select_kernel_variant(void) { return BH_KERNEL_FP32_BASELINE; }
+
+int bh_legacy_set_shading(int mode) {
+  if (mode != BH_SHADING_REFERENCE && mode != BH_SHADING_PHYSICAL)
+    return fail_msg("bh_legacy_set_shading: mode must be BH_SHADING_REFERENCE (0) or BH_SHADING_PHYSICAL (1), got %d",
+                    mode);
+  std::lock_guard<std::mutex> lock(g_mu);
+  g_shading = mode;
+  return 0;
+}
+
+int bh_legacy_get_shading(void) {
+  std::lock_guard<std::mutex> lock(g_mu);
+  return shading_mode();
+}
 
 void bh_upload_lut_textures(unsigned long long emissivity, unsigned long long redshift, unsigned long long spectral,
                             unsigned long long grb, unsigned long long galaxy, unsigned long long grmhd,

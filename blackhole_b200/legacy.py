@@ -143,12 +143,27 @@ def _declare(lib: C.CDLL) -> C.CDLL:
     lib.bhb_cuda_render_lensing_map.argtypes = [f, f, f, i, i, vp]
     lib.bhb_cuda_render_disk_texture.argtypes = [f, f, f, i, i, vp]
     lib.bhb_cuda_postprocess.argtypes = [vp, i, i, f, f, f, f]
+    lib.bh_legacy_set_shading.argtypes = [i]
+    lib.bh_legacy_get_shading.argtypes = []
     lib._legacy_declared = True
     return lib
 
 
 def library() -> C.CDLL:
     return _declare(load_library())
+
+
+SHADING_REFERENCE, SHADING_PHYSICAL = 0, 1
+
+
+def set_shading(mode: int) -> None:
+    """Colour of the render calls: SHADING_REFERENCE (the reference shader's
+    look, the default) or SHADING_PHYSICAL (bh_legacy_set_shading)."""
+    check(library().bh_legacy_set_shading(int(mode)))
+
+
+def get_shading() -> int:
+    return int(library().bh_legacy_get_shading())
 
 
 def launch(params: LaunchParams, framebuffer, variant: int = -1, stream=None) -> None:

@@ -16,12 +16,20 @@
  * compiled against the reference header passes the same bytes. What happens
  * behind the calls is this library's: every pixel's ray is a Kerr null
  * geodesic traced by the mixed-precision DP45 tracer of bh_kerr.h (FP32 bulk,
- * FP64 set-up), the disk colour is the observed blackbody of a Novikov-Thorne
- * disk (exact Keplerian redshift g), and the background is the caller's
- * texture looked up in the ray's escape direction. The fields of the
- * reference's art-directed look (glow, wiregrid, sector shaping, layered
- * background, debug exports, Stokes and volumetric modes) are accepted and
- * ignored; the calls that need an OpenGL texture return -1 (no graphics stack).
+ * FP64 set-up). Two ways to colour it (bh_legacy_set_shading):
+ *   BH_SHADING_REFERENCE (the default): the reference shader's own look
+ *     (src/cuda/device_physics.cuh, d_shade_hit and what it calls) -- colour
+ *     ramp, tints, Doppler beaming, sector shaping, static-observer redshift,
+ *     procedural stars or the caller's textures, escaped-sky shaping and
+ *     photon-ring glow -- evaluated on this tracer's hit points, closest
+ *     approaches and escape positions, so existing callers get the picture
+ *     they were tuned for;
+ *   BH_SHADING_PHYSICAL: the observed blackbody of a Novikov-Thorne disk
+ *     (exact Keplerian redshift g) and the caller's texture in the ray's
+ *     escape direction.
+ * Still accepted and ignored in both: wiregrid, debug exports, Stokes and
+ * volumetric (RTE) modes. The calls that need an OpenGL texture return -1 (no
+ * graphics stack).
  *
  * Conventions: 0 on success, -1 on error with the message in bh_last_error()
  * (bh_kerr.h). World coordinates are those of the reference renderer: lengths
@@ -73,7 +81,7 @@ struct BH_LaunchParams {
     float spectral_radius_max;
 
     float time_sec;
-    float doppler_strength;     /* accepted; g is exact */
+    float doppler_strength;     /* reference look: strength of its Doppler approximation */
     float background_intensity; /* background texture multiplier */
     int background_enabled;
     float photon_glow_strength;
@@ -127,6 +135,14 @@ enum BH_KernelVariant {
  * the per-pixel scratch (grow-only, kept until bhbCudaResetDevice or exit).
  * Replaces bh_launch_geodesic_kernel, src/cuda/kernel_launch.h:143-146. */
 int bh_launch_geodesic_kernel(void *framebuffer, const struct BH_LaunchParams *params, int variant, void *stream);
+
+/* Shading of the render calls (no counterpart in the reference, whose look is
+ * fixed): BH_SHADING_REFERENCE (0, default) or BH_SHADING_PHYSICAL (1); the
+ * default can also be set by BLACKHOLE_SHADING=physical in the environment,
+ * read on the first render. Process-wide; returns -1 on an unknown mode. */
+enum BH_Shading { BH_SHADING_REFERENCE = 0, BH_SHADING_PHYSICAL = 1 };
+int bh_legacy_set_shading(int mode);
+int bh_legacy_get_shading(void);
 
 /* BH_KERNEL_FP32_BASELINE (kernel_launch.h:156). */
 int bh_select_kernel_variant(void);

@@ -24,10 +24,15 @@ pytestmark = pytest.mark.gpu
 
 @pytest.fixture(scope="module")
 def leg():
+    """The bindings, with the physical shading these tests pin (the reference
+    look, the default, is pinned in test_gpu_legacy_look.py)."""
     from blackhole_b200 import legacy
 
     legacy.library()
-    return legacy
+    before = legacy.get_shading()
+    legacy.set_shading(legacy.SHADING_PHYSICAL)
+    yield legacy
+    legacy.set_shading(before)
 
 
 def _render(leg, p, variant=-1):
