@@ -93,6 +93,28 @@ SURROGATE_MMA_FLOPS_PER_RAY = 2.0 * (192 * 256 + 3 * 256 * 256 + 256 * 16)
 OUT_FIELDS_USED = ("cls", "steps", "n_cross", "r_hit", "phi_hit", "g", "flux", "intensity", "theta_inf", "phi_inf")
 
 
+CARTER_DRIFT_DEF = ("largest relative residual |eta(state) - eta| / (|q_Th| + a^2) that the tracer's projection "
+                    "removed from a ray (BH_KerrImageOut.carter_drift), over the frame; 0 for solved pixels")
+
+
+def carter_drift_stats(trace, n: int, device) -> dict:
+    """Carter-constant drift of one untimed render: ``trace(outs)`` writes the
+    frame's steps and carter_drift into ``outs``."""
+    import torch
+
+    outs = {"steps": torch.empty(n, dtype=torch.int32, device=device),
+            "carter_drift": torch.empty(n, dtype=torch.float64, device=device)}
+    trace(outs)
+    torch.cuda.synchronize(device)
+    d = outs["carter_drift"]
+    stepped = outs["steps"] > 0
+    ds = d[stepped]
+    return {"max": float(d.max().item()),
+            "median_stepped": float(ds.median().item()) if ds.numel() else 0.0,
+            "p99_stepped": float(torch.quantile(ds[:1 << 24].float(), 0.99).item()) if ds.numel() else 0.0,
+            "stepped_pixels": int(stepped.sum().item())}
+
+
 def fma_probe():
     """The bench's FMA-pipe peak probe (blackhole_b200/lib/libbh_bench_probe.so,
     built beside the tracer library but not part of it)."""
@@ -335,7 +357,7 @@ def accuracy(ref_outs, test_outs, reference: str = "this run's FP64 path (bit-id
 def run_ours(args, rank: int, world: int, dist):
     import torch
 
-    from blackhole_b200 import _abi
+    from blackhole_b200 import _abi, kerr
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
@@ -362,6 +384,14 @@ def run_ours(args, rank: int, world: int, dist):
                                "steps_per_render": f["total_steps"], "clocks": f["clocks"]}
         extra["speedup_vs_fp64_plain"] = value / extra["fp64_plain"]["value"]
         extra["accuracy_vs_fp64"] = accuracy(f["outs"], head["outs"])
+
+    drift = {"definition": CARTER_DRIFT_DEF}
+    for p, r in runs.items():
+        s0 = r["scenes"][0]
+        drift[p] = carter_drift_stats(lambda o, s0=s0: kerr.trace_image(s0, o, stream=stream),
+                                      s0.width * s0.height, dev)
+        drift[p]["frame"] = f"first frame of the workload ({s0.width}x{s0.height}, {p})"
+    extra["carter_drift"] = drift
 
     # ---- end to end through the host-buffer C entry point (pinned host memory) ----
     e2e = None
@@ -568,6 +598,12 @@ def run_surrogate(args, rank: int, world: int, dist):
         "disk_outputs_only": {"value": n / (statistics.mean(ms_an_d) * 1e-3), "unit": UNIT,
                               "ms_per_step": statistics.mean(ms_an_d), "fields": disk_fields,
                               "speedup_vs_fp64_plain": statistics.mean(ms64) / statistics.mean(ms_an_d)},
+    }
+    extra["carter_drift"] = {
+        "definition": CARTER_DRIFT_DEF,
+        "surrogate_render": carter_drift_stats(lambda o: net.trace_image(smx, o, stream=stream), n, dev),
+        "fp64_dp45": carter_drift_stats(lambda o: kerr.trace_image(s64, o, stream=stream), n, dev),
+        "mixed_dp45": carter_drift_stats(lambda o: kerr.trace_image(smx, o, stream=stream), n, dev),
     }
     extra["ablation_equal_outputs"] = {
         "all_fields": {"fields": list(OUT_FIELDS_USED), "surrogate_ms": statistics.mean(render_ms),

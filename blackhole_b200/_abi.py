@@ -73,6 +73,7 @@ class KerrImageOut(C.Structure):
         ("intensity", C.c_void_p),
         ("theta_inf", C.c_void_p),
         ("phi_inf", C.c_void_p),
+        ("carter_drift", C.c_void_p),
     ]
 
 
@@ -135,7 +136,10 @@ class SurrogateStats(C.Structure):
                                          "disagreement")]
 
 
-OUT_FIELDS = [name for name, _ in KerrImageOut._fields_]
+# the ten standard fields (carter_drift, the mixed tracer's diagnostic, is asked for by name)
+OUT_FIELDS = [name for name, _ in KerrImageOut._fields_ if name != "carter_drift"]
+# carter_drift is a diagnostic the device entry points write on request only.
+DEVICE_OUT_FIELDS = [name for name, _ in KerrImageOut._fields_]
 INT_FIELDS = ("cls", "steps", "n_cross")
 PLANE_FIELDS = ("r_hit", "phi_hit", "g")
 

@@ -48,6 +48,8 @@ typedef struct BhkImageOut {
   // r [M], cos(theta) and phi (from the camera's azimuth) there; the camera's
   // own position if the ray never came closer
   float *closest;
+  // [n] Carter-constant residual removed by the projection (mixed tracer)
+  double *carter_drift;
 } BhkImageOut;
 
 typedef struct BhkLaunch {

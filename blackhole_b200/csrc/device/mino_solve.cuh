@@ -95,6 +95,25 @@ __constant__
                                      {7.96666477413626740e-01f, 2.22381034453374471e-01f},
                                      {9.60289856497536232e-01f, 1.01228536290376259e-01f}};
 
+// Unrolling of the FP32 quadrature's node loops (4 node pairs of a short
+// interval, 8 of a panel): full unrolling trades instruction-cache footprint
+// for loop overhead in the refinement kernel.
+#ifndef BHM_GL_UNROLL
+#define BHM_GL_UNROLL 8
+#endif
+constexpr int kGlUnroll = BHM_GL_UNROLL;
+
+// a / b: IEEE division in FP64 (the closed-form tracer's results stay those
+// of plain division); in FP32 on the device the 2-ulp __fdividef, ample for
+// elliptic integrals carried to FP32's ~1e-7.
+template <class T>
+BHM_HD T qdiv(T a, T b) {
+#ifdef __CUDA_ARCH__
+  if constexpr (sizeof(T) == 4) return __fdividef(a, b);
+#endif
+  return a / b;
+}
+
 // Carlson's symmetric integral R_F(x, y, z) = 1/2 int_0^inf dt / sqrt((t+x)(t+y)(t+z)),
 // x, y, z >= 0 with at most one zero.
 template <class T>
@@ -107,7 +126,7 @@ BHM_HD T carlson_rf(T x, T y, T z) {
     y = T(0.25) * (y + lam);
     z = T(0.25) * (z + lam);
     const T A = (x + y + z) * T(1.0 / 3.0);
-    const T dx = T(1) - x / A, dy = T(1) - y / A;
+    const T dx = T(1) - qdiv(x, A), dy = T(1) - qdiv(y, A);
     const T dz = -(dx + dy);
     if (fmax(fabs(dx), fmax(fabs(dy), fabs(dz))) < tol) {
       const T e2 = dx * dy - dz * dz, e3 = dx * dy * dz;
@@ -146,10 +165,10 @@ BHM_HD T rc1(T e) {
     return T(1) - e * (T(1.0 / 3.0) - e * (T(0.2) - e * (T(1.0 / 7.0) - e * (T(1.0 / 9.0) - e * T(1.0 / 11.0)))));
   if (e > T(0)) {
     const T se = sqrt(e);
-    return atan(se) / se;
+    return qdiv(atan(se), se);
   }
   const T se = sqrt(-e);
-  return atanh(se) / se;
+  return qdiv(atanh(se), se);
 }
 
 // The fifth-order expansion of R_J about the mean of its arguments.
@@ -177,7 +196,7 @@ BHM_HD T rj_pos(T x, T y, T z, T p) {
     const T sx = sqrt(x), sy = sqrt(y), sz = sqrt(z), sp = sqrt(p);
     const T lam = sx * sy + sy * sz + sz * sx;
     const T d = (sp + sx) * (sp + sy) * (sp + sz);
-    sum += fac * rc1<T>(f3 * delta / (d * d)) / d;
+    sum += qdiv(fac * rc1<T>(qdiv(f3 * delta, d * d)), d);
     fac *= T(0.25);
     f3 *= T(1.0 / 64.0);
     x = T(0.25) * (x + lam);
@@ -185,9 +204,9 @@ BHM_HD T rj_pos(T x, T y, T z, T p) {
     z = T(0.25) * (z + lam);
     p = T(0.25) * (p + lam);
     const T A = (x + y + z + T(2) * p) * T(0.2);
-    const T X = (A - x) / A, Y = (A - y) / A, Z = (A - z) / A, P = (A - p) / A;
+    const T X = qdiv(A - x, A), Y = qdiv(A - y, A), Z = qdiv(A - z, A), P = qdiv(A - p, A);
     if (fmax(fmax(fabs(X), fabs(Y)), fmax(fabs(Z), fabs(P))) < tol)
-      return T(6) * sum + fac * rj_series<T>(X, Y, Z, P) * inv_sqrt(A) / A;
+      return T(6) * sum + qdiv(fac * rj_series<T>(X, Y, Z, P) * inv_sqrt(A), A);
   }
   return T(NAN);
 }
@@ -203,20 +222,20 @@ BHM_HD T cel(T kc, T p, T a, T b) {
   T e = kc, em = T(1);
   if (p > T(0)) {
     p = sqrt(p);
-    b /= p;
+    b = qdiv(b, p);
   } else {
     T f = kc * kc, q = T(1) - f;
     const T g = T(1) - p;
     f -= p;
     q *= (b - a * p);
-    p = sqrt(f / g);
-    a = (a - b) / g;
-    b = -q / (g * g * p) + a * p;
+    p = sqrt(qdiv(f, g));
+    a = qdiv(a - b, g);
+    b = -qdiv(q, g * g * p) + a * p;
   }
   for (int it = 0; it < 40; ++it) {
     const T f = a;
-    a += b / p;
-    T g = e / p;
+    a += qdiv(b, p);
+    T g = qdiv(e, p);
     b += f * g;
     b += b;
     p = g + p;
@@ -227,7 +246,7 @@ BHM_HD T cel(T kc, T p, T a, T b) {
     kc += kc;
     e = kc * em;
   }
-  return T(1.5707963267948966) * (b + a * em) / (em * (em + p));
+  return qdiv(T(1.5707963267948966) * (b + a * em), em * (em + p));
 }
 
 // ---- polar motion ---------------------------------------------------------------
@@ -519,7 +538,7 @@ BHM_HD TauPhi integrate_f2(const RadialF& q, double v0, double v1, double hmax) 
   if (fabs(len) <= 0.25 * hmax) {
     const float c = (float)(v0 + 0.5 * len), hh = (float)(0.5 * len);
     float s = 0.0f, sp = 0.0f;
-#pragma unroll
+#pragma unroll kGlUnroll
     for (int k = 0; k < 4; ++k) {
       float xa, xb;
       const float fa = integrand_fx<KIND>(q, c - hh * kGl8f[k].x, xa);
@@ -536,7 +555,7 @@ BHM_HD TauPhi integrate_f2(const RadialF& q, double v0, double v1, double hmax) 
   for (int p = 0; p < n; ++p) {
     const float c = (float)(v0 + (p + 0.5) * h), hh = (float)(0.5 * h);
     float s = 0.0f, sp = 0.0f;
-#pragma unroll
+#pragma unroll kGlUnroll
     for (int k = 0; k < 8; ++k) {
       float xa, xb;
       const float fa = integrand_fx<KIND>(q, c - hh * kGl16f[k].x, xa);
@@ -735,9 +754,14 @@ BHM_HD void crossing_loop(const Radial& q, const Polar& th, double r_in, double 
     c.t_last = tv;
     c.p_last = pv;
     if (r >= r_in && r <= r_out) {
-      c.r[c.n_hits] = r;
-      c.tau[c.n_hits] = T;
-      c.phr[c.n_hits] = pv;
+      // constant indices keep the per-hit records in registers
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+        if (k == c.n_hits) {
+          c.r[k] = r;
+          c.tau[k] = T;
+          c.phr[k] = pv;
+        }
       if (++c.n_hits >= max_hits) return;
     }
   }

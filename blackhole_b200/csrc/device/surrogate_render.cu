@@ -41,8 +41,16 @@ __device__ __forceinline__ void warp_count(unsigned *stats, int slot, bool pred)
   if ((threadIdx.x & 31u) == 0 && m) atomicAdd(stats + slot, (unsigned)__popc(m));
 }
 
+// Resident 128-thread CTAs per SM the refinement is compiled for: 6 caps it
+// at 80 registers, so that one CTA fits beside the inference kernel's
+// persistent CTA (576 threads x 96 registers) and refines chunk k while the
+// network infers chunk k + 1.
+#ifndef BH_REFINE_MIN_CTAS
+#define BH_REFINE_MIN_CTAS 1
+#endif
+
 template <bool FAST, bool PHI>
-__global__ void __launch_bounds__(128) k_surrogate_refine(const __grid_constant__ BhkImageParams p,
+__global__ void __launch_bounds__(128, BH_REFINE_MIN_CTAS) k_surrogate_refine(const __grid_constant__ BhkImageParams p,
                                                           const __grid_constant__ BhkImageOut o,
                                                           const float *__restrict__ head, float min_conf,
                                                           double band, int verify, int *__restrict__ list,
@@ -122,7 +130,9 @@ __global__ void __launch_bounds__(128) k_surrogate_refine(const __grid_constant_
             if (PHI) ph_inf = -(te.ph + phth);
           }
           double inten = 0.0;
-          for (int k = 0; k < p.max_cross; ++k) {
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {  // max_cross <= 3; constant k keeps c's records in registers
+            if (k >= p.max_cross) break;
             const long long off = (long long)k * p.n_pix + pix;
             double r = 0.0, g = 0.0, ph = 0.0;
             if (k < nhit) {
@@ -143,6 +153,7 @@ __global__ void __launch_bounds__(128) k_surrogate_refine(const __grid_constant_
           if (o.intensity) o.intensity[pix] = inten;
           if (o.theta_inf) o.theta_inf[pix] = th_inf;
           if (o.phi_inf) o.phi_inf[pix] = ph_inf;
+          if (o.carter_drift) o.carter_drift[pix] = 0.0;  // solved, not stepped
         }
       }
     }

@@ -127,6 +127,7 @@ __device__ __forceinline__ bool trace_pixel(const BhkImageParams &p, const BhkIm
   if (o.intensity) o.intensity[pix] = inten;
   if (o.theta_inf) o.theta_inf[pix] = th_inf;
   if (o.phi_inf) o.phi_inf[pix] = ph_inf;
+  if (o.carter_drift) o.carter_drift[pix] = 0.0;  // no stepping: nothing to project
   return true;
 }
 

@@ -37,6 +37,7 @@ struct RayFp64 {
   int steps;
   int attempts;
   int ncross;
+  double drift;  // largest Carter-constant residual the projection removed
 };
 
 __device__ __forceinline__ void init_ray(const BhkImageParams &p, long long pix, RayFp64 &R) {
@@ -62,6 +63,7 @@ __device__ __forceinline__ void init_ray(const BhkImageParams &p, long long pix,
   R.inten = 0.0;
   R.pix = pix;
   project(R.y, R.c);  // idempotent from here on (see iterate)
+  R.drift = 0.0;
   if (p.integrator == 1) {
     const double hh = p.step_coeff * dmin_(R.y.r, p.step_rcap);
     const double sigma = (R.y.r * R.y.r) + ((p.a2 * R.y.u) * R.y.u);
@@ -126,6 +128,7 @@ __device__ __forceinline__ void finish(const BhkImageParams &p, const BhkImageOu
   if (o.intensity) o.intensity[pix] = inten;
   if (o.theta_inf) o.theta_inf[pix] = th;
   if (o.phi_inf) o.phi_inf[pix] = ph;
+  if (o.carter_drift) o.carter_drift[pix] = R.drift;
 }
 
 // One iteration of the trace loop for an active ray; returns the class when
@@ -147,7 +150,7 @@ __device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOu
       step_crossing(R.y, k0, yn, rhs(yn, R.c), h, r_c, phi_c);
       if (on_crossing(p, o, R, r_c, phi_c)) return 1;
     }
-    project(yn, R.c);
+    R.drift = dmax_(R.drift, project(yn, R.c));
     R.y = yn;
     return -1;
   } else {
@@ -172,7 +175,8 @@ __device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOu
     }
     R.y = acc ? d.y5 : R.y;
     R.k1 = acc ? d.k7 : R.k1;
-    project(R.y, R.c);
+    const double drift = project(R.y, R.c);
+    if (acc) R.drift = dmax_(R.drift, drift);
     R.k1.r = R.y.pr;  // projection moves only the momenta
     R.k1.u = R.y.pu;
     R.h = R.h * step_factor(d.err, acc);

@@ -47,6 +47,7 @@ struct RayMx {
   int attempts;
   int ncross;
   float cl_r, cl_u, cl_psi;  // closest approach so far (camera rays only)
+  float drift;               // largest Carter-constant residual the projection removed
 };
 
 __device__ __forceinline__ void split(double v, float &hi, float &lo) {
@@ -95,6 +96,7 @@ __device__ __forceinline__ void init_ray(const BhkImageParams &p, long long pix,
   R.rtol = (float)p.rtol;
   R.atol = (float)p.atol;
   project(R.y, R.lo, R.cd);  // idempotent from here on (see iterate)
+  R.drift = 0.0f;
   const float hh = (float)p.step_coeff * fminf(R.y.r, (float)p.step_rcap);
   R.h = hh / fmaf(R.c.a2 * R.y.u, R.y.u, R.y.r * R.y.r);
   R.k1 = rhs(R.y, R.c);
@@ -173,6 +175,7 @@ __device__ __forceinline__ void init_ray_camera(const BhkImageParams &p, const B
   R.rtol = (float)p.rtol;
   R.atol = (float)p.atol;
   project(R.y, R.lo, R.cd);
+  R.drift = 0.0f;
   const float hh = (float)p.step_coeff * fminf(R.y.r, (float)p.step_rcap);
   R.h = hh / fmaf(R.c.a2 * R.y.u, R.y.u, R.y.r * R.y.r);
   R.k1 = rhs(R.y, R.c);
@@ -259,6 +262,7 @@ __device__ __forceinline__ void finish(const BhkImageParams &p, const BhkImageOu
   if (o.intensity) o.intensity[pix] = inten;
   if (o.theta_inf) o.theta_inf[pix] = th;
   if (o.phi_inf) o.phi_inf[pix] = ph;
+  if (o.carter_drift) o.carter_drift[pix] = (double)R.drift;
 }
 
 // Applies the increment d of an accepted step (acc) to the ray: compensated
@@ -314,7 +318,8 @@ __device__ __forceinline__ bool accept(const BhkImageParams &p, const BhkImageOu
     bhh_dev::hermite_crossing(e, (double)h, r_c, phi_c);
     stop = on_crossing(p, o, R, r_c, phi_c);
   }
-  project(R.y, R.lo, R.cd);
+  const float drift = project(R.y, R.lo, R.cd);
+  if (acc) R.drift = fmaxf(R.drift, drift);
   return stop;
 }
 

@@ -293,7 +293,7 @@ int bh_kerr_trace_image(const BH_KerrScene *scene, const BH_KerrImageOut *out, v
   DeviceScratch *ds = nullptr;
   if (device_scratch(&ds) != 0) return -1;
   const BhkImageOut o{out->cls,   out->steps,     out->n_cross,   out->r_hit,     out->phi_hit,
-                      out->g,     out->flux,      out->intensity, out->theta_inf, out->phi_inf, nullptr, nullptr};
+                      out->g,     out->flux,      out->intensity, out->theta_inf, out->phi_inf, nullptr, nullptr, out->carter_drift};
   return bhh_launch_image(&p, &o, ds->counter, L, stream, nullptr);
 }
 
@@ -356,7 +356,7 @@ int bh_kerr_trace_image_host(const BH_KerrScene *scene, const BH_KerrImageOut *h
   BH_KerrImageOut dev_out{static_cast<int32_t *>(d[0]), static_cast<int32_t *>(d[1]), static_cast<int32_t *>(d[2]),
                           static_cast<double *>(d[3]),  static_cast<double *>(d[4]),  static_cast<double *>(d[5]),
                           static_cast<double *>(d[6]),  static_cast<double *>(d[7]),  static_cast<double *>(d[8]),
-                          static_cast<double *>(d[9])};
+                          static_cast<double *>(d[9]), nullptr};  // the drift diagnostic is not staged
   if (bh_kerr_trace_image(scene, &dev_out, g_hb.stream) != 0) return -1;
   for (int i = 0; i < 10; ++i) {
     if (!fields[i].host) continue;

@@ -496,7 +496,7 @@ int bh_surrogate_trace_image(BH_Surrogate *s, const BH_KerrScene *scene, const B
   if (int rc = cuda_check(cudaMemsetAsync(s->r_counts, 0, 8 * sizeof(unsigned int), st), "cudaMemsetAsync"))
     return rc;
   const BhkImageOut o{out->cls,   out->steps,     out->n_cross,   out->r_hit,     out->phi_hit,
-                      out->g,     out->flux,      out->intensity, out->theta_inf, out->phi_inf, nullptr, nullptr};
+                      out->g,     out->flux,      out->intensity, out->theta_inf, out->phi_inf, nullptr, nullptr, out->carter_drift};
   if (!s->side) {
     if (int rc = cuda_check(cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking), "cudaStreamCreate")) return rc;
     for (cudaEvent_t &e : s->ev)
@@ -571,7 +571,7 @@ int bh_surrogate_trace_image_host(BH_Surrogate *s, const BH_KerrScene *scene, co
   const BH_KerrImageOut dev{static_cast<int32_t *>(d[0]), static_cast<int32_t *>(d[1]), static_cast<int32_t *>(d[2]),
                             static_cast<double *>(d[3]),  static_cast<double *>(d[4]),  static_cast<double *>(d[5]),
                             static_cast<double *>(d[6]),  static_cast<double *>(d[7]),  static_cast<double *>(d[8]),
-                            static_cast<double *>(d[9])};
+                            static_cast<double *>(d[9]), nullptr};  // the drift diagnostic is not staged
   if (int rc = bh_surrogate_trace_image(s, scene, &dev, policy, s->host_stream)) return rc;
   for (int i = 0; i < 10; ++i)
     if (host[i])

@@ -65,8 +65,9 @@ def alloc_image_outputs(s: KerrScene, device="cuda", fields=None) -> dict[str, t
         "r_hit": ((mc, n), torch.float64), "phi_hit": ((mc, n), torch.float64), "g": ((mc, n), torch.float64),
         "flux": ((n,), torch.float64), "intensity": ((n,), torch.float64),
         "theta_inf": ((n,), torch.float64), "phi_inf": ((n,), torch.float64),
+        "carter_drift": ((n,), torch.float64),
     }
-    fields = fields or list(shapes)
+    fields = fields or list(_abi.OUT_FIELDS)
     return {k: torch.empty(*shapes[k][0], dtype=shapes[k][1], device=device) for k in fields}
 
 
@@ -104,7 +105,7 @@ def trace_image(s: KerrScene, outs: dict[str, torch.Tensor] | None = None, strea
     if outs is None:
         outs = alloc_image_outputs(s)
     for k, v in outs.items():
-        if k not in _abi.OUT_FIELDS:
+        if k not in _abi.DEVICE_OUT_FIELDS:
             raise KeyError(f"unknown output field {k!r}")
         if not v.is_cuda or not v.is_contiguous():
             raise TypeError(f"output {k} must be a contiguous CUDA tensor")

@@ -249,6 +249,15 @@ typedef struct BH_KerrImageOut {
     double *intensity;   /**< [n] sum_k g_k^4 (r_in / r_k)^3 */
     double *theta_inf;   /**< [n] polar angle at escape [rad] */
     double *phi_inf;     /**< [n] azimuth at escape [rad] */
+    /** [n] Carter-constant check of the mixed-precision tracer: the largest,
+     *  over the ray's accepted steps, of |eta(state) - eta| / (|q_Th| + a^2),
+     *  eta(state) = (p_u^2 + lambda^2 u^2) / (1 - u^2) - a^2 u^2 from the FP32
+     *  step before its momenta are projected back onto the first integrals
+     *  (evaluated in FP64, away from polar turning points; the reference's
+     *  ConservationMonitor drift of Q, src/physics/conservation_monitor.h:64-105).
+     *  Written by the mixed tracer only (0 for pixels the surrogate or the
+     *  closed form answer); not returned by the host-buffer entry points. */
+    double *carter_drift;
 } BH_KerrImageOut;
 
 /** Check a scene; returns 0 if valid, else -1 with bh_last_error() set. */

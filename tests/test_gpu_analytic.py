@@ -123,7 +123,8 @@ def test_analytic_pole_passing_rays(cuda, oracle):
     the same outputs as the column at alpha = 1e-12 to 1e-9."""
     for a0 in (1e-3, -1e-3):
         s = _scene(width=1, height=48, alpha_min=a0 - 0.5, alpha_max=a0 + 0.5)
-        _compare(_gpu(s), oracle.trace_pixels(s), 3)
+        # the stepper's own error passing the pole there is ~3e-7 rad; a missing turn would be pi
+        _compare(_gpu(s), oracle.trace_pixels(s), 3, ang_tol=1e-6)
     z = _gpu(_scene(width=1, height=48, alpha_min=-0.5, alpha_max=0.5))  # alpha = +0 exactly
     e = _gpu(_scene(width=1, height=48, alpha_min=1e-12 - 0.5, alpha_max=1e-12 + 0.5))
     np.testing.assert_array_equal(z["cls"], e["cls"])

@@ -2,12 +2,16 @@
 default of bh_launch_geodesic_kernel / bhCuda* / bhbCuda*), against the
 reference's own render kernel (geodesicTraceFp32 through its
 bh_launch_geodesic_kernel, src/cuda/kernels_fp32.cu, compiled from its
-source into oracle/_ref/libbh_ref_render.so) on the scene of the reference's
-variant tests (tests/cuda_variants_test.cu:41-80: 64 x 64, rs = 2, isco 4.5,
-camera at (0, 3, 15), redshift on, LUTs off), at a = 0 where the reference's
-own stepping (Schwarzschild RK4, :968-1010) is sound; at a != 0 its Kerr
-path traces the time-reversed photon (a mirror image), so frames are not
-compared there.
+source into oracle/_ref/libbh_ref_render.so), with the settings of the
+reference's variant tests (tests/cuda_variants_test.cu:41-80: redshift on,
+LUTs off, Doppler strength 1; its steps at 0.04, 20,000 at most) on a Blender-bridge camera at 15 rs
+aimed at the hole, at a = 0 where the reference's own stepping
+(Schwarzschild RK4, device_physics.cuh:968-1010) is sound; at a != 0 its
+Kerr path traces the time-reversed photon (a mirror image), so frames are
+not compared there. (The variant tests' own camera, at (0, 3, 15) with the
+identity basis, looks along +z, away from the hole -- d_ray_dir maps local
++z to the basis' third column -- so their frames show only the sky behind
+the camera.)
 
 Checks in the manner of the reference's own variant tests:
 * the captured-pixel set (pure black with the background on, where every
@@ -44,18 +48,13 @@ def leg():
 
 
 def variants_scene(leg, spin=0.0, background=0):
-    """The scene of the reference's cuda_variants_test.cu:41-80."""
-    p = leg.LaunchParams()
-    p.rs, p.spin, p.isco, p.step_size, p.fov_scale, p.max_dist = 2.0, spin, 4.5, 0.08, 1.2, 150.0
-    p.max_steps, p.width, p.height = 500, 64, 64
+    """A 160 x 120 bridge camera at 15 rs, 1.3 rad from the spin axis, aimed
+    at the hole, with the variant tests' settings (cuda_variants_test.cu:41-80)."""
+    p = leg.bridge_params(spin, 15.0, 1.3, 0.6, 160, 120)
+    p.step_size, p.max_steps = 0.04, 20000
     p.adisk_enabled, p.redshift_enabled, p.kerr_enabled, p.use_luts = 1, 1, 1, 0
-    p.cam_pos[0], p.cam_pos[1], p.cam_pos[2] = 0.0, 3.0, 15.0
-    for k, v in enumerate((1.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 1.0)):
-        p.cam_basis[k] = v
-    p.lut_radius_min, p.lut_radius_max = p.isco, 100.0
-    p.redshift_radius_min, p.redshift_radius_max = p.isco, 100.0
-    p.spectral_radius_min, p.spectral_radius_max = p.isco, 100.0
     p.doppler_strength = 1.0
+    p.photon_glow_strength = 0.0
     p.background_intensity = 1.0 if background else 0.0
     p.background_enabled = background
     p.adisk_lit = 1.0

@@ -84,3 +84,34 @@ def test_mixed_edge_cases(cuda):
         a = gpu_trace(scene(width=w, height=h, integrator=1, precision=1))
         assert a["cls"].shape == (w * h,) and (a["cls"] >= 0).all()
     torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("spin,inc", [(0.9, 60.0), (0.998, 85.0)])
+def test_carter_constant_drift(cuda, spin, inc):
+    """The Carter-constant check (carter_drift): the largest relative residual
+    |eta(state) - eta| / (|q_Th| + a^2) each ray's projection removed. The
+    FP64 tracer's steps keep it near its rtol; the mixed tracer's FP32 steps
+    near FP32 resolution; the closed form, which does not step, reports 0.
+    Every pixel gets a finite value, and asking for the field changes no
+    other output."""
+    from blackhole_b200 import _abi, kerr
+
+    fields = list(_abi.OUT_FIELDS) + ["carter_drift"]
+    out = {}
+    for prec in (0, 1):
+        s = scene(width=96, height=96, spin=spin, theta_obs=math.radians(inc), integrator=1, max_crossings=2,
+                  precision=prec)
+        o = kerr.trace_image(s, kerr.alloc_image_outputs(s, fields=fields))
+        out[prec] = {k: v.cpu().numpy() for k, v in o.items()}
+        plain = gpu_trace(s)
+        for k in plain:
+            np.testing.assert_array_equal(out[prec][k], plain[k], err_msg=k)
+    d64, d32 = out[0]["carter_drift"], out[1]["carter_drift"]
+    assert np.all(np.isfinite(d64)) and np.all(np.isfinite(d32)) and (d64 >= 0).all() and (d32 >= 0).all()
+    stepped = out[1]["steps"] > 0
+    assert stepped.mean() > 0.9
+    assert np.median(d64[stepped]) < 1e-9 and d64.max() < 1e-6, (np.median(d64[stepped]), d64.max())
+    assert 0 < np.median(d32[stepped]) < 1e-5 and d32.max() < 1e-3, (np.median(d32[stepped]), d32.max())
+    sa = scene(width=32, height=32, spin=spin, theta_obs=math.radians(inc), integrator=_abi.INTEGRATOR_ANALYTIC)
+    oa = kerr.trace_image(sa, kerr.alloc_image_outputs(sa, fields=fields))
+    assert torch.all(oa["carter_drift"] == 0.0)
