@@ -78,6 +78,8 @@ WORKLOADS = {
     "c4_analytic": dict(width=2048, height=2048, integrator=2, max_crossings=1, frames=[(0.9, 60.0)], analytic=True),
     "disk1_512_analytic": dict(width=512, height=512, integrator=2, max_crossings=3, frames=[(0.9, 45.0)],
                                analytic=True),
+    "disk1_1024_analytic": dict(width=1024, height=1024, integrator=2, max_crossings=3, frames=[(0.9, 45.0)],
+                                analytic=True),
     "c2_128": dict(width=128, height=128, integrator=1, max_crossings=1, frames=[(0.94, 17.0)], rt=True),
 }
 SURROGATE_WEIGHTS = ROOT / "blackhole_b200" / "data" / "surrogate_c4.npz"

@@ -89,10 +89,11 @@ constexpr double kProjTau = 1e-6;
 // p_u^2 = U(u), keeping their signs, where those are well conditioned (away
 // from turning points). Without it the second-order form lets b^2 drift by
 // ~rtol r^2 per step at r ~ 1000, where b enters R only at order b^2/r^2.
-// Returns the Carter-constant residual the projection removed, |eta(state) -
-// eta| / (|q_Th| + a^2) with eta(state) - eta = (p_u^2 - U(u)) / (1 - u^2),
-// where the polar momentum was projected (0 near a polar turning point).
-__device__ __forceinline__ double project(Yd &y, const RayC &c) {
+// With want_drift, returns the Carter-constant residual the projection
+// removed, |eta(state) - eta| / (|q_Th| + a^2) with eta(state) - eta =
+// (p_u^2 - U(u)) / (1 - u^2), where the polar momentum was projected (0 near
+// a polar turning point); otherwise 0, and the division is skipped.
+__device__ __forceinline__ double project(Yd &y, const RayC &c, bool want_drift = false) {
   const double Rv = pot_R(y.r, c);
   const double r2 = y.r * y.r;
   if (Rv > kProjTau * (r2 * r2)) {
@@ -103,7 +104,7 @@ __device__ __forceinline__ double project(Yd &y, const RayC &c) {
   const double scale = fabs(c.qTh) + (c.a * c.a);
   double drift = 0.0;
   if (Uv > kProjTau * scale) {
-    drift = fabs((y.pu * y.pu) - Uv) / ((1.0 - (y.u * y.u)) * scale);
+    if (want_drift) drift = fabs((y.pu * y.pu) - Uv) / ((1.0 - (y.u * y.u)) * scale);
     const double m = sqrt(Uv);
     y.pu = (y.pu < 0.0) ? -m : m;
   }

@@ -83,10 +83,12 @@ constexpr double kProjTau = 1e-6;
 // a turning point, where R ~ 1e-4 r^4, would already move p_r by 4e-4; in
 // FP64 the reset is exact at the 1e-6 threshold of the FP64 path. Only the
 // square root's argument is FP64: the result is rounded to FP32 once.
-// Returns the Carter-constant residual the projection removed, |eta(state) -
-// eta| / (|q_Th| + a^2) with eta(state) - eta = (p_u^2 - U(u)) / (1 - u^2),
-// where the polar momentum was projected (0 near a polar turning point).
-__device__ __forceinline__ float project(Yf &y, const Lof &lo, const RayCd &c) {
+// With want_drift, returns the Carter-constant residual the projection
+// removed, |eta(state) - eta| / (|q_Th| + a^2) with eta(state) - eta =
+// (p_u^2 - U(u)) / (1 - u^2), where the polar momentum was projected (0 near
+// a polar turning point): the difference in FP64 (p_u^2 and U nearly
+// cancel), the quotient in FP32; otherwise 0.
+__device__ __forceinline__ float project(Yf &y, const Lof &lo, const RayCd &c, bool want_drift = false) {
   const double r = (double)y.r + (double)lo.r;
   const double u = (double)y.u + (double)lo.u;
   const double A = r * r + c.a * c.a - c.a * c.lam;
@@ -99,8 +101,10 @@ __device__ __forceinline__ float project(Yf &y, const Lof &lo, const RayCd &c) {
   const double scale = fabs(c.qTh) + c.a * c.a;
   float drift = 0.0f;
   if (Uv > kProjTau * scale) {
-    const double pu = (double)y.pu;
-    drift = (float)(fabs(pu * pu - Uv) / ((1.0 - u2) * scale));
+    if (want_drift) {
+      const double pu = (double)y.pu;
+      drift = __fdividef((float)fabs(pu * pu - Uv), (float)((1.0 - u2) * scale));
+    }
     y.pu = copysignf(sqrtf((float)Uv), y.pu);
   }
   return drift;

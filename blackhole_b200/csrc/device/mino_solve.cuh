@@ -96,10 +96,12 @@ __constant__
                                      {9.60289856497536232e-01f, 1.01228536290376259e-01f}};
 
 // Unrolling of the FP32 quadrature's node loops (4 node pairs of a short
-// interval, 8 of a panel): full unrolling trades instruction-cache footprint
-// for loop overhead in the refinement kernel.
+// interval, 8 of a panel). By 2: the refinement kernel then fits in 80
+// registers (see BH_REFINE_MIN_CTAS) without spilling its hot loop; a 2048^2
+// render with azimuths measured 3.41 ms against 3.61 ms fully unrolled at
+// 80 registers and 3.72 ms fully unrolled at 148.
 #ifndef BHM_GL_UNROLL
-#define BHM_GL_UNROLL 8
+#define BHM_GL_UNROLL 2
 #endif
 constexpr int kGlUnroll = BHM_GL_UNROLL;
 

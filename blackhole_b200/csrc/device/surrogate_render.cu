@@ -43,14 +43,15 @@ __device__ __forceinline__ void warp_count(unsigned *stats, int slot, bool pred)
 
 // Resident 128-thread CTAs per SM the refinement is compiled for: 6 caps it
 // at 80 registers, so that one CTA fits beside the inference kernel's
-// persistent CTA (576 threads x 96 registers) and refines chunk k while the
-// network infers chunk k + 1.
+// persistent CTA (576 threads x 96 registers leave 10,240 of the SM's 65,536)
+// and refines chunk k while the network infers chunk k + 1. The all-FP64
+// solve (refine_fp64) would spill at 80 and keeps 2.
 #ifndef BH_REFINE_MIN_CTAS
-#define BH_REFINE_MIN_CTAS 1
+#define BH_REFINE_MIN_CTAS 6
 #endif
 
 template <bool FAST, bool PHI>
-__global__ void __launch_bounds__(128, BH_REFINE_MIN_CTAS) k_surrogate_refine(const __grid_constant__ BhkImageParams p,
+__global__ void __launch_bounds__(128, FAST ? BH_REFINE_MIN_CTAS : 2) k_surrogate_refine(const __grid_constant__ BhkImageParams p,
                                                           const __grid_constant__ BhkImageOut o,
                                                           const float *__restrict__ head, float min_conf,
                                                           double band, int verify, int *__restrict__ list,

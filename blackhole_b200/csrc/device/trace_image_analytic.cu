@@ -131,7 +131,13 @@ __device__ __forceinline__ bool trace_pixel(const BhkImageParams &p, const BhkIm
   return true;
 }
 
-__global__ void __launch_bounds__(128, 4) k_trace_image_analytic(const __grid_constant__ BhkImageParams p,
+// Resident 128-thread CTAs per SM the closed form is compiled for (4: 128
+// registers per thread).
+#ifndef BH_ANALYTIC_MIN_CTAS
+#define BH_ANALYTIC_MIN_CTAS 4
+#endif
+
+__global__ void __launch_bounds__(128, BH_ANALYTIC_MIN_CTAS) k_trace_image_analytic(const __grid_constant__ BhkImageParams p,
                                                               const __grid_constant__ BhkImageOut o,
                                                               int *__restrict__ list,
                                                               unsigned int *__restrict__ count) {
@@ -142,7 +148,7 @@ __global__ void __launch_bounds__(128, 4) k_trace_image_analytic(const __grid_co
 
 // The same over a list of pixels (the surrogate renderer's rejected pixels);
 // those it does not cover go on to list2.
-__global__ void __launch_bounds__(128, 4) k_trace_list_analytic(const __grid_constant__ BhkImageParams p,
+__global__ void __launch_bounds__(128, BH_ANALYTIC_MIN_CTAS) k_trace_list_analytic(const __grid_constant__ BhkImageParams p,
                                                                 const __grid_constant__ BhkImageOut o,
                                                                 const int *__restrict__ list,
                                                                 const unsigned int *__restrict__ count,

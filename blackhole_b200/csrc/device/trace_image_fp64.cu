@@ -150,7 +150,7 @@ __device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOu
       step_crossing(R.y, k0, yn, rhs(yn, R.c), h, r_c, phi_c);
       if (on_crossing(p, o, R, r_c, phi_c)) return 1;
     }
-    R.drift = dmax_(R.drift, project(yn, R.c));
+    R.drift = dmax_(R.drift, project(yn, R.c, o.carter_drift != nullptr));
     R.y = yn;
     return -1;
   } else {
@@ -175,7 +175,7 @@ __device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOu
     }
     R.y = acc ? d.y5 : R.y;
     R.k1 = acc ? d.k7 : R.k1;
-    const double drift = project(R.y, R.c);
+    const double drift = project(R.y, R.c, o.carter_drift != nullptr);
     if (acc) R.drift = dmax_(R.drift, drift);
     R.k1.r = R.y.pr;  // projection moves only the momenta
     R.k1.u = R.y.pu;

@@ -318,7 +318,7 @@ __device__ __forceinline__ bool accept(const BhkImageParams &p, const BhkImageOu
     bhh_dev::hermite_crossing(e, (double)h, r_c, phi_c);
     stop = on_crossing(p, o, R, r_c, phi_c);
   }
-  const float drift = project(R.y, R.lo, R.cd);
+  const float drift = project(R.y, R.lo, R.cd, o.carter_drift != nullptr);
   if (acc) R.drift = fmaxf(R.drift, drift);
   return stop;
 }
@@ -445,14 +445,14 @@ __device__ __forceinline__ void trace_loop(const Src &src, unsigned long long *_
 }
 
 template <int INTEG>
-__global__ void __launch_bounds__(128) k_trace_image_mixed(const __grid_constant__ BhkImageParams p,
+__global__ void __launch_bounds__(128, 4) k_trace_image_mixed(const __grid_constant__ BhkImageParams p,
                                                            const __grid_constant__ BhkImageOut o,
                                                            unsigned long long *__restrict__ counter, int refill) {
   trace_loop<INTEG>(bhsrc::SingleSrc{p, o}, counter, refill);
 }
 
 template <int INTEG>
-__global__ void __launch_bounds__(128) k_trace_list_mixed(const __grid_constant__ BhkImageParams p,
+__global__ void __launch_bounds__(128, 4) k_trace_list_mixed(const __grid_constant__ BhkImageParams p,
                                                           const __grid_constant__ BhkImageOut o,
                                                           const int *__restrict__ list,
                                                           const unsigned int *__restrict__ count,
@@ -468,7 +468,7 @@ __global__ void __launch_bounds__(128) k_trace_camera_mixed(const __grid_constan
 }
 
 template <int INTEG>
-__global__ void __launch_bounds__(128) k_trace_batch_mixed(const __grid_constant__ BhkBatchDev b,
+__global__ void __launch_bounds__(128, 4) k_trace_batch_mixed(const __grid_constant__ BhkBatchDev b,
                                                            unsigned long long *__restrict__ counter, int refill) {
   if (threadIdx.x == 0) atomicMin(b.start_ns, bhsrc::globaltimer_ns());
   trace_loop<INTEG>(bhsrc::BatchSrc{b}, counter, refill);
