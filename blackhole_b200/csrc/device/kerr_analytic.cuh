@@ -60,6 +60,13 @@
 #else
 #define BHA_SCALL BHA_CALL
 #endif
+// The azimuth's routines among them (the elliptic integrals of the third
+// kind and their per-ray constants) alone: BHA_INLINE_PHI.
+#if defined(BHA_INLINE_SOLUTION) || defined(BHA_INLINE_PHI)
+#define BHA_PCALL BHM_HD
+#else
+#define BHA_PCALL BHA_CALL
+#endif
 
 namespace bhan {
 
@@ -224,7 +231,7 @@ BHM_HD double ellip_f(double s, double c, double m1) { return s * carlson_rf(c *
 BHM_HD double q_part(double n, double s, double c, double m1) {
   return s * s * s * carlson_rj(c * c, c * c + m1 * s * s, 1.0, 1.0 - n * s * s) * (1.0 / 3.0);
 }
-BHA_SCALL double ellip_q_sc(double n, double s, double c, double m1, double &qc) {
+BHA_PCALL double ellip_q_sc(double n, double s, double c, double m1, double &qc) {
   if (c >= 0.0) return q_part(n, s, c, m1);
   if (isnan(qc)) qc = ellip_qc(n, m1);
   return 2.0 * qc - q_part(n, s, -c, m1);
@@ -236,13 +243,13 @@ BHM_HD double ellip_qc_nc(double nc, double m1) { return bulirsch_cel(sqrt(m1), 
 BHM_HD double q_part_nc(double nc, double s, double c, double m1) {
   return s * s * s * carlson_rj(c * c, c * c + m1 * s * s, 1.0, c * c + nc * s * s) * (1.0 / 3.0);
 }
-BHA_SCALL double ellip_q_sc_nc(double nc, double s, double c, double m1, double &qc) {
+BHA_PCALL double ellip_q_sc_nc(double nc, double s, double c, double m1, double &qc) {
   if (c >= 0.0) return q_part_nc(nc, s, c, m1);
   if (isnan(qc)) qc = ellip_qc_nc(nc, m1);
   return 2.0 * qc - q_part_nc(nc, s, -c, m1);
 }
 // Both poles at once (the same amplitude, characteristics n1, n2; c >= 0).
-BHA_SCALL void ellip_q2_sc(double n1, double n2, double s, double c, double m1, double &q1, double &q2) {
+BHA_PCALL void ellip_q2_sc(double n1, double n2, double s, double c, double m1, double &q1, double &q2) {
   const double x = c * c, y = c * c + m1 * s * s, s2 = s * s, s3 = s2 * s * (1.0 / 3.0);
   const double p1 = 1.0 - n1 * s2, p2 = 1.0 - n2 * s2;
   if (p1 > 0.0 && p2 > 0.0) {
@@ -527,7 +534,7 @@ BHM_HD double p2_r1(JPole &J, double m1, double X, const Amp &a) {
   return (X + J.par * ellip_q_sc(J.par, a.s, a.c, m1, J.qc)) / J.Aq - J.al * p2_g(J, a);
 }
 
-BHA_SCALL void j_poles(const RadSol &q, double r_plus, double r_minus, JPole &jp, JPole &jm) {
+BHA_PCALL void j_poles(const RadSol &q, double r_plus, double r_minus, JPole &jp, JPole &jm) {
   for (int k = 0; k < 2; ++k) {
     JPole &J = k == 0 ? jp : jm;
     const double rpm = k == 0 ? r_plus : r_minus;
@@ -565,9 +572,9 @@ BHM_HD double q_integrand(double n, double m1, double ph) {
 // observer's mirror image (+phi_obs), so Q(h; phi_end) = -Q(h; -phi_obs) +
 // int_(phi_obs)^(phi_end) by 4-point Gauss-Legendre when that interval is
 // short (< 0.05 rad: error ~ 1e-20 relative); otherwise as at any point.
-BHA_SCALL void j_eval_escape(const RadSol &q, JPole &jp, JPole &jm, double &vp, double &vm);
+BHA_PCALL void j_eval_escape(const RadSol &q, JPole &jp, JPole &jm, double &vp, double &vm);
 
-BHA_SCALL void j_eval(const RadSol &q, JPole &jp, JPole &jm, double X, const Amp &a, double &vp, double &vm) {
+BHA_PCALL void j_eval(const RadSol &q, JPole &jp, JPole &jm, double X, const Amp &a, double &vp, double &vm) {
   if (q.type == kP2) {
     vp = jp.k1 * (q.X0 - X) + jp.k2 * (jp.t0 - p2_r1(jp, q.m1, X, a));
     vm = jm.k1 * (q.X0 - X) + jm.k2 * (jm.t0 - p2_r1(jm, q.m1, X, a));
@@ -579,7 +586,7 @@ BHA_SCALL void j_eval(const RadSol &q, JPole &jp, JPole &jm, double X, const Amp
   vm = jm.k1 * ((X - q.X0) + jm.k2 * (qm - jm.t0));
 }
 
-BHA_SCALL void j_eval_escape(const RadSol &q, JPole &jp, JPole &jm, double &vp, double &vm) {
+BHA_PCALL void j_eval_escape(const RadSol &q, JPole &jp, JPole &jm, double &vp, double &vm) {
   const double p0 = atan2(-q.a0.s, q.a0.c), p1 = atan2(q.a_end.s, q.a_end.c);  // both in (0, pi/2)
   const double d = p1 - p0;
   if (q.type != kS || !(fabs(d) < 0.05)) {
@@ -667,7 +674,7 @@ BHM_HD double pole_turns(const PolSol &t, double lam, double tau) {
   return copysign(3.141592653589793, lam) * passes;
 }
 
-BHA_SCALL double phi_theta_crossing(PolSol &t, double lam, double tau) {
+BHA_PCALL double phi_theta_crossing(PolSol &t, double lam, double tau) {
   if (!(t.zc > 0.0)) return pole_turns(t, lam, tau);
   polar_q0(t);
   const double j = rint((t.phi_start + tau) / t.period);
@@ -675,7 +682,7 @@ BHA_SCALL double phi_theta_crossing(PolSol &t, double lam, double tau) {
 }
 
 // u, du/dtau and lambda int_0^tau dtau / (1 - u^2) at any tau.
-BHA_SCALL void polar_at(PolSol &t, double lam, double tau, double &u, double &pu, double &phi_th) {
+BHA_PCALL void polar_at(PolSol &t, double lam, double tau, double &u, double &pu, double &phi_th) {
   const double total = t.phi_start + tau;
   const double j = floor(total / t.period);
   double sa, ca, da;  // amplitude in [0, pi): sa >= 0

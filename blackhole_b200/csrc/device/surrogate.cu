@@ -465,6 +465,10 @@ __global__ void k_loss(const float* __restrict__ out, const float* __restrict__ 
 // While one slot's epilogue (bias, SiLU, BF16, store to shared) runs, the
 // tensor core works on the other slot.
 
+#ifndef BHS_EPI_PIPE
+#define BHS_EPI_PIPE 1
+#endif
+
 constexpr int kInfThreads = 576;  // 2 control warps + 2 slots x 8 epilogue warps
 constexpr int kEpiThreads = 256;  // epilogue threads per slot
 constexpr int kInfRing = 3;
@@ -648,6 +652,28 @@ __global__ void __launch_bounds__(kInfThreads, 1)
         if (!ok) break;
         umma::tc_fence_after();
         const float* b = A.bias + l * BHS_HIDDEN;
+#if BHS_EPI_PIPE
+        // 32 columns at a time, the next chunk's TMEM load in flight while
+        // this one is activated and stored (two register buffers).
+        float va[32], vb[32];
+        umma::tmem_ld32_nowait(tacc + 32u * (4 * hf), va);
+        umma::tmem_wait_ld();
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+          const int j = 4 * hf + h;
+          if (h < 3) umma::tmem_ld32_nowait(tacc + 32u * (j + 1), (h & 1) ? va : vb);
+          const float* v = (h & 1) ? vb : va;
+          uint32_t pk[16];
+#pragma unroll
+          for (int i = 0; i < 16; ++i)  // b: halved biases, so hy = acc / 2 + b / 2
+            pk[i] = silu_f16x2(fmaf(v[2 * i], 0.5f, b[32 * j + 2 * i]), fmaf(v[2 * i + 1], 0.5f, b[32 * j + 2 * i + 1]));
+          const uint32_t cb = act + (uint32_t)(j >> 1) * kActChunk;
+#pragma unroll
+          for (int uu = 0; uu < 4; ++uu)
+            st_unit(cb, r, (j & 1) * 4 + uu, pk[4 * uu], pk[4 * uu + 1], pk[4 * uu + 2], pk[4 * uu + 3]);
+          if (h < 3) umma::tmem_wait_ld();
+        }
+#else
 #pragma unroll 1
         for (int jj = 0; jj < 2; ++jj) {  // 64 columns per TMEM wait: two loads in flight
           const int j0 = 4 * hf + 2 * jj;
@@ -669,6 +695,7 @@ __global__ void __launch_bounds__(kInfThreads, 1)
               st_unit(cb, r, (j & 1) * 4 + uu, pk[4 * uu], pk[4 * uu + 1], pk[4 * uu + 2], pk[4 * uu + 3]);
           }
         }
+#endif
         umma::fence_async_smem();
         umma::tc_fence_before();
         umma::mbar_arrive(act_ready(s));

@@ -48,6 +48,7 @@ struct RayMx {
   int ncross;
   float cl_r, cl_u, cl_psi;  // closest approach so far (camera rays only)
   float drift;               // largest Carter-constant residual the projection removed
+  bool drift_on;             // the caller asked for carter_drift (read once per ray)
 };
 
 __device__ __forceinline__ void split(double v, float &hi, float &lo) {
@@ -97,6 +98,7 @@ __device__ __forceinline__ void init_ray(const BhkImageParams &p, long long pix,
   R.atol = (float)p.atol;
   project(R.y, R.lo, R.cd);  // idempotent from here on (see iterate)
   R.drift = 0.0f;
+  R.drift_on = false;
   const float hh = (float)p.step_coeff * fminf(R.y.r, (float)p.step_rcap);
   R.h = hh / fmaf(R.c.a2 * R.y.u, R.y.u, R.y.r * R.y.r);
   R.k1 = rhs(R.y, R.c);
@@ -176,6 +178,7 @@ __device__ __forceinline__ void init_ray_camera(const BhkImageParams &p, const B
   R.atol = (float)p.atol;
   project(R.y, R.lo, R.cd);
   R.drift = 0.0f;
+  R.drift_on = false;
   const float hh = (float)p.step_coeff * fminf(R.y.r, (float)p.step_rcap);
   R.h = hh / fmaf(R.c.a2 * R.y.u, R.y.u, R.y.r * R.y.r);
   R.k1 = rhs(R.y, R.c);
@@ -318,7 +321,7 @@ __device__ __forceinline__ bool accept(const BhkImageParams &p, const BhkImageOu
     bhh_dev::hermite_crossing(e, (double)h, r_c, phi_c);
     stop = on_crossing(p, o, R, r_c, phi_c);
   }
-  const float drift = project(R.y, R.lo, R.cd, o.carter_drift != nullptr);
+  const float drift = project(R.y, R.lo, R.cd, R.drift_on);
   if (acc) R.drift = fmaxf(R.drift, drift);
   return stop;
 }
@@ -422,6 +425,7 @@ __device__ __forceinline__ void trace_loop(const Src &src, unsigned long long *_
           const int f = src.frame_of((long long)mine, pix);
           init_from(src, f, pix, R);
           R.f = f;
+          R.drift_on = src.out(f).carter_drift != nullptr;
           active = true;
         } else {
           exhausted = true;
