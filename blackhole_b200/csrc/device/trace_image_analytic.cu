@@ -176,6 +176,9 @@ extern "C" int bhk_trace_list_analytic(const BhkImageParams *p, const BhkImageOu
 extern "C" int bhk_trace_image_analytic(const BhkImageParams *p, const BhkImageOut *o, int *list,
                                         unsigned int *count, BhkLaunch L, void *stream) {
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+#ifdef BH_ANALYTIC_CARVEOUT
+  cudaFuncSetAttribute(k_trace_image_analytic, cudaFuncAttributePreferredSharedMemoryCarveout, BH_ANALYTIC_CARVEOUT);
+#endif
   if (cudaMemsetAsync(count, 0, sizeof(unsigned int), s) != cudaSuccess) return -1;
   k_trace_image_analytic<<<L.grid, L.block, 0, s>>>(*p, *o, list, count);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;

@@ -145,9 +145,10 @@ class Surrogate:
     def save(self, path, manifest: dict | None = None):
         """Checkpoint: parameters and Adam state in ``path`` (.npz), and beside
         it ``path`` + ``.json``, a manifest of what made it (``manifest``:
-        seed, training and data configuration; added here: the network's
-        shapes, the SHA-256 of the parameters, the data configuration's hash,
-        the git commit of the source tree when there is one)."""
+        seed, training and data configuration, optionally ``git_commit``;
+        added here: the network's shapes, the SHA-256 of the parameters, the
+        data configuration's hash, and the git commit of the source tree when
+        the caller gave none and the tree is a git checkout)."""
         import hashlib
         import json
         import subprocess
@@ -164,11 +165,12 @@ class Surrogate:
         })
         if "data" in man:
             man["data_hash"] = hashlib.sha256(json.dumps(man["data"], sort_keys=True).encode()).hexdigest()
-        try:
-            man["git_commit"] = subprocess.run(["git", "rev-parse", "HEAD"], capture_output=True, text=True,
-                                               cwd=Path(__file__).resolve().parent, check=True).stdout.strip()
-        except (OSError, subprocess.CalledProcessError):
-            man["git_commit"] = None
+        if not man.get("git_commit"):  # the caller's, else the source tree's when it is a git checkout
+            try:
+                man["git_commit"] = subprocess.run(["git", "rev-parse", "HEAD"], capture_output=True, text=True,
+                                                   cwd=Path(__file__).resolve().parent, check=True).stdout.strip()
+            except (OSError, subprocess.CalledProcessError):
+                man["git_commit"] = None
         Path(str(path) + ".json").write_text(json.dumps(man, indent=1, sort_keys=True) + "\n")
 
     def load(self, path):

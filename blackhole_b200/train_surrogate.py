@@ -60,6 +60,8 @@ def main(argv=None) -> dict:
     ap.add_argument("--holdout-frames", type=int, default=64)
     ap.add_argument("--out", default="blackhole_b200/data/surrogate_c4.npz")
     ap.add_argument("--log", default=None, help="JSON lines log file")
+    ap.add_argument("--source-commit", default=None,
+                    help="git commit of the sources, for the manifest (default: asked of git)")
     a = ap.parse_args(argv)
 
     t0 = time.time()
@@ -91,6 +93,7 @@ def main(argv=None) -> dict:
     log(rec)
     net.save(a.out, manifest={
         "seed": a.seed,
+        "git_commit": a.source_commit,
         "train": {"epochs": a.epochs, "batch": a.batch, "lr": a.lr, "optimizer": "Adam, cosine learning rate",
                   "train_seconds": t_train},
         "data": {"frames": a.frames, "size": a.size, "holdout_frames": a.holdout_frames,
