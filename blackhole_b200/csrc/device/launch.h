@@ -50,6 +50,10 @@ typedef struct BhkImageOut {
   float *closest;
   // [n] Carter-constant residual removed by the projection (mixed tracer)
   double *carter_drift;
+  // mixed camera tracer with a BhkVolume: [8][n] front-to-back emission of
+  // the disk slab (r, g, b), transmittance, Stokes Q, U, V, and 1 where the
+  // slab made the ray opaque (0 otherwise)
+  float *vol;
 } BhkImageOut;
 
 typedef struct BhkLaunch {
@@ -182,11 +186,28 @@ typedef struct BhkCamera {
   int32_t width, height;
 } BhkCamera;
 
+// The volumetric disk of the render launch ABI's RTE and Stokes modes (the
+// reference's d_trace_geodesic_rte / d_trace_geodesic_stokes): a slab of
+// Gaussian height h about z = 0 between r_in and r_out (cylindrical radius,
+// world units), composited front to back along each camera ray with the
+// reference's emission, opacity and polarization model. Path elements are the
+// reference's: its Mino time in world units, d lambda = d tau / m.
+typedef struct BhkVolume {
+  int32_t mode;          // 1: intensity only (RTE), 2: with Stokes Q, U, V
+  int32_t emit;          // the disk emits (adisk_enabled)
+  float m, rs;           // world units per M; rs (world)
+  float r_in, r_out, h;  // slab: cylindrical radii and Gaussian height (world)
+  float opacity;         // absorption per unit emissivity (rte_opacity_scale)
+  float b_angle, ne_scale;  // Stokes: field angle (EVPA of emission), Faraday rate per unit density
+  float cphi, sphi;      // camera azimuth: tracer frame -> world
+} BhkVolume;
+
 // Traces every pixel of a camera with the mixed tracer (p: spin, horizon,
 // escape and disk radii, integrator, tolerances; p.r_obs = cam.r0, Carter
-// potentials).
+// potentials). With vol (non-NULL, mode 1 or 2) the rays also integrate the disk slab
+// into o->vol, and a ray the slab makes opaque stops with class 1.
 int bhk_trace_camera_mixed(const BhkImageParams *p, const BhkCamera *cam, const BhkImageOut *o,
-                           unsigned long long *work_counter, BhkLaunch L, void *stream);
+                           unsigned long long *work_counter, BhkLaunch L, void *stream, const BhkVolume *vol);
 int bhk_trace_camera_mixed_occupancy(int block, int *blocks_per_sm);
 
 // Positions (x, y, z) [M] after every FP64 RK4 step of image-plane rays, up
@@ -215,7 +236,8 @@ typedef struct BhkLook {
   double r_esc;                  // escape radius [M]
   float cam_pos[3], cam_right[3];
   float cphi, sphi;              // camera azimuth: tracer frame -> world
-  int32_t redshift_enabled, use_luts, background_enabled, pad;
+  int32_t redshift_enabled, use_luts, background_enabled;
+  int32_t vol_mode;              // 1, 2: the slab of the RTE / Stokes modes was traced into `vol`
   float adisk_lit, doppler_strength, bg_intensity, time_sec, glow_strength;
   float bg_yaw, bg_pitch, bg_filter;
   float bg_layers[12], bg_lod_bias[3];
@@ -225,7 +247,11 @@ typedef struct BhkLook {
       tex_equirect;
 } BhkLook;
 int bhk_legacy_look(const BhkLook *L, const int32_t *cls, const double *r_hit, const double *phi_hit,
-                    const double *theta_inf, const double *phi_inf, const float *closest, float *rgba, void *stream);
+                    const double *theta_inf, const double *phi_inf, const float *closest, const float *vol, float *rgba,
+                    void *stream);
+
+// n exact Stokes transfer steps (vol.cuh), device arrays state [n][4], coef [n][7], out [n][4].
+int bhk_stokes_steps(long long n, const float *state, const float *coef, float *out, void *stream);
 
 int bhk_legacy_set_blackbody(const float *rgb_table, int n, float log2_t0, float log2_t1);
 int bhk_legacy_shade(const BhkShade *s, const int32_t *cls, const double *r_hit, const double *g, const double *flux,

@@ -23,6 +23,7 @@
 #include <cstdint>
 
 #include "launch.h"
+#include "vol.cuh"
 
 namespace {
 
@@ -387,11 +388,33 @@ __global__ void __launch_bounds__(256) k_legacy_look(const __grid_constant__ Bhk
                                                      const double *__restrict__ phi_hit,
                                                      const double *__restrict__ theta_inf,
                                                      const double *__restrict__ phi_inf,
-                                                     const float *__restrict__ closest, float4 *__restrict__ rgba) {
+                                                     const float *__restrict__ closest,
+                                                     const float *__restrict__ vol, float4 *__restrict__ rgba) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= L.n) return;
   const int c = cls[i];
   float4 out = make_float4(0.0f, 0.0f, 0.0f, 1.0f);  // captured: black
+  if (L.vol_mode) {
+    // The slab's emission in front of the ray's end; an escaped ray adds the
+    // shaped sky (no ring glow) times the transmittance left. The Stokes
+    // mode tints every pixel but those the horizon ended.
+    const long long n = L.n;
+    float rgb[3] = {vol[i], vol[n + i], vol[2 * n + i]};
+    if (c == 2) {
+      const V cam = v3(L.cam_pos[0], L.cam_pos[1], L.cam_pos[2]);
+      const V esc = world(L, L.r_esc, cos(theta_inf[i]), phi_inf[i]);
+      const float rmin_m = closest[i];
+      const V cp = world(L, (double)rmin_m, (double)closest[L.n + i], (double)closest[2 * L.n + i]);
+      const V sky = shape_sky(L, sky_color(L, unit(sub(esc, cam))), rmin_m * L.m, cp);
+      const float T = vol[3 * n + i];
+      rgb[0] += T * sky.x;
+      rgb[1] += T * sky.y;
+      rgb[2] += T * sky.z;
+    }
+    if (L.vol_mode == 2 && c != 0) bhvol::stokes_tint(rgb, vol[4 * n + i], vol[5 * n + i], vol[6 * n + i]);
+    rgba[i] = make_float4(rgb[0], rgb[1], rgb[2], 1.0f);
+    return;
+  }
   if (c == 1) {
     float inten = 0.0f;
     const V col = disk_color(L, world(L, r_hit[i], 0.0, phi_hit[i]), inten);
@@ -410,14 +433,32 @@ __global__ void __launch_bounds__(256) k_legacy_look(const __grid_constant__ Bhk
   rgba[i] = out;
 }
 
+__global__ void k_stokes_steps(long long n, const float4 *__restrict__ state, const float *__restrict__ coef,
+                               float4 *__restrict__ out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 s = state[i];
+  const float *c = coef + 7 * i;
+  const bhvol::Stokes o = bhvol::stokes_step(bhvol::Stokes{s.x, s.y, s.z, s.w}, c[0], c[1], c[2], c[3], c[4], c[5], c[6]);
+  out[i] = make_float4(o.i, o.q, o.u, o.v);
+}
+
 }  // namespace
 
+extern "C" int bhk_stokes_steps(long long n, const float *state, const float *coef, float *out, void *stream) {
+  if (n <= 0) return 0;
+  const unsigned blocks = (unsigned)((n + 255) / 256);
+  k_stokes_steps<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      n, reinterpret_cast<const float4 *>(state), coef, reinterpret_cast<float4 *>(out));
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
 extern "C" int bhk_legacy_look(const BhkLook *L, const int32_t *cls, const double *r_hit, const double *phi_hit,
-                               const double *theta_inf, const double *phi_inf, const float *closest, float *rgba,
-                               void *stream) {
+                               const double *theta_inf, const double *phi_inf, const float *closest, const float *vol,
+                               float *rgba, void *stream) {
   if (L->n <= 0) return 0;
   const unsigned blocks = (unsigned)((L->n + 255) / 256);
   k_legacy_look<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(*L, cls, r_hit, phi_hit, theta_inf, phi_inf,
-                                                                        closest, reinterpret_cast<float4 *>(rgba));
+                                                                        closest, vol, reinterpret_cast<float4 *>(rgba));
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

@@ -27,6 +27,7 @@
 #include "image_mixed.cuh"
 #include "launch.h"
 #include "rt.cuh"
+#include "vol.cuh"
 
 namespace bhm {
 
@@ -49,6 +50,7 @@ struct RayMx {
   float cl_r, cl_u, cl_psi;  // closest approach so far (camera rays only)
   float drift;               // largest Carter-constant residual the projection removed
   bool drift_on;             // the caller asked for carter_drift (read once per ray)
+  bhvol::Accum va;           // disk slab seen so far (camera rays of the volumetric modes)
 };
 
 __device__ __forceinline__ void split(double v, float &hi, float &lo) {
@@ -268,6 +270,74 @@ __device__ __forceinline__ void finish(const BhkImageParams &p, const BhkImageOu
   if (o.carter_drift) o.carter_drift[pix] = (double)R.drift;
 }
 
+// The disk slab along one accepted step (camera rays of the RTE and Stokes
+// modes), from the step's start y0 + lo0, end R.y + R.lo, their derivatives k0,
+// k1 and Mino-time length h. Only the part of the step within 5 slab heights
+// of the equatorial plane is sampled: with z = r u taken linear over the step
+// that part is an interval of step fraction, widened by a tenth at either end;
+// a step whose ends lie on one side of the slab is skipped unless the cubic
+// Hermite bound on z lets it dip into it, and then sampled whole. The
+// interval's midpoints (16, or one per M of radius crossed if more, at most
+// 128) lie on the cubic Hermite interpolant of (r, u, psi). Each is a segment
+// of the reference's path length |d tau| / m. Returns true once the slab has
+// made the ray opaque.
+__device__ __forceinline__ bool vol_step(const BhkImageParams &p, const BhkVolume &v, RayMx &R, const Yf &y0,
+                                         const Lof &lo0, const Yf &k0, const Yf &k1, float h) {
+  if (!v.emit) return false;
+  const float r0 = y0.r + lo0.r, r1 = R.y.r + R.lo.r;
+  const float u0 = y0.u + lo0.u, u1 = R.y.u + R.lo.u;
+  const float inv_m = 1.0f / v.m;
+  const float rin = v.r_in * inv_m, rout = v.r_out * inv_m, zw = 5.0f * v.h * inv_m;
+  const float ah = fabsf(h);
+  const float slack_r = (4.0f / 27.0f) * ah * (fabsf(k0.r) + fabsf(k1.r));
+  if (fminf(r0, r1) - slack_r > 1.02f * rout || fmaxf(r0, r1) + slack_r < rin) return false;
+  const float z0 = r0 * u0, z1 = r1 * u1, dz = z1 - z0;
+  float fa = 0.0f, fb = 1.0f;
+  if (z0 * z1 > 0.0f && fminf(fabsf(z0), fabsf(z1)) > zw) {
+    const float dz0 = k0.r * u0 + r0 * k0.u, dz1 = k1.r * u1 + r1 * k1.u;
+    if (fminf(fabsf(z0), fabsf(z1)) - (4.0f / 27.0f) * ah * (fabsf(dz0) + fabsf(dz1)) > zw) return false;
+  } else if (fabsf(dz) > 1e-6f * zw) {
+    float f1 = (-zw - z0) / dz, f2 = (zw - z0) / dz;
+    if (f1 > f2) {
+      const float t = f1;
+      f1 = f2;
+      f2 = t;
+    }
+    const float pad = 0.1f * (f2 - f1);
+    fa = fmaxf(0.0f, f1 - pad);
+    fb = fminf(1.0f, f2 + pad);
+    if (!(fb > fa)) return false;
+  }
+  const int n = min(128, max(16, (int)ceilf(fabsf(r1 - r0) * (fb - fa))));
+  const float ds = ah * (fb - fa) / (float)n * inv_m;
+  const float psi0 = y0.phi + lo0.phi, psi1 = R.y.phi + R.lo.phi;
+  const float rp = (float)p.r_plus, rmn = (float)p.r_minus, ro = (float)p.r_obs;
+  const float gscale = p.a == 0.0 ? 0.0f : (float)p.a / (rp - rmn);
+  const float g_obs = (ro - rmn) / (ro - rp);
+  float c2b, s2b;
+  __sincosf(2.0f * v.b_angle, &s2b, &c2b);
+  for (int m = 0; m < n; ++m) {
+    const float t = fa + (fb - fa) * ((float)m + 0.5f) / (float)n;
+    const float t2 = t * t, t3 = t2 * t;
+    const float h00 = 2.0f * t3 - 3.0f * t2 + 1.0f, h10 = (t3 - 2.0f * t2 + t) * h;
+    const float h01 = 3.0f * t2 - 2.0f * t3, h11 = (t3 - t2) * h;
+    const float r = h00 * r0 + h10 * k0.r + h01 * r1 + h11 * k1.r;
+    if (!(r > rp)) continue;
+    const float u = fmaxf(-1.0f, fminf(1.0f, h00 * u0 + h10 * k0.u + h01 * u1 + h11 * k1.u));
+    const float psi = h00 * psi0 + h10 * k0.phi + h01 * psi1 + h11 * k1.phi;
+    const float phi = psi + gscale * __logf(__fdividef(r - rp, r - rmn) * g_obs);  // phi = psi + a (G(r) - G(r_obs))
+    float sp, cp;
+    __sincosf(phi, &sp, &cp);
+    const float rw = r * v.m, sw = rw * sqrtf(fmaxf(0.0f, (1.0f - u) * (1.0f + u)));
+    const float x = sw * (cp * v.cphi - sp * v.sphi), y = sw * (sp * v.cphi + cp * v.sphi), z = rw * u;
+    float col[3], rho;
+    const float j = bhvol::slab_emission(x, y, z, v.rs, v.r_in, v.r_out, v.h, col, rho);
+    if (j < 0.0f) continue;
+    if (bhvol::accum_segment(R.va, j, col, rho, ds, v.opacity, v.mode, c2b, s2b, v.ne_scale)) return true;
+  }
+  return false;
+}
+
 // Applies the increment d of an accepted step (acc) to the ray: compensated
 // positions, crossing test and record, projection; returns true if the ray
 // stops. A rejected attempt (acc false) runs the same instructions with a
@@ -280,9 +350,11 @@ __device__ __forceinline__ void finish(const BhkImageParams &p, const BhkImageOu
 // positive the radial turning point, with p_r linear over the step: at the
 // fraction s = -p_r0 / (p_r1 - p_r0) of it, r = r0 + p_r0 s h / 2, u and psi
 // interpolated linearly.
-template <bool TRACK = false>
+// VOL: also integrate the disk slab of vol over the step (needs k1).
+template <bool TRACK = false, bool VOL = false>
 __device__ __forceinline__ bool accept(const BhkImageParams &p, const BhkImageOut &o, RayMx &R, const Yf &d,
-                                       bool acc, float h, const Yf &k0, const Yf *k1) {
+                                       bool acc, float h, const Yf &k0, const Yf *k1,
+                                       const BhkVolume *vol = nullptr) {
   const Yf y0 = R.y;
   const Lof lo0 = R.lo;
   comp_add(R.y.r, R.lo.r, acc ? d.r : 0.0f);
@@ -309,6 +381,7 @@ __device__ __forceinline__ bool accept(const BhkImageParams &p, const BhkImageOu
     }
   }
   bool stop = false;
+  if (VOL && acc && k1) stop = vol_step(p, *vol, R, y0, lo0, k0, *k1, h);
   if (acc && (y0.u + lo0.u) * (R.y.u + R.lo.u) < 0.0f) {
     const Yf kk = k1 ? *k1 : rhs(R.y, R.c);
     const bhh_dev::Ends e{to_f64(y0.r, lo0.r),   to_f64(y0.u, lo0.u),   to_f64(y0.phi, lo0.phi),
@@ -319,15 +392,16 @@ __device__ __forceinline__ bool accept(const BhkImageParams &p, const BhkImageOu
                           (double)kk.phi};
     double r_c, phi_c;
     bhh_dev::hermite_crossing(e, (double)h, r_c, phi_c);
-    stop = on_crossing(p, o, R, r_c, phi_c);
+    stop = on_crossing(p, o, R, r_c, phi_c) || stop;
   }
   const float drift = project(R.y, R.lo, R.cd, R.drift_on);
   if (acc) R.drift = fmaxf(R.drift, drift);
   return stop;
 }
 
-template <int INTEG, bool TRACK = false>
-__device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOut &o, RayMx &R) {
+template <int INTEG, bool TRACK = false, bool VOL = false>
+__device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOut &o, RayMx &R,
+                                       const BhkVolume *vol = nullptr) {
   const float r_hor = R.r_hor, r_esc = R.r_esc;
   if (INTEG == 0) {
     if (R.steps >= p.max_steps) return 3;
@@ -337,7 +411,7 @@ __device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOu
     const float h = __fdividef(hh, fmaf(R.c.a2 * R.y.u, R.y.u, R.y.r * R.y.r));
     const Yf k0 = rhs(R.y, R.c);
     const Yf d = rk4_inc(R.y, h, R.c, k0);
-    return accept<TRACK>(p, o, R, d, true, h, k0, nullptr) ? 1 : -1;
+    return accept<TRACK, VOL>(p, o, R, d, true, h, k0, nullptr, vol) ? 1 : -1;
   } else {
     const long long max_attempts = 4LL * p.max_steps + 64;
     if (R.steps >= p.max_steps || R.attempts >= max_attempts) return 3;
@@ -347,7 +421,7 @@ __device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOu
     const DPf d = dp45(R.y, R.h, R.c, R.k1, R.rtol, R.atol, true);
     const bool acc = d.err <= 1.0f;
     const float h = R.h;
-    const bool stop = accept<TRACK>(p, o, R, d.d, acc, h, R.k1, &d.k7);
+    const bool stop = accept<TRACK, VOL>(p, o, R, d.d, acc, h, R.k1, &d.k7, vol);
     R.k1 = acc ? d.k7 : R.k1;
     R.k1.r = R.y.pr;  // projection moved only the momenta
     R.k1.u = R.y.pu;
@@ -382,6 +456,43 @@ struct tracks_closest<CameraSrc> {
   static constexpr bool value = true;
 };
 
+// A camera frame whose rays also integrate the disk slab (RTE and Stokes modes).
+struct CameraVolSrc : CameraSrc {
+  const BhkVolume &vol;
+};
+template <>
+struct tracks_closest<CameraVolSrc> {
+  static constexpr bool value = true;
+};
+template <class Src>
+struct has_volume {
+  static constexpr bool value = false;
+};
+template <>
+struct has_volume<CameraVolSrc> {
+  static constexpr bool value = true;
+};
+template <class Src>
+__device__ __forceinline__ const BhkVolume *volume_of(const Src &) {
+  return nullptr;
+}
+__device__ __forceinline__ const BhkVolume *volume_of(const CameraVolSrc &src) { return &src.vol; }
+
+// The slab's totals of a finished ray: [8][n] r, g, b, transmittance, Q, U, V,
+// 1 if the slab made it opaque.
+__device__ __forceinline__ void write_vol(const BhkImageParams &p, const BhkImageOut &o, const RayMx &R, bool opaque) {
+  if (!o.vol) return;
+  const long long n = p.n_pix, i = R.pix;
+  o.vol[i] = R.va.rgb[0];
+  o.vol[n + i] = R.va.rgb[1];
+  o.vol[2 * n + i] = R.va.rgb[2];
+  o.vol[3 * n + i] = R.va.T;
+  o.vol[4 * n + i] = R.va.s.q;
+  o.vol[5 * n + i] = R.va.s.u;
+  o.vol[6 * n + i] = R.va.s.v;
+  o.vol[7 * n + i] = opaque ? 1.0f : 0.0f;
+}
+
 __device__ __forceinline__ void write_closest(const BhkImageParams &p, const BhkImageOut &o, const RayMx &R) {
   if (!o.closest) return;
   o.closest[R.pix] = R.cl_r;
@@ -399,6 +510,10 @@ __device__ __forceinline__ void init_from(const CameraSrc &src, int, long long p
   R.cl_r = R.y.r + R.lo.r;
   R.cl_u = R.y.u;
   R.cl_psi = 0.0f;
+}
+__device__ __forceinline__ void init_from(const CameraVolSrc &src, int f, long long pix, RayMx &R) {
+  init_from(static_cast<const CameraSrc &>(src), f, pix, R);
+  bhvol::accum_init(R.va);
 }
 
 // The persistent loop shared by the single-frame and batch kernels (see
@@ -436,9 +551,11 @@ __device__ __forceinline__ void trace_loop(const Src &src, unsigned long long *_
     for (int k = 0; k < refill; ++k) {
       if (active) {
         const BhkImageParams &P = src.params(R.f);
-        const int cls = iterate<INTEG, tracks_closest<Src>::value>(P, src.out(R.f), R);
+        const int cls =
+            iterate<INTEG, tracks_closest<Src>::value, has_volume<Src>::value>(P, src.out(R.f), R, volume_of(src));
         if (cls >= 0) {
           if (tracks_closest<Src>::value) write_closest(P, src.out(R.f), R);
+          if (has_volume<Src>::value) write_vol(P, src.out(R.f), R, cls == 1);
           finish(P, src.out(R.f), R, cls);
           src.pixel_done(R.f);
           active = false;
@@ -469,6 +586,14 @@ __global__ void __launch_bounds__(128) k_trace_camera_mixed(const __grid_constan
                                                             const __grid_constant__ BhkImageOut o,
                                                             unsigned long long *__restrict__ counter, int refill) {
   trace_loop<1>(CameraSrc{p, cam, o}, counter, refill);
+}
+
+__global__ void __launch_bounds__(128) k_trace_camera_vol_mixed(const __grid_constant__ BhkImageParams p,
+                                                                const __grid_constant__ BhkCamera cam,
+                                                                const __grid_constant__ BhkVolume vol,
+                                                                const __grid_constant__ BhkImageOut o,
+                                                                unsigned long long *__restrict__ counter, int refill) {
+  trace_loop<1>(CameraVolSrc{{p, cam, o}, vol}, counter, refill);
 }
 
 template <int INTEG>
@@ -638,10 +763,13 @@ extern "C" int bhk_trace_list_mixed(const BhkImageParams *p, const BhkImageOut *
 }
 
 extern "C" int bhk_trace_camera_mixed(const BhkImageParams *p, const BhkCamera *cam, const BhkImageOut *o,
-                                      unsigned long long *counter, BhkLaunch L, void *stream) {
+                                      unsigned long long *counter, BhkLaunch L, void *stream, const BhkVolume *vol) {
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s) != cudaSuccess) return -1;
-  bhm::k_trace_camera_mixed<<<L.grid, L.block, 0, s>>>(*p, *cam, *o, counter, L.refill);
+  if (vol && (vol->mode == 1 || vol->mode == 2))
+    bhm::k_trace_camera_vol_mixed<<<L.grid, L.block, 0, s>>>(*p, *cam, *vol, *o, counter, L.refill);
+  else
+    bhm::k_trace_camera_mixed<<<L.grid, L.block, 0, s>>>(*p, *cam, *o, counter, L.refill);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

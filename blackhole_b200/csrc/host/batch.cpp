@@ -118,7 +118,7 @@ BH_KerrBatch *bh_kerr_batch_create(const BH_KerrScene *scenes, const BH_KerrImag
     }
     const BH_KerrImageOut &o = outs[i];
     b->frames[i].o = BhkImageOut{o.cls, o.steps, o.n_cross, o.r_hit, o.phi_hit, o.g, o.flux, o.intensity,
-                                 o.theta_inf, o.phi_inf, nullptr, nullptr, o.carter_drift};
+                                 o.theta_inf, o.phi_inf, nullptr, nullptr, o.carter_drift, nullptr};
     if (i > 0 && (scenes[i].integrator != scenes[0].integrator || scenes[i].precision != scenes[0].precision)) {
       fail_msg("frame %d: all frames of a batch must share integrator and precision", i);
       return nullptr;

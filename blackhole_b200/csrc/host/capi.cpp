@@ -293,7 +293,7 @@ int bh_kerr_trace_image(const BH_KerrScene *scene, const BH_KerrImageOut *out, v
   DeviceScratch *ds = nullptr;
   if (device_scratch(&ds) != 0) return -1;
   const BhkImageOut o{out->cls,   out->steps,     out->n_cross,   out->r_hit,     out->phi_hit,
-                      out->g,     out->flux,      out->intensity, out->theta_inf, out->phi_inf, nullptr, nullptr, out->carter_drift};
+                      out->g,     out->flux,      out->intensity, out->theta_inf, out->phi_inf, nullptr, nullptr, out->carter_drift, nullptr};
   return bhh_launch_image(&p, &o, ds->counter, L, stream, nullptr);
 }
 

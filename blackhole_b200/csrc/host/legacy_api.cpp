@@ -101,6 +101,7 @@ struct Scratch {
   double *phi_hit = nullptr, *theta_inf = nullptr, *phi_inf = nullptr;
   float *esc_dir = nullptr;
   float *closest = nullptr;
+  float *vol = nullptr;  // [8][n] the slab of the RTE and Stokes modes
   unsigned long long *counter = nullptr;
   float *post = nullptr;  // bloom planes and composite of bhb_cuda_postprocess
   int64_t post_cap = 0;
@@ -129,8 +130,9 @@ int scratch(int64_t n, Scratch **out) {
     s.base = nullptr;
     s.cap = 0;
     const size_t b_cls = up256(size_t(n) * 4), b_d = up256(size_t(n) * 8), b_dir = up256(size_t(n) * 12);
+    const size_t b_vol = up256(size_t(n) * 32);
     char *p = nullptr;
-    if (int rc = cuda_check(bhh_malloc((&p), b_cls + 6 * b_d + 2 * b_dir + 256),
+    if (int rc = cuda_check(bhh_malloc((&p), b_cls + 6 * b_d + 2 * b_dir + b_vol + 256),
                             "cudaMalloc(legacy scratch)"))
       return rc;
     s.base = p;
@@ -145,7 +147,8 @@ int scratch(int64_t n, Scratch **out) {
     s.phi_inf = d + 5 * nd;
     s.esc_dir = reinterpret_cast<float *>(p + b_cls + 6 * b_d);
     s.closest = reinterpret_cast<float *>(p + b_cls + 6 * b_d + b_dir);
-    s.counter = reinterpret_cast<unsigned long long *>(p + b_cls + 6 * b_d + 2 * b_dir);
+    s.vol = reinterpret_cast<float *>(p + b_cls + 6 * b_d + 2 * b_dir);
+    s.counter = reinterpret_cast<unsigned long long *>(p + b_cls + 6 * b_d + 2 * b_dir + b_vol);
     s.cap = n;
   }
   *out = &s;
@@ -254,6 +257,27 @@ int render(void *fb, const BH_LaunchParams *lp, int variant, cudaStream_t st) {
   BhkLaunch L;
   if (launch_shape(*sc, n, &L) != 0) return -1;
   const bool look = shading_mode() == BH_SHADING_REFERENCE;
+  // The reference's RTE and Stokes modes (Stokes first), which it traces only
+  // for a spinning hole; otherwise its single-scatter look
+  // (src/cuda/kernels_fp32.cu:47-70, device_physics.cuh:2037-2046).
+  BhkVolume vol{};
+  const bool kerr = lp->kerr_enabled && std::fabs(0.5f * lp->spin * lp->rs) >= 1e-6f;
+  vol.mode = (look && kerr) ? (lp->stokes_enabled ? 2 : (lp->rte_enabled ? 1 : 0)) : 0;
+  if (vol.mode) {
+    vol.emit = lp->adisk_enabled;
+    vol.m = 0.5f * lp->rs;
+    vol.rs = lp->rs;
+    vol.r_in = lp->isco;
+    vol.r_out = 100.0f * lp->rs;
+    vol.h = std::max(0.1f * lp->rs, 1e-6f);
+    vol.opacity = lp->rte_opacity_scale;
+    vol.b_angle = lp->stokes_b_field_angle;
+    vol.ne_scale = lp->stokes_ne_scale;
+    vol.cphi = float(job.cam.cphi);
+    vol.sphi = float(job.cam.sphi);
+    job.p.r_out = 0.0;  // the disk is the slab: no opaque crossing
+    job.p.r_in = 1.0;
+  }
   BhkImageOut o{};
   o.cls = sc->cls;
   o.r_hit = sc->r_hit;
@@ -262,12 +286,13 @@ int render(void *fb, const BH_LaunchParams *lp, int variant, cudaStream_t st) {
     o.theta_inf = sc->theta_inf;
     o.phi_inf = sc->phi_inf;
     o.closest = sc->closest;
+    if (vol.mode) o.vol = sc->vol;
   } else {
     o.g = sc->g;
     o.flux = sc->flux;
     o.esc_dir = sc->esc_dir;
   }
-  if (bhk_trace_camera_mixed(&job.p, &job.cam, &o, sc->counter, L, st) != 0)
+  if (bhk_trace_camera_mixed(&job.p, &job.cam, &o, sc->counter, L, st, vol.mode ? &vol : nullptr) != 0)
     return cuda_check(cudaGetLastError(), "k_trace_camera_mixed launch");
   if (look) {
     BhkLook lk{};
@@ -286,6 +311,7 @@ int render(void *fb, const BH_LaunchParams *lp, int variant, cudaStream_t st) {
     lk.redshift_enabled = lp->redshift_enabled;
     lk.use_luts = lp->use_luts;
     lk.background_enabled = lp->background_enabled;
+    lk.vol_mode = vol.mode;
     lk.adisk_lit = lp->adisk_lit;
     lk.doppler_strength = lp->doppler_strength;
     lk.bg_intensity = lp->background_intensity;
@@ -312,7 +338,7 @@ int render(void *fb, const BH_LaunchParams *lp, int variant, cudaStream_t st) {
     lk.tex_grmhd = g_lut[5];
     lk.tex_grmhd_right = g_lut[7];
     lk.tex_equirect = g_equirect;
-    if (bhk_legacy_look(&lk, sc->cls, sc->r_hit, sc->phi_hit, sc->theta_inf, sc->phi_inf, sc->closest,
+    if (bhk_legacy_look(&lk, sc->cls, sc->r_hit, sc->phi_hit, sc->theta_inf, sc->phi_inf, sc->closest, sc->vol,
                         static_cast<float *>(fb), st) != 0)
       return cuda_check(cudaGetLastError(), "k_legacy_look launch");
     return 0;
@@ -544,6 +570,15 @@ int bh_legacy_set_shading(int mode) {
                     mode);
   std::lock_guard<std::mutex> lock(g_mu);
   g_shading = mode;
+  return 0;
+}
+
+int bh_stokes_steps(long long n, const float *state, const float *coef, float *out, void *stream) {
+  if (n < 0) return fail_msg("bh_stokes_steps: n must be >= 0, got %lld", (long long)n);
+  if (n > 0 && (!state || !coef || !out)) return fail_msg("bh_stokes_steps: state, coef and out must be non-NULL");
+  if (reinterpret_cast<uintptr_t>(state) % 16 || reinterpret_cast<uintptr_t>(out) % 16)
+    return fail_msg("bh_stokes_steps: state and out must be 16-byte aligned");
+  if (bhk_stokes_steps(n, state, coef, out, stream) != 0) return cuda_check(cudaGetLastError(), "k_stokes_steps launch");
   return 0;
 }
 

@@ -83,7 +83,7 @@ int bh_kerr_trace_image_sky(const BH_KerrScene* scene, const BH_KerrImageOut* ou
   unsigned long long* counter = nullptr;
   if (bhh_work_counter(&counter) != 0) return -1;
   const BhkImageOut o{out->cls,   out->steps,     out->n_cross,   out->r_hit,     out->phi_hit,
-                      out->g,     out->flux,      out->intensity, out->theta_inf, out->phi_inf, nullptr, nullptr, out->carter_drift};
+                      out->g,     out->flux,      out->intensity, out->theta_inf, out->phi_inf, nullptr, nullptr, out->carter_drift, nullptr};
   return bhh_launch_image(&p, &o, counter, L, stream, nullptr);
 }
 

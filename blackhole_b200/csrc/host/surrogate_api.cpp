@@ -496,7 +496,7 @@ int bh_surrogate_trace_image(BH_Surrogate *s, const BH_KerrScene *scene, const B
   if (int rc = cuda_check(cudaMemsetAsync(s->r_counts, 0, 8 * sizeof(unsigned int), st), "cudaMemsetAsync"))
     return rc;
   const BhkImageOut o{out->cls,   out->steps,     out->n_cross,   out->r_hit,     out->phi_hit,
-                      out->g,     out->flux,      out->intensity, out->theta_inf, out->phi_inf, nullptr, nullptr, out->carter_drift};
+                      out->g,     out->flux,      out->intensity, out->theta_inf, out->phi_inf, nullptr, nullptr, out->carter_drift, nullptr};
   if (!s->side) {
     if (int rc = cuda_check(cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking), "cudaStreamCreate")) return rc;
     for (cudaEvent_t &e : s->ev)

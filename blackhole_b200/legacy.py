@@ -145,6 +145,7 @@ def _declare(lib: C.CDLL) -> C.CDLL:
     lib.bhb_cuda_postprocess.argtypes = [vp, i, i, f, f, f, f]
     lib.bh_legacy_set_shading.argtypes = [i]
     lib.bh_legacy_get_shading.argtypes = []
+    lib.bh_stokes_steps.argtypes = [C.c_int64, vp, vp, vp, vp]
     lib._legacy_declared = True
     return lib
 
@@ -164,6 +165,23 @@ def set_shading(mode: int) -> None:
 
 def get_shading() -> int:
     return int(library().bh_legacy_get_shading())
+
+
+def stokes_steps(state, coef, stream=None):
+    """bh_stokes_steps: one exact polarized transfer step for each row of
+    ``state`` [n, 4] (I, Q, U, V) with ``coef`` [n, 7] (jI, jQ, jU, jV,
+    alpha_I, rho_V, ds); contiguous float32 CUDA tensors. Returns [n, 4]."""
+    import torch
+
+    if state.dtype != torch.float32 or coef.dtype != torch.float32 or not state.is_cuda or not coef.is_cuda:
+        raise TypeError("state and coef must be float32 CUDA tensors")
+    if state.dim() != 2 or state.shape[1] != 4 or coef.shape != (state.shape[0], 7):
+        raise ValueError("state must be [n, 4] and coef [n, 7]")
+    state, coef = state.contiguous(), coef.contiguous()
+    out = torch.empty_like(state)
+    s = stream.cuda_stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    check(library().bh_stokes_steps(state.shape[0], state.data_ptr(), coef.data_ptr(), out.data_ptr(), s))
+    return out
 
 
 def launch(params: LaunchParams, framebuffer, variant: int = -1, stream=None) -> None:

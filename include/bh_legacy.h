@@ -144,6 +144,18 @@ enum BH_Shading { BH_SHADING_REFERENCE = 0, BH_SHADING_PHYSICAL = 1 };
 int bh_legacy_set_shading(int mode);
 int bh_legacy_get_shading(void);
 
+/* The polarized transfer step of the render calls' Stokes mode
+ * (stokes_enabled; replaces d_stokes_step, src/cuda/device_physics.cuh:
+ * 2216-2284), on n independent states at once, on the GPU. Device arrays:
+ * state [n][4] (I, Q, U, V), coef [n][7] (jI, jQ, jU, jV, alpha_I, rho_V, ds),
+ * out [n][4]. The step is the exact solution over ds of
+ *   dI/ds = jI - alpha_I I,  dV/ds = jV - alpha_I V,
+ *   d(Q, U)/ds = (jQ, jU) - alpha_I (Q, U) + rho_V (-U, Q)
+ * (absorption alpha_I on every channel, Faraday rotation rho_V of Q into U),
+ * in FP32; ds <= 0 leaves the state unchanged, alpha_I < 0 counts as 0.
+ * Asynchronous on `stream`; -1 on NULL arrays or n < 0. */
+int bh_stokes_steps(long long n, const float *state, const float *coef, float *out, void *stream);
+
 /* BH_KERNEL_FP32_BASELINE (kernel_launch.h:156). */
 int bh_select_kernel_variant(void);
 
