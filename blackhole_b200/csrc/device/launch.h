@@ -79,7 +79,7 @@ typedef struct BhkBatchDev {
   unsigned long long *start_ns;    // [1] earliest %globaltimer at which a CTA started
   long long n_total;               // sum of the frames' pixels
   int32_t n_frames;
-  int32_t pad;
+  int32_t drift;                   // some frame asks for carter_drift
 } BhkBatchDev;
 
 // Persistent batch tracers (all frames share integrator and precision).

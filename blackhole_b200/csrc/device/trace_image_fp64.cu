@@ -133,7 +133,9 @@ __device__ __forceinline__ void finish(const BhkImageParams &p, const BhkImageOu
 
 // One iteration of the trace loop for an active ray; returns the class when
 // the ray terminates, -1 otherwise.
-template <int INTEG>
+// DRIFT: keep the largest Carter-constant residual the projection removes (a
+// separate instantiation, so the plain kernels carry none of it).
+template <int INTEG, bool DRIFT = false>
 __device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOut &o, RayFp64 &R) {
   if (INTEG == 0) {
     if (R.steps >= p.max_steps) return 3;
@@ -150,7 +152,10 @@ __device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOu
       step_crossing(R.y, k0, yn, rhs(yn, R.c), h, r_c, phi_c);
       if (on_crossing(p, o, R, r_c, phi_c)) return 1;
     }
-    R.drift = dmax_(R.drift, project(yn, R.c, o.carter_drift != nullptr));
+    if (DRIFT)
+      R.drift = dmax_(R.drift, project(yn, R.c, true));
+    else
+      project(yn, R.c);
     R.y = yn;
     return -1;
   } else {
@@ -175,8 +180,8 @@ __device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOu
     }
     R.y = acc ? d.y5 : R.y;
     R.k1 = acc ? d.k7 : R.k1;
-    const double drift = project(R.y, R.c, o.carter_drift != nullptr);
-    if (acc) R.drift = dmax_(R.drift, drift);
+    const double drift = project(R.y, R.c, DRIFT);
+    if (DRIFT && acc) R.drift = dmax_(R.drift, drift);
     R.k1.r = R.y.pr;  // projection moves only the momenta
     R.k1.u = R.y.pu;
     R.h = R.h * step_factor(d.err, acc);
@@ -187,7 +192,7 @@ __device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOu
 // The persistent loop shared by the single-frame and batch kernels. Every
 // `refill` integration steps, the lanes whose ray finished take new work
 // items with one warp-aggregated atomicAdd on the counter (ballot + popc).
-template <int INTEG, class Src>
+template <int INTEG, bool DRIFT = false, class Src>
 __device__ __forceinline__ void trace_loop(const Src &src, unsigned long long *__restrict__ counter, int refill) {
   const unsigned lane = threadIdx.x & 31u;
   const unsigned lanemask_lt = (1u << lane) - 1u;
@@ -219,7 +224,7 @@ __device__ __forceinline__ void trace_loop(const Src &src, unsigned long long *_
     for (int k = 0; k < refill; ++k) {
       if (active) {
         const BhkImageParams &P = src.params(R.f);
-        const int cls = iterate<INTEG>(P, src.out(R.f), R);
+        const int cls = iterate<INTEG, DRIFT>(P, src.out(R.f), R);
         if (cls >= 0) {
           finish(P, src.out(R.f), R, cls);
           src.pixel_done(R.f);
@@ -230,27 +235,27 @@ __device__ __forceinline__ void trace_loop(const Src &src, unsigned long long *_
   }
 }
 
-template <int INTEG>
+template <int INTEG, bool DRIFT>
 __global__ void __launch_bounds__(128, 4) k_trace_image_fp64(const __grid_constant__ BhkImageParams p,
                                                           const __grid_constant__ BhkImageOut o,
                                                           unsigned long long *__restrict__ counter, int refill) {
-  trace_loop<INTEG>(bhsrc::SingleSrc{p, o}, counter, refill);
+  trace_loop<INTEG, DRIFT>(bhsrc::SingleSrc{p, o}, counter, refill);
 }
 
-template <int INTEG>
+template <int INTEG, bool DRIFT>
 __global__ void __launch_bounds__(128, 4) k_trace_list_fp64(const __grid_constant__ BhkImageParams p,
                                                          const __grid_constant__ BhkImageOut o,
                                                          const int *__restrict__ list,
                                                          const unsigned int *__restrict__ count,
                                                          unsigned long long *__restrict__ counter, int refill) {
-  trace_loop<INTEG>(bhsrc::ListSrc{p, o, list, count}, counter, refill);
+  trace_loop<INTEG, DRIFT>(bhsrc::ListSrc{p, o, list, count}, counter, refill);
 }
 
-template <int INTEG>
+template <int INTEG, bool DRIFT>
 __global__ void __launch_bounds__(128, 4) k_trace_batch_fp64(const __grid_constant__ BhkBatchDev b,
                                                           unsigned long long *__restrict__ counter, int refill) {
   if (threadIdx.x == 0) atomicMin(b.start_ns, bhsrc::globaltimer_ns());
-  trace_loop<INTEG>(bhsrc::BatchSrc{b}, counter, refill);
+  trace_loop<INTEG, DRIFT>(bhsrc::BatchSrc{b}, counter, refill);
 }
 
 // ---- along-ray radiative transfer -------------------------------------------
@@ -371,10 +376,10 @@ extern "C" int bhk_trace_image_fp64(const BhkImageParams *p, const BhkImageOut *
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s);
   if (e != cudaSuccess) return set_err(e, "work-counter reset");
-  if (p->integrator == 0)
-    bhk::k_trace_image_fp64<0><<<launch.grid, launch.block, 0, s>>>(*p, *o, counter, launch.refill);
-  else
-    bhk::k_trace_image_fp64<1><<<launch.grid, launch.block, 0, s>>>(*p, *o, counter, launch.refill);
+  const bool drift = o->carter_drift != nullptr;
+  auto k = p->integrator == 0 ? (drift ? bhk::k_trace_image_fp64<0, true> : bhk::k_trace_image_fp64<0, false>)
+                              : (drift ? bhk::k_trace_image_fp64<1, true> : bhk::k_trace_image_fp64<1, false>);
+  k<<<launch.grid, launch.block, 0, s>>>(*p, *o, counter, launch.refill);
   e = cudaGetLastError();
   if (e != cudaSuccess) return set_err(e, "k_trace_image_fp64 launch");
   return 0;
@@ -386,10 +391,10 @@ extern "C" int bhk_trace_list_fp64(const BhkImageParams *p, const BhkImageOut *o
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s);
   if (e != cudaSuccess) return set_err(e, "work-counter reset");
-  if (p->integrator == 0)
-    bhk::k_trace_list_fp64<0><<<L.grid, L.block, 0, s>>>(*p, *o, list, count, counter, L.refill);
-  else
-    bhk::k_trace_list_fp64<1><<<L.grid, L.block, 0, s>>>(*p, *o, list, count, counter, L.refill);
+  const bool drift = o->carter_drift != nullptr;
+  auto k = p->integrator == 0 ? (drift ? bhk::k_trace_list_fp64<0, true> : bhk::k_trace_list_fp64<0, false>)
+                              : (drift ? bhk::k_trace_list_fp64<1, true> : bhk::k_trace_list_fp64<1, false>);
+  k<<<L.grid, L.block, 0, s>>>(*p, *o, list, count, counter, L.refill);
   e = cudaGetLastError();
   if (e != cudaSuccess) return set_err(e, "k_trace_list_fp64 launch");
   return 0;
@@ -397,9 +402,9 @@ extern "C" int bhk_trace_list_fp64(const BhkImageParams *p, const BhkImageOut *o
 
 extern "C" int bhk_trace_image_fp64_occupancy(int integrator, int block, int *blocks_per_sm) {
   cudaError_t e = (integrator == 0)
-                      ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhk::k_trace_image_fp64<0>,
+                      ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhk::k_trace_image_fp64<0, false>,
                                                                       block, 0)
-                      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhk::k_trace_image_fp64<1>,
+                      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhk::k_trace_image_fp64<1, false>,
                                                                       block, 0);
   if (e != cudaSuccess) return set_err(e, "occupancy query");
   return 0;
@@ -410,10 +415,9 @@ extern "C" int bhk_trace_batch_fp64(const BhkBatchDev *b, int integrator, unsign
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s);
   if (e != cudaSuccess) return set_err(e, "work-counter reset");
-  if (integrator == 0)
-    bhk::k_trace_batch_fp64<0><<<L.grid, L.block, 0, s>>>(*b, counter, L.refill);
-  else
-    bhk::k_trace_batch_fp64<1><<<L.grid, L.block, 0, s>>>(*b, counter, L.refill);
+  auto k = integrator == 0 ? (b->drift ? bhk::k_trace_batch_fp64<0, true> : bhk::k_trace_batch_fp64<0, false>)
+                           : (b->drift ? bhk::k_trace_batch_fp64<1, true> : bhk::k_trace_batch_fp64<1, false>);
+  k<<<L.grid, L.block, 0, s>>>(*b, counter, L.refill);
   e = cudaGetLastError();
   if (e != cudaSuccess) return set_err(e, "k_trace_batch_fp64 launch");
   return 0;
@@ -421,9 +425,9 @@ extern "C" int bhk_trace_batch_fp64(const BhkBatchDev *b, int integrator, unsign
 
 extern "C" int bhk_trace_batch_fp64_occupancy(int integrator, int block, int *blocks_per_sm) {
   cudaError_t e = (integrator == 0)
-                      ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhk::k_trace_batch_fp64<0>,
+                      ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhk::k_trace_batch_fp64<0, false>,
                                                                       block, 0)
-                      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhk::k_trace_batch_fp64<1>,
+                      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhk::k_trace_batch_fp64<1, false>,
                                                                       block, 0);
   if (e != cudaSuccess) return set_err(e, "occupancy query");
   return 0;

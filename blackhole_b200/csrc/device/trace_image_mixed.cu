@@ -49,7 +49,6 @@ struct RayMx {
   int ncross;
   float cl_r, cl_u, cl_psi;  // closest approach so far (camera rays only)
   float drift;               // largest Carter-constant residual the projection removed
-  bool drift_on;             // the caller asked for carter_drift (read once per ray)
   bhvol::Accum va;           // disk slab seen so far (camera rays of the volumetric modes)
 };
 
@@ -100,7 +99,6 @@ __device__ __forceinline__ void init_ray(const BhkImageParams &p, long long pix,
   R.atol = (float)p.atol;
   project(R.y, R.lo, R.cd);  // idempotent from here on (see iterate)
   R.drift = 0.0f;
-  R.drift_on = false;
   const float hh = (float)p.step_coeff * fminf(R.y.r, (float)p.step_rcap);
   R.h = hh / fmaf(R.c.a2 * R.y.u, R.y.u, R.y.r * R.y.r);
   R.k1 = rhs(R.y, R.c);
@@ -180,7 +178,6 @@ __device__ __forceinline__ void init_ray_camera(const BhkImageParams &p, const B
   R.atol = (float)p.atol;
   project(R.y, R.lo, R.cd);
   R.drift = 0.0f;
-  R.drift_on = false;
   const float hh = (float)p.step_coeff * fminf(R.y.r, (float)p.step_rcap);
   R.h = hh / fmaf(R.c.a2 * R.y.u, R.y.u, R.y.r * R.y.r);
   R.k1 = rhs(R.y, R.c);
@@ -351,7 +348,9 @@ __device__ __forceinline__ bool vol_step(const BhkImageParams &p, const BhkVolum
 // fraction s = -p_r0 / (p_r1 - p_r0) of it, r = r0 + p_r0 s h / 2, u and psi
 // interpolated linearly.
 // VOL: also integrate the disk slab of vol over the step (needs k1).
-template <bool TRACK = false, bool VOL = false>
+// DRIFT: keep the largest Carter-constant residual the projection removes (a
+// separate instantiation, so the plain kernels carry none of it).
+template <bool TRACK = false, bool VOL = false, bool DRIFT = false>
 __device__ __forceinline__ bool accept(const BhkImageParams &p, const BhkImageOut &o, RayMx &R, const Yf &d,
                                        bool acc, float h, const Yf &k0, const Yf *k1,
                                        const BhkVolume *vol = nullptr) {
@@ -394,12 +393,12 @@ __device__ __forceinline__ bool accept(const BhkImageParams &p, const BhkImageOu
     bhh_dev::hermite_crossing(e, (double)h, r_c, phi_c);
     stop = on_crossing(p, o, R, r_c, phi_c) || stop;
   }
-  const float drift = project(R.y, R.lo, R.cd, R.drift_on);
-  if (acc) R.drift = fmaxf(R.drift, drift);
+  const float drift = project(R.y, R.lo, R.cd, DRIFT);
+  if (DRIFT && acc) R.drift = fmaxf(R.drift, drift);
   return stop;
 }
 
-template <int INTEG, bool TRACK = false, bool VOL = false>
+template <int INTEG, bool TRACK = false, bool VOL = false, bool DRIFT = false>
 __device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOut &o, RayMx &R,
                                        const BhkVolume *vol = nullptr) {
   const float r_hor = R.r_hor, r_esc = R.r_esc;
@@ -411,7 +410,7 @@ __device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOu
     const float h = __fdividef(hh, fmaf(R.c.a2 * R.y.u, R.y.u, R.y.r * R.y.r));
     const Yf k0 = rhs(R.y, R.c);
     const Yf d = rk4_inc(R.y, h, R.c, k0);
-    return accept<TRACK, VOL>(p, o, R, d, true, h, k0, nullptr, vol) ? 1 : -1;
+    return accept<TRACK, VOL, DRIFT>(p, o, R, d, true, h, k0, nullptr, vol) ? 1 : -1;
   } else {
     const long long max_attempts = 4LL * p.max_steps + 64;
     if (R.steps >= p.max_steps || R.attempts >= max_attempts) return 3;
@@ -421,7 +420,7 @@ __device__ __forceinline__ int iterate(const BhkImageParams &p, const BhkImageOu
     const DPf d = dp45(R.y, R.h, R.c, R.k1, R.rtol, R.atol, true);
     const bool acc = d.err <= 1.0f;
     const float h = R.h;
-    const bool stop = accept<TRACK, VOL>(p, o, R, d.d, acc, h, R.k1, &d.k7, vol);
+    const bool stop = accept<TRACK, VOL, DRIFT>(p, o, R, d.d, acc, h, R.k1, &d.k7, vol);
     R.k1 = acc ? d.k7 : R.k1;
     R.k1.r = R.y.pr;  // projection moved only the momenta
     R.k1.u = R.y.pu;
@@ -518,7 +517,7 @@ __device__ __forceinline__ void init_from(const CameraVolSrc &src, int f, long l
 
 // The persistent loop shared by the single-frame and batch kernels (see
 // trace_image_fp64.cu).
-template <int INTEG, class Src>
+template <int INTEG, bool DRIFT = false, class Src>
 __device__ __forceinline__ void trace_loop(const Src &src, unsigned long long *__restrict__ counter, int refill) {
   const unsigned lane = threadIdx.x & 31u;
   const unsigned lanemask_lt = (1u << lane) - 1u;
@@ -540,7 +539,6 @@ __device__ __forceinline__ void trace_loop(const Src &src, unsigned long long *_
           const int f = src.frame_of((long long)mine, pix);
           init_from(src, f, pix, R);
           R.f = f;
-          R.drift_on = src.out(f).carter_drift != nullptr;
           active = true;
         } else {
           exhausted = true;
@@ -552,7 +550,8 @@ __device__ __forceinline__ void trace_loop(const Src &src, unsigned long long *_
       if (active) {
         const BhkImageParams &P = src.params(R.f);
         const int cls =
-            iterate<INTEG, tracks_closest<Src>::value, has_volume<Src>::value>(P, src.out(R.f), R, volume_of(src));
+            iterate<INTEG, tracks_closest<Src>::value, has_volume<Src>::value, DRIFT>(P, src.out(R.f), R,
+                                                                                     volume_of(src));
         if (cls >= 0) {
           if (tracks_closest<Src>::value) write_closest(P, src.out(R.f), R);
           if (has_volume<Src>::value) write_vol(P, src.out(R.f), R, cls == 1);
@@ -565,20 +564,20 @@ __device__ __forceinline__ void trace_loop(const Src &src, unsigned long long *_
   }
 }
 
-template <int INTEG>
+template <int INTEG, bool DRIFT>
 __global__ void __launch_bounds__(128, 4) k_trace_image_mixed(const __grid_constant__ BhkImageParams p,
                                                            const __grid_constant__ BhkImageOut o,
                                                            unsigned long long *__restrict__ counter, int refill) {
-  trace_loop<INTEG>(bhsrc::SingleSrc{p, o}, counter, refill);
+  trace_loop<INTEG, DRIFT>(bhsrc::SingleSrc{p, o}, counter, refill);
 }
 
-template <int INTEG>
+template <int INTEG, bool DRIFT>
 __global__ void __launch_bounds__(128, 4) k_trace_list_mixed(const __grid_constant__ BhkImageParams p,
                                                           const __grid_constant__ BhkImageOut o,
                                                           const int *__restrict__ list,
                                                           const unsigned int *__restrict__ count,
                                                           unsigned long long *__restrict__ counter, int refill) {
-  trace_loop<INTEG>(bhsrc::ListSrc{p, o, list, count}, counter, refill);
+  trace_loop<INTEG, DRIFT>(bhsrc::ListSrc{p, o, list, count}, counter, refill);
 }
 
 __global__ void __launch_bounds__(128) k_trace_camera_mixed(const __grid_constant__ BhkImageParams p,
@@ -596,11 +595,11 @@ __global__ void __launch_bounds__(128) k_trace_camera_vol_mixed(const __grid_con
   trace_loop<1>(CameraVolSrc{{p, cam, o}, vol}, counter, refill);
 }
 
-template <int INTEG>
-__global__ void __launch_bounds__(128, 4) k_trace_batch_mixed(const __grid_constant__ BhkBatchDev b,
+template <int INTEG, bool DRIFT>
+__global__ void __launch_bounds__(128) k_trace_batch_mixed(const __grid_constant__ BhkBatchDev b,
                                                            unsigned long long *__restrict__ counter, int refill) {
   if (threadIdx.x == 0) atomicMin(b.start_ns, bhsrc::globaltimer_ns());
-  trace_loop<INTEG>(bhsrc::BatchSrc{b}, counter, refill);
+  trace_loop<INTEG, DRIFT>(bhsrc::BatchSrc{b}, counter, refill);
 }
 
 // ---- along-ray transfer on the mixed tracer ---------------------------------------
@@ -735,18 +734,18 @@ extern "C" int bhk_trace_image_mixed(const BhkImageParams *p, const BhkImageOut 
                                      BhkLaunch launch, void *stream) {
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s) != cudaSuccess) return -1;
-  if (p->integrator == 0)
-    bhm::k_trace_image_mixed<0><<<launch.grid, launch.block, 0, s>>>(*p, *o, counter, launch.refill);
-  else
-    bhm::k_trace_image_mixed<1><<<launch.grid, launch.block, 0, s>>>(*p, *o, counter, launch.refill);
+  const bool drift = o->carter_drift != nullptr;
+  auto k = p->integrator == 0 ? (drift ? bhm::k_trace_image_mixed<0, true> : bhm::k_trace_image_mixed<0, false>)
+                              : (drift ? bhm::k_trace_image_mixed<1, true> : bhm::k_trace_image_mixed<1, false>);
+  k<<<launch.grid, launch.block, 0, s>>>(*p, *o, counter, launch.refill);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
 extern "C" int bhk_trace_image_mixed_occupancy(int integrator, int block, int *blocks_per_sm) {
   const cudaError_t e =
       (integrator == 0)
-          ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhm::k_trace_image_mixed<0>, block, 0)
-          : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhm::k_trace_image_mixed<1>, block, 0);
+          ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhm::k_trace_image_mixed<0, false>, block, 0)
+          : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhm::k_trace_image_mixed<1, false>, block, 0);
   return e == cudaSuccess ? 0 : -1;
 }
 
@@ -755,10 +754,10 @@ extern "C" int bhk_trace_list_mixed(const BhkImageParams *p, const BhkImageOut *
                                     void *stream) {
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s) != cudaSuccess) return -1;
-  if (p->integrator == 0)
-    bhm::k_trace_list_mixed<0><<<L.grid, L.block, 0, s>>>(*p, *o, list, count, counter, L.refill);
-  else
-    bhm::k_trace_list_mixed<1><<<L.grid, L.block, 0, s>>>(*p, *o, list, count, counter, L.refill);
+  const bool drift = o->carter_drift != nullptr;
+  auto k = p->integrator == 0 ? (drift ? bhm::k_trace_list_mixed<0, true> : bhm::k_trace_list_mixed<0, false>)
+                              : (drift ? bhm::k_trace_list_mixed<1, true> : bhm::k_trace_list_mixed<1, false>);
+  k<<<L.grid, L.block, 0, s>>>(*p, *o, list, count, counter, L.refill);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
@@ -784,17 +783,16 @@ extern "C" int bhk_trace_batch_mixed(const BhkBatchDev *b, int integrator, unsig
                                      void *stream) {
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s) != cudaSuccess) return -1;
-  if (integrator == 0)
-    bhm::k_trace_batch_mixed<0><<<L.grid, L.block, 0, s>>>(*b, counter, L.refill);
-  else
-    bhm::k_trace_batch_mixed<1><<<L.grid, L.block, 0, s>>>(*b, counter, L.refill);
+  auto k = integrator == 0 ? (b->drift ? bhm::k_trace_batch_mixed<0, true> : bhm::k_trace_batch_mixed<0, false>)
+                           : (b->drift ? bhm::k_trace_batch_mixed<1, true> : bhm::k_trace_batch_mixed<1, false>);
+  k<<<L.grid, L.block, 0, s>>>(*b, counter, L.refill);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
 extern "C" int bhk_trace_batch_mixed_occupancy(int integrator, int block, int *blocks_per_sm) {
   const cudaError_t e =
       (integrator == 0)
-          ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhm::k_trace_batch_mixed<0>, block, 0)
-          : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhm::k_trace_batch_mixed<1>, block, 0);
+          ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhm::k_trace_batch_mixed<0, false>, block, 0)
+          : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, bhm::k_trace_batch_mixed<1, false>, block, 0);
   return e == cudaSuccess ? 0 : -1;
 }

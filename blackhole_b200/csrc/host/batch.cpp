@@ -156,6 +156,8 @@ BH_KerrBatch *bh_kerr_batch_create(const BH_KerrScene *scenes, const BH_KerrImag
   b->d.start_ns = reinterpret_cast<unsigned long long *>(base + o_start);
   b->d.n_total = b->n_total;
   b->d.n_frames = n_frames;
+  b->d.drift = 0;
+  for (int i = 0; i < n_frames; ++i) b->d.drift |= outs[i].carter_drift != nullptr ? 1 : 0;
   b->counter = reinterpret_cast<unsigned long long *>(base + o_counter);
   if (cuda_check(cudaMemcpy(base + o_frames, b->frames.data(), sizeof(BhkFrame) * n, cudaMemcpyHostToDevice),
                  "frame table upload") ||
