@@ -104,12 +104,17 @@ BHSKY_HD void direction_of_motion(double r, double u, double phi, double pr, dou
 
 #ifdef __CUDACC__
 // Radiance of the nearest texel in the direction of motion (see above).
+// Radiance of the texel in direction (x, y, z) (need not be unit).
+__device__ __forceinline__ double radiance_dir(const uint16_t* tex, int N, double x, double y, double z) {
+  const unsigned short bits = tex[texel_of(x, y, z, N)];
+  return (double)__half2float(__ushort_as_half(bits));
+}
+
 __device__ __forceinline__ double radiance(const uint16_t* tex, int N, double r, double u, double phi, double pr,
                                            double pu, double dphi) {
   double x, y, z;
   direction_of_motion(r, u, phi, pr, pu, dphi, x, y, z);
-  const unsigned short bits = tex[texel_of(x, y, z, N)];
-  return (double)__half2float(__ushort_as_half(bits));
+  return radiance_dir(tex, N, x, y, z);
 }
 #endif
 

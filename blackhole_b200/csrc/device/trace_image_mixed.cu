@@ -222,6 +222,26 @@ __device__ __forceinline__ bool on_crossing(const BhkImageParams &p, const BhkIm
   return R.ncross >= p.max_cross;
 }
 
+// The escaping ray's direction of motion (bhsky::direction_of_motion) in
+// FP32: the mixed tracer's own state is FP32, and a texel of the sky spans
+// 2e-3 rad. The azimuth is reduced to [-pi, pi] in FP64 first, so the fast
+// sine and cosine keep their accuracy. A finishing lane runs this while the
+// rest of its warp waits, so its cost counts once per ray for the whole warp.
+__device__ __forceinline__ void direction_of_motion_f(double r, double u, double phi, float pr, float pu, double dphi,
+                                                      float &x, float &y, float &z) {
+  const double two_pi = 6.283185307179586;
+  float sp, cp;
+  __sincosf((float)(phi - two_pi * rint(phi / two_pi)), &sp, &cp);
+  const float uc = fminf(1.0f, fmaxf(-1.0f, (float)u));
+  const float st = sqrtf((1.0f - uc) * (1.0f + uc));
+  const float rf = (float)r;
+  const float dst = st > 1e-30f ? -uc * pu / st : 0.0f;  // d(sin theta)
+  const float a = pr * st + rf * dst, b = rf * st * (float)dphi;
+  x = a * cp - b * sp;
+  y = a * sp + b * cp;
+  z = pr * uc + rf * pu;
+}
+
 __device__ __forceinline__ void finish(const BhkImageParams &p, const BhkImageOut &o, const RayMx &R, int cls) {
   const long long pix = R.pix;
   if (o.cls) o.cls[pix] = cls;
@@ -245,14 +265,17 @@ __device__ __forceinline__ void finish(const BhkImageParams &p, const BhkImageOu
       const double r = to_f64(R.y.r, R.lo.r);
       const double delta = r * r - 2.0 * r + p.a2;
       const double dphi = (double)k.phi + p.a * (double)R.y.pr / delta;
-      if (p.sky) inten += bhsky::radiance(p.sky, p.sky_size, r, u, ph, (double)R.y.pr, (double)R.y.pu, dphi);
-      double x, y, z;
-      bhsky::direction_of_motion(r, u, ph, (double)R.y.pr, (double)R.y.pu, dphi, x, y, z);
-      const double nn = sqrt(x * x + y * y + z * z);
-      if (nn > 0.0) {
-        dir[0] = (float)(x / nn);
-        dir[1] = (float)(y / nn);
-        dir[2] = (float)(z / nn);
+      float fx, fy, fz;  // one direction of motion for the sky and the caller
+      direction_of_motion_f(r, u, ph, R.y.pr, R.y.pu, dphi, fx, fy, fz);
+      if (p.sky) inten += bhsky::radiance_dir(p.sky, p.sky_size, (double)fx, (double)fy, (double)fz);
+      if (o.esc_dir) {
+        const float nn = sqrtf(fx * fx + fy * fy + fz * fz);
+        if (nn > 0.0f) {
+          const float inv = 1.0f / nn;
+          dir[0] = fx * inv;
+          dir[1] = fy * inv;
+          dir[2] = fz * inv;
+        }
       }
     }
   }
