@@ -142,8 +142,17 @@ __global__ void __launch_bounds__(128, BH_ANALYTIC_MIN_CTAS) k_trace_image_analy
                                                               int *__restrict__ list,
                                                               unsigned int *__restrict__ count) {
   const long long stride = (long long)gridDim.x * blockDim.x;
+#ifdef BH_ANALYTIC_SYNC
+  // every thread of the CTA takes the same trips; the warps start each pixel together
+  for (long long base = (long long)blockIdx.x * blockDim.x; base < p.n_pix; base += stride) {
+    const long long pix = base + threadIdx.x;
+    if (pix < p.n_pix && !trace_pixel(p, o, pix)) list[atomicAdd(count, 1u)] = (int)pix;
+    __syncthreads();
+  }
+#else
   for (long long pix = (long long)blockIdx.x * blockDim.x + threadIdx.x; pix < p.n_pix; pix += stride)
     if (!trace_pixel(p, o, pix)) list[atomicAdd(count, 1u)] = (int)pix;
+#endif
 }
 
 // The same over a list of pixels (the surrogate renderer's rejected pixels);
