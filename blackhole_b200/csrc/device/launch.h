@@ -274,6 +274,7 @@ int bhk_post_process(float *fb, int w, int h, const BhkPostTaps *taps, float thr
 int bhk_trace_image_analytic(const BhkImageParams *p, const BhkImageOut *o, int *list, unsigned int *count,
                              BhkLaunch L, void *stream);
 int bhk_trace_image_analytic_occupancy(int block, int *blocks_per_sm);
+int bhk_trace_image_analytic_block(void);  // threads per CTA the closed form is compiled for
 // The same over list[0..*count); pixels it does not cover go to list2[0..*count2).
 int bhk_trace_list_analytic(const BhkImageParams *p, const BhkImageOut *o, const int *list, const unsigned int *count,
                             int *list2, unsigned int *count2, BhkLaunch L, void *stream);

@@ -196,9 +196,10 @@ int bhh_prepare_image_launch(const BH_KerrScene *scene, BhkImageParams *p, BhkLa
   if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
   e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute(SM count)");
-  const int block = g_block_override ? g_block_override : 128;
+  const bool analytic = p->integrator == BH_INTEGRATOR_ANALYTIC;
+  const int block = analytic ? bhk_trace_image_analytic_block() : (g_block_override ? g_block_override : 128);
   int per_sm = 0;
-  const int occ_rc = (p->integrator == BH_INTEGRATOR_ANALYTIC) ? bhk_trace_image_analytic_occupancy(block, &per_sm)
+  const int occ_rc = analytic ? bhk_trace_image_analytic_occupancy(block, &per_sm)
                      : (p->precision == BH_PRECISION_MIXED)
                          ? bhk_trace_image_mixed_occupancy(p->integrator, block, &per_sm)
                          : bhk_trace_image_fp64_occupancy(p->integrator, block, &per_sm);

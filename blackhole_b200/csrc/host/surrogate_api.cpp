@@ -522,12 +522,13 @@ int bh_surrogate_trace_image(BH_Surrogate *s, const BH_KerrScene *scene, const B
   // near-critical band costs no more than the rest), then mixed DP45 on what
   // it does not cover.
   int per_sm = 0;
-  if (bhk_trace_image_analytic_occupancy(128, &per_sm) != 0 || per_sm < 1)
+  const int a_block = bhk_trace_image_analytic_block();
+  if (bhk_trace_image_analytic_occupancy(a_block, &per_sm) != 0 || per_sm < 1)
     return fail_msg("surrogate render: occupancy query failed");
   int dev = 0, sms = 0;
   if (int rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice")) return rc;
   if (int rc = cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count")) return rc;
-  const BhkLaunch La{sms * per_sm, 128, 1, 0};
+  const BhkLaunch La{sms * per_sm, a_block, 1, 0};
   if (bhk_trace_list_analytic(&p, &o, s->r_list, s->r_counts, s->r_list2, s->r_counts + 6, La, s->side))
     return fail_msg("surrogate render: closed-form fallback launch failed");
   if (bhk_trace_list_mixed(&p, &o, s->r_list2, s->r_counts + 6, s->r_counter, L, s->side))

@@ -313,7 +313,8 @@ int bh_kerr_trace_image_host(const BH_KerrScene *scene, const BH_KerrImageOut *o
  */
 int bh_kerr_trace_image_host_noalloc(const BH_KerrScene *scene, const BH_KerrImageOut *out_host, void *stream);
 
-/** Launch configuration of the image tracer (0 = automatic). */
+/** Launch configuration of the image tracer (0 = automatic; the closed-form
+ * integrator keeps the CTA size it is compiled for). */
 int bh_kerr_set_launch(int32_t block_threads, int32_t ctas_per_sm);
 
 /* ---------------------------------------------------------------------------
