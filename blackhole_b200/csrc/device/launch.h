@@ -105,6 +105,19 @@ int bhk_trace_image_mixed_occupancy(int integrator, int block, int *blocks_per_s
 int bhk_trace_list_mixed(const BhkImageParams *p, const BhkImageOut *o, const int *list, const unsigned int *count,
                          unsigned long long *work_counter, BhkLaunch L, void *stream);
 
+// Output fields of a set of pixels gathered into compact arrays (the host-
+// buffer render's rejected pixels, written after their rows were copied):
+// src: the 10 BH_KerrImageOut fields in their order (NULL: skip), size 4 or
+// 8 bytes, planes 1 or max_cross; dst[f][c * cap + w] = src[f][c * n_pix + list[w]]
+// for w < min(*count, cap).
+typedef struct BhkGather {
+  const void *src[10];
+  void *dst[10];
+  int32_t size[10], planes[10];
+} BhkGather;
+int bhk_gather_pixels(const BhkGather *g, const int *list, const unsigned int *count, long long n_pix, int cap,
+                      void *stream);
+
 // Surrogate renderer (surrogate_render.cu): per-pixel acceptance of the
 // network's head outputs [n_pix][16] for pixels [p0, p1), exact refinement of
 // accepted disk hits, and the list of pixels left to the integrator. stats[5] += pixels accepted,

@@ -23,6 +23,8 @@
 // one side of the equator go to the integrator.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "image_fp64.cuh"
 #include "launch.h"
 #include "mino_solve.cuh"
@@ -170,7 +172,35 @@ __global__ void __launch_bounds__(128, FAST ? BH_REFINE_MIN_CTAS : 2) k_surrogat
   for (int r = 0; r < 5; ++r) warp_count(stats, r, live && reason == r);
 }
 
+// Copies the outputs of the first min(*count, cap) pixels of `list` into
+// compact arrays: field f's entry w (plane c) goes to dst[f][c * cap + w].
+__global__ void k_gather_pixels(BhkGather g, const int *__restrict__ list, const unsigned int *__restrict__ count,
+                                long long n_pix, int cap) {
+  const unsigned int m = min(*count, (unsigned int)cap);
+  for (unsigned int w = blockIdx.x * blockDim.x + threadIdx.x; w < m; w += gridDim.x * blockDim.x) {
+    const long long pix = list[w];
+    for (int f = 0; f < 10; ++f) {
+      if (!g.src[f]) continue;
+      for (int c = 0; c < g.planes[f]; ++c) {
+        const long long from = (long long)c * n_pix + pix, to = (long long)c * cap + w;
+        if (g.size[f] == 4)
+          static_cast<int *>(g.dst[f])[to] = static_cast<const int *>(g.src[f])[from];
+        else
+          static_cast<double *>(g.dst[f])[to] = static_cast<const double *>(g.src[f])[from];
+      }
+    }
+  }
+}
+
 }  // namespace
+
+extern "C" int bhk_gather_pixels(const BhkGather *g, const int *list, const unsigned int *count, long long n_pix,
+                                 int cap, void *stream) {
+  if (cap <= 0) return 0;
+  const unsigned blocks = (unsigned)std::min<long long>(1184, (cap + 255) / 256);
+  k_gather_pixels<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(*g, list, count, n_pix, cap);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
 
 extern "C" int bhk_surrogate_refine(const BhkImageParams *p, const BhkImageOut *o, const float *head, float min_conf,
                                     double band, int verify, int refine_fp64, long long p0, long long p1, int *list,

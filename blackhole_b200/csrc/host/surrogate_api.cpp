@@ -13,6 +13,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <vector>
 
 #include "../../../include/bh_surrogate.h"
@@ -60,6 +61,13 @@ struct BH_Surrogate {
   char *host_out = nullptr;
   size_t host_out_bytes = 0;
   cudaStream_t host_stream = nullptr;
+  // its copies: each chunk's rows go to the host as soon as they are refined
+  // (copy_stream), and the rejected pixels, which the fallback writes later,
+  // follow in compact form (gather: device, gather_host: pinned host)
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t copy_ev[kRenderChunks] = {};
+  char *gather = nullptr, *gather_host = nullptr;
+  size_t gather_bytes = 0;
   // host copy of the biases for the fused inference launch
   std::vector<float> host_bias;
   bool bias_stale = true;
@@ -237,8 +245,12 @@ void bh_surrogate_destroy(BH_Surrogate *s) {
   for (void *p : s->allocs) cudaFree(p);
   for (cudaEvent_t e : s->ev)
     if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : s->copy_ev)
+    if (e) cudaEventDestroy(e);
   if (s->side) cudaStreamDestroy(s->side);
   if (s->host_stream) cudaStreamDestroy(s->host_stream);
+  if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
+  if (s->gather_host) cudaFreeHost(s->gather_host);
   if (cur >= 0) cudaSetDevice(cur);
   delete s;
 }
@@ -449,8 +461,15 @@ void bh_surrogate_policy_defaults(BH_SurrogatePolicy *p) {
   p->chunks = 0;
 }
 
-int bh_surrogate_trace_image(BH_Surrogate *s, const BH_KerrScene *scene, const BH_KerrImageOut *out,
-                             const BH_SurrogatePolicy *policy, void *stream) {
+}  // extern "C"
+
+namespace {
+
+// The render of bh_surrogate_trace_image; after the refinement of each chunk
+// of pixels [p0, p1) is enqueued on s->side, chunk_done(k, p0, p1) is called
+// (when given), and `chunks` (1..kRenderChunks) overrides the policy's.
+int render(BH_Surrogate *s, const BH_KerrScene *scene, const BH_KerrImageOut *out, const BH_SurrogatePolicy *policy,
+           void *stream, int chunks, const std::function<int(int, int64_t, int64_t)> &chunk_done) {
   if (!s || !scene || !out) return fail_msg("surrogate render: NULL argument");
   BH_SurrogatePolicy pol;
   bh_surrogate_policy_defaults(&pol);
@@ -459,7 +478,7 @@ int bh_surrogate_trace_image(BH_Surrogate *s, const BH_KerrScene *scene, const B
       !(pol.critical_band >= 0.0) || pol.chunks < 0 || pol.chunks > kRenderChunks)
     return fail_msg("surrogate render: policy needs min_confidence in [0, 1], verify 1, 2 or 3, critical_band >= 0, "
                     "chunks in [0, %d]", kRenderChunks);
-  const int n_chunks = pol.chunks > 0 ? pol.chunks : kDefaultChunks;
+  const int n_chunks = chunks > 0 ? chunks : (pol.chunks > 0 ? pol.chunks : kDefaultChunks);
   BH_KerrScene sc = *scene;
   sc.precision = BH_PRECISION_MIXED;  // the fallback integrator
   if (sc.integrator == BH_INTEGRATOR_ANALYTIC) sc.integrator = BH_INTEGRATOR_DP45;
@@ -517,6 +536,8 @@ int bh_surrogate_trace_image(BH_Surrogate *s, const BH_KerrScene *scene, const B
     if (bhk_surrogate_refine(&p, &o, s->r_head, pol.min_confidence, pol.critical_band, pol.verify, pol.refine_fp64,
                              p0, p1, s->r_list, s->r_counts, s->r_counts + 1, s->side))
       return fail_msg("surrogate render: refine launch failed");
+    if (chunk_done)
+      if (int rc = chunk_done(k, p0, p1)) return rc;
   }
   // Rejected pixels: the closed-form tracer (O(1) per crossing, so the
   // near-critical band costs no more than the rest), then mixed DP45 on what
@@ -535,6 +556,29 @@ int bh_surrogate_trace_image(BH_Surrogate *s, const BH_KerrScene *scene, const B
     return fail_msg("surrogate render: fallback tracer launch failed");
   if (int rc = cuda_check(cudaEventRecord(s->ev[kRenderChunks + 1], s->side), "cudaEventRecord")) return rc;
   return cuda_check(cudaStreamWaitEvent(st, s->ev[kRenderChunks + 1], 0), "cudaStreamWaitEvent");
+}
+
+// A bounded wait of the network's kernels that ran out leaves its pixels
+// undefined: report it (and clear the flag) after a synchronized render.
+int check_wait_flag(BH_Surrogate *s) {
+  int code = 0;
+  if (int rc = cuda_check(cudaMemcpy(&code, s->err, sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy(error flag)"))
+    return rc;
+  if (code) {
+    cudaMemset(s->err, 0, sizeof(int));
+    return fail_msg("bh_surrogate_trace_image_host: a bounded device wait of the network ran out (code %d); "
+                    "the outputs are not valid", code);
+  }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bh_surrogate_trace_image(BH_Surrogate *s, const BH_KerrScene *scene, const BH_KerrImageOut *out,
+                             const BH_SurrogatePolicy *policy, void *stream) {
+  return render(s, scene, out, policy, stream, 0, nullptr);
 }
 
 int bh_surrogate_trace_image_host(BH_Surrogate *s, const BH_KerrScene *scene, const BH_KerrImageOut *h,
@@ -564,32 +608,144 @@ int bh_surrogate_trace_image_host(BH_Surrogate *s, const BH_KerrScene *scene, co
     if (int rc = alloc(s, &s->host_out, total, "cudaMalloc(render outputs)")) return rc;
     s->host_out_bytes = total;
   }
-  if (!s->host_stream)
+  if (!s->host_stream) {
     if (int rc = cuda_check(cudaStreamCreateWithFlags(&s->host_stream, cudaStreamNonBlocking), "cudaStreamCreate"))
       return rc;
+    if (int rc = cuda_check(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking), "cudaStreamCreate"))
+      return rc;
+    for (cudaEvent_t &e : s->copy_ev)
+      if (int rc = cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate")) return rc;
+  }
   void *d[10];
   for (int i = 0; i < 10; ++i) d[i] = host[i] ? s->host_out + off[i] : nullptr;
   const BH_KerrImageOut dev{static_cast<int32_t *>(d[0]), static_cast<int32_t *>(d[1]), static_cast<int32_t *>(d[2]),
                             static_cast<double *>(d[3]),  static_cast<double *>(d[4]),  static_cast<double *>(d[5]),
                             static_cast<double *>(d[6]),  static_cast<double *>(d[7]),  static_cast<double *>(d[8]),
                             static_cast<double *>(d[9]), nullptr};  // the drift diagnostic is not staged
-  if (int rc = bh_surrogate_trace_image(s, scene, &dev, policy, s->host_stream)) return rc;
-  for (int i = 0; i < 10; ++i)
-    if (host[i])
-      if (int rc = cuda_check(cudaMemcpyAsync(host[i], d[i], bytes[i], cudaMemcpyDeviceToHost, s->host_stream),
-                              "cudaMemcpyAsync(D2H)"))
-        return rc;
-  if (int rc = cuda_check(cudaStreamSynchronize(s->host_stream), "bh_surrogate_trace_image_host")) return rc;
-  // a bounded wait of the network's kernels that ran out leaves its pixels undefined
-  int code = 0;
-  if (int rc = cuda_check(cudaMemcpy(&code, s->err, sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy(error flag)"))
-    return rc;
-  if (code) {
-    cudaMemset(s->err, 0, sizeof(int));
-    return fail_msg("bh_surrogate_trace_image_host: a bounded device wait of the network ran out (code %d); "
-                    "the outputs are not valid", code);
+  const int planes[10] = {1, 1, 1, int(mc), int(mc), int(mc), 1, 1, 1, 1};
+  const int esize[10] = {4, 4, 4, 8, 8, 8, 8, 8, 8, 8};
+  // Copies into pageable memory return only when done, which would hold back
+  // the next chunk's launch: those buffers get the whole frame at the end.
+  bool pinned = true;
+  for (int i = 0; i < 10; ++i) {
+    if (!host[i]) continue;
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, host[i]) != cudaSuccess || at.type != cudaMemoryTypeHost) {
+      cudaGetLastError();
+      pinned = false;
+    }
   }
-  return 0;
+  if (!pinned) {
+    if (int rc = render(s, scene, &dev, policy, s->host_stream, 0, nullptr)) return rc;
+    for (int i = 0; i < 10; ++i)
+      if (host[i])
+        if (int rc = cuda_check(cudaMemcpyAsync(host[i], d[i], bytes[i], cudaMemcpyDeviceToHost, s->host_stream),
+                                "cudaMemcpyAsync(D2H)"))
+          return rc;
+    if (int rc = cuda_check(cudaStreamSynchronize(s->host_stream), "bh_surrogate_trace_image_host")) return rc;
+    return check_wait_flag(s);
+  }
+  // Rows go to the host chunk by chunk while the next chunk is inferred: the
+  // accepted pixels of [p0, p1) are final once its refinement has run. The
+  // rejected ones are written later by the fallback tracers; they follow in
+  // compact form (gathered on the device, scattered here), up to `cap` of
+  // them; past that the whole frame is copied again.
+  auto copy_rows = [&](int k, int64_t p0, int64_t p1) -> int {
+    if (int rc = cuda_check(cudaEventRecord(s->copy_ev[k], s->side), "cudaEventRecord")) return rc;
+    if (int rc = cuda_check(cudaStreamWaitEvent(s->copy_stream, s->copy_ev[k], 0), "cudaStreamWaitEvent")) return rc;
+    for (int i = 0; i < 10; ++i) {
+      if (!host[i]) continue;
+      for (int c = 0; c < planes[i]; ++c) {
+        const size_t at = (size_t(c) * n + size_t(p0)) * esize[i];
+        if (int rc = cuda_check(cudaMemcpyAsync(static_cast<char *>(host[i]) + at, static_cast<char *>(d[i]) + at,
+                                                size_t(p1 - p0) * esize[i], cudaMemcpyDeviceToHost, s->copy_stream),
+                                "cudaMemcpyAsync(D2H rows)"))
+          return rc;
+      }
+    }
+    return 0;
+  };
+  const int chunks = policy && policy->chunks > 0 ? policy->chunks : kRenderChunks;
+  if (int rc = render(s, scene, &dev, policy, s->host_stream, chunks, copy_rows)) return rc;
+  // compact buffers: the count, the list, then each field's planes of `cap` entries
+  const int64_t cap = std::min<int64_t>(int64_t(n), std::max<int64_t>(4096, int64_t(n) / 25));
+  size_t gbytes = 256 + ((size_t(cap) * 4 + 255) & ~size_t(255)), goff[10];
+  for (int i = 0; i < 10; ++i) {
+    goff[i] = gbytes;
+    if (host[i]) gbytes += (size_t(cap) * planes[i] * esize[i] + 255) & ~size_t(255);
+  }
+  if (gbytes > s->gather_bytes) {
+    if (s->gather) {
+      auto it = std::find(s->allocs.begin(), s->allocs.end(), s->gather);
+      if (it != s->allocs.end()) s->allocs.erase(it);
+      cudaFree(s->gather);
+      s->gather = nullptr;
+    }
+    if (s->gather_host) cudaFreeHost(s->gather_host);
+    s->gather_host = nullptr;
+    s->gather_bytes = 0;
+    if (int rc = alloc(s, &s->gather, gbytes, "cudaMalloc(gathered pixels)")) return rc;
+    if (int rc = cuda_check(cudaMallocHost(&s->gather_host, gbytes), "cudaMallocHost(gathered pixels)")) return rc;
+    s->gather_bytes = gbytes;
+  }
+  BhkGather g{};
+  for (int i = 0; i < 10; ++i) {
+    g.src[i] = d[i];
+    g.dst[i] = host[i] ? s->gather + goff[i] : nullptr;
+    g.size[i] = esize[i];
+    g.planes[i] = planes[i];
+  }
+  if (bhk_gather_pixels(&g, s->r_list, s->r_counts, int64_t(n), int(cap), s->host_stream))
+    return fail_msg("bh_surrogate_trace_image_host: gather launch failed");
+  if (int rc = cuda_check(cudaMemcpyAsync(s->gather_host, s->r_counts, sizeof(unsigned int), cudaMemcpyDeviceToHost,
+                                          s->host_stream),
+                          "cudaMemcpyAsync(D2H count)"))
+    return rc;
+  if (int rc = cuda_check(cudaStreamSynchronize(s->host_stream), "bh_surrogate_trace_image_host")) return rc;
+  const int64_t m = *reinterpret_cast<const unsigned int *>(s->gather_host);
+  if (m <= cap) {
+    if (m > 0) {
+      if (int rc = cuda_check(cudaMemcpyAsync(s->gather_host + 256, s->r_list, size_t(m) * 4, cudaMemcpyDeviceToHost,
+                                              s->host_stream),
+                              "cudaMemcpyAsync(D2H list)"))
+        return rc;
+      for (int i = 0; i < 10; ++i)
+        if (host[i])
+          for (int c = 0; c < planes[i]; ++c) {
+            const size_t at = goff[i] + size_t(c) * cap * esize[i];
+            if (int rc = cuda_check(cudaMemcpyAsync(s->gather_host + at, s->gather + at, size_t(m) * esize[i],
+                                                    cudaMemcpyDeviceToHost, s->host_stream),
+                                    "cudaMemcpyAsync(D2H gathered)"))
+              return rc;
+          }
+    }
+    if (int rc = cuda_check(cudaStreamSynchronize(s->host_stream), "bh_surrogate_trace_image_host")) return rc;
+    if (int rc = cuda_check(cudaStreamSynchronize(s->copy_stream), "bh_surrogate_trace_image_host")) return rc;
+    const int *list = reinterpret_cast<const int *>(s->gather_host + 256);
+    for (int i = 0; i < 10; ++i) {
+      if (!host[i]) continue;
+      for (int c = 0; c < planes[i]; ++c) {
+        const char *from = s->gather_host + goff[i] + size_t(c) * cap * esize[i];
+        char *to = static_cast<char *>(host[i]) + size_t(c) * n * esize[i];
+        if (esize[i] == 4)
+          for (int64_t w = 0; w < m; ++w)
+            reinterpret_cast<int32_t *>(to)[list[w]] = reinterpret_cast<const int32_t *>(from)[w];
+        else
+          for (int64_t w = 0; w < m; ++w)
+            reinterpret_cast<double *>(to)[list[w]] = reinterpret_cast<const double *>(from)[w];
+      }
+    }
+  } else {
+    // more rejected pixels than the compact buffers hold: the whole frame again
+    if (int rc = cuda_check(cudaStreamSynchronize(s->copy_stream), "bh_surrogate_trace_image_host")) return rc;
+    for (int i = 0; i < 10; ++i)
+      if (host[i])
+        if (int rc = cuda_check(cudaMemcpyAsync(host[i], d[i], bytes[i], cudaMemcpyDeviceToHost, s->host_stream),
+                                "cudaMemcpyAsync(D2H)"))
+          return rc;
+    if (int rc = cuda_check(cudaStreamSynchronize(s->host_stream), "bh_surrogate_trace_image_host")) return rc;
+  }
+  return check_wait_flag(s);
 }
 
 int bh_surrogate_last_stats(BH_Surrogate *s, BH_SurrogateStats *out) {

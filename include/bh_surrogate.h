@@ -140,8 +140,14 @@ int bh_surrogate_trace_image(BH_Surrogate* s, const BH_KerrScene* scene, const B
                              const BH_SurrogatePolicy* policy, void* stream);
 
 /* The same with HOST output buffers (BH_KerrImageOut of host pointers, NULL =
- * not wanted): grow-only device buffers owned by the network, one
- * device-to-host copy per requested field, returns when the copies are done.
+ * not wanted): grow-only device buffers owned by the network; returns when
+ * the copies are done. With page-locked buffers (cudaMallocHost,
+ * cudaHostRegister) the frame is rendered in policy->chunks chunks (0: 8)
+ * and each chunk's rows are copied while the next one is inferred; the
+ * pixels the policy rejected follow, gathered on the device into compact
+ * arrays and scattered on the host (past max(4096, pixels / 25) of them the
+ * frame is copied again). Pageable buffers get one copy per field after the
+ * render. The outputs are the same either way.
  * Returns -1 with a message when an allocation fails or when a bounded wait
  * of the network's kernels ran out (the outputs are then not valid); the
  * next call starts afresh. */

@@ -259,3 +259,52 @@ def test_trained_network_gain_at_equal_outputs(cuda):
     t_cf_d = _ms(lambda: kerr.trace_image(sa, o_a))
     print(f"\nall fields: trained {t_net:.3f} ms, fallback only {t_blank:.3f} ms, mixed DP45 {t_plain:.3f} ms; "
           f"disk fields: trained {t_net_d:.3f} ms, closed form {t_cf_d:.3f} ms")
+
+
+def _host_render(net, s, pinned, chunks=0):
+    """bh_surrogate_trace_image_host into pinned (torch) or pageable (numpy)
+    buffers of every field."""
+    import ctypes as C
+
+    from blackhole_b200 import _abi
+
+    n = s.width * s.height
+    outs = {f: torch.zeros(n * (s.max_crossings if f in _abi.PLANE_FIELDS else 1),
+                           dtype=torch.int32 if f in _abi.INT_FIELDS else torch.float64) for f in ALL_FIELDS}
+    if pinned:
+        outs = {f: t.pin_memory() for f, t in outs.items()}
+    o = _abi.KerrImageOut()
+    for f, t in outs.items():
+        setattr(o, f, t.data_ptr())
+    pol = _abi.SurrogatePolicy(0.99, 1, 0.05, 0, chunks)
+    _abi.check(net._lib.bh_surrogate_trace_image_host(net._h, C.byref(s), C.byref(o), C.byref(pol)))
+    return {f: t.numpy().reshape(-1) for f, t in outs.items()}
+
+
+@pytest.mark.parametrize("trained,pinned,chunks", [(True, True, 0), (True, True, 3), (True, False, 0),
+                                                   (False, True, 0), (False, False, 0)])
+def test_host_buffers_match_device_render(cuda, trained, pinned, chunks):
+    """The host-buffer entry point returns the device render's outputs bit
+    for bit. Pinned buffers take the overlapped path: each chunk's rows are
+    copied while the next is inferred, and the rejected pixels follow in
+    compact form (the trained network rejects under 1 %); with an untrained
+    network every pixel is rejected, more than the compact buffers hold, and
+    the frame is copied again. Pageable buffers are copied after the render."""
+    from blackhole_b200 import kerr
+    from blackhole_b200 import surrogate as S
+
+    if trained and not WEIGHTS.exists():
+        pytest.skip("trained weights not shipped")
+    net = S.Surrogate(max_batch=128, seed=3)
+    if trained:
+        net.load(WEIGHTS)
+    s = c4_scene(320, precision=1)
+    ref = host(net.trace_image(s, kerr.alloc_image_outputs(s, fields=list(ALL_FIELDS))))
+    torch.cuda.synchronize()
+    st = net.last_stats()
+    rejected = st["pixels"] - st["accepted"]
+    assert (0 < rejected < 4096) if trained else rejected == st["pixels"], st
+    for _ in range(2):  # the second call reuses the grown buffers
+        got = _host_render(net, s, pinned, chunks)
+        for f in ALL_FIELDS:
+            np.testing.assert_array_equal(got[f], ref[f].reshape(-1), err_msg=f)
