@@ -109,11 +109,15 @@ int bhk_trace_list_mixed(const BhkImageParams *p, const BhkImageOut *o, const in
 // buffer render's rejected pixels, written after their rows were copied):
 // src: the 10 BH_KerrImageOut fields in their order (NULL: skip), size 4 or
 // 8 bytes, planes 1 or max_cross; dst[f][c * cap + w] = src[f][c * n_pix + list[w]]
-// for w < min(*count, cap).
+// and list_out[w] = list[w] for w < min(*count, cap); *count_out = *count.
+// The destinations may be mapped host memory (the writes end with a
+// system-scope fence).
 typedef struct BhkGather {
   const void *src[10];
   void *dst[10];
   int32_t size[10], planes[10];
+  int *list_out;
+  unsigned int *count_out;
 } BhkGather;
 int bhk_gather_pixels(const BhkGather *g, const int *list, const unsigned int *count, long long n_pix, int cap,
                       void *stream);

@@ -176,9 +176,11 @@ __global__ void __launch_bounds__(128, FAST ? BH_REFINE_MIN_CTAS : 2) k_surrogat
 // compact arrays: field f's entry w (plane c) goes to dst[f][c * cap + w].
 __global__ void k_gather_pixels(BhkGather g, const int *__restrict__ list, const unsigned int *__restrict__ count,
                                 long long n_pix, int cap) {
-  const unsigned int m = min(*count, (unsigned int)cap);
+  const unsigned int total = *count, m = min(total, (unsigned int)cap);
+  if (blockIdx.x == 0 && threadIdx.x == 0) *g.count_out = total;
   for (unsigned int w = blockIdx.x * blockDim.x + threadIdx.x; w < m; w += gridDim.x * blockDim.x) {
     const long long pix = list[w];
+    g.list_out[w] = (int)pix;
     for (int f = 0; f < 10; ++f) {
       if (!g.src[f]) continue;
       for (int c = 0; c < g.planes[f]; ++c) {
@@ -190,6 +192,7 @@ __global__ void k_gather_pixels(BhkGather g, const int *__restrict__ list, const
       }
     }
   }
+  __threadfence_system();
 }
 
 }  // namespace

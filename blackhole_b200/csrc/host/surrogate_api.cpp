@@ -63,10 +63,13 @@ struct BH_Surrogate {
   cudaStream_t host_stream = nullptr;
   // its copies: each chunk's rows go to the host as soon as they are refined
   // (copy_stream), and the rejected pixels, which the fallback writes later,
-  // follow in compact form (gather: device, gather_host: pinned host)
+  // follow in compact form
   cudaStream_t copy_stream = nullptr;
-  cudaEvent_t copy_ev[kRenderChunks] = {};
-  char *gather = nullptr, *gather_host = nullptr;
+  cudaEvent_t copy_ev[kRenderChunks] = {};    // chunk k refined (recorded on side)
+  cudaEvent_t copy_done[kRenderChunks] = {};  // chunk k's rows on the host (copy_stream)
+  cudaEvent_t gathered = nullptr;             // compact arrays written (host_stream)
+  char *gather_host = nullptr;  // mapped, page-locked: written by the gather kernel over the bus
+  char *gather_dev = nullptr;   // its device address
   size_t gather_bytes = 0;
   // host copy of the biases for the fused inference launch
   std::vector<float> host_bias;
@@ -247,6 +250,9 @@ void bh_surrogate_destroy(BH_Surrogate *s) {
     if (e) cudaEventDestroy(e);
   for (cudaEvent_t e : s->copy_ev)
     if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : s->copy_done)
+    if (e) cudaEventDestroy(e);
+  if (s->gathered) cudaEventDestroy(s->gathered);
   if (s->side) cudaStreamDestroy(s->side);
   if (s->host_stream) cudaStreamDestroy(s->host_stream);
   if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
@@ -517,7 +523,15 @@ int render(BH_Surrogate *s, const BH_KerrScene *scene, const BH_KerrImageOut *ou
   const BhkImageOut o{out->cls,   out->steps,     out->n_cross,   out->r_hit,     out->phi_hit,
                       out->g,     out->flux,      out->intensity, out->theta_inf, out->phi_inf, nullptr, nullptr, out->carter_drift, nullptr};
   if (!s->side) {
-    if (int rc = cuda_check(cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking), "cudaStreamCreate")) return rc;
+    // The refinement and fallback go first when SMs free up: a chunk's rows
+    // are then final (and, in the host-buffer render, copied) while later
+    // chunks are still being inferred. The total work is the same.
+    int least = 0, greatest = 0;
+    if (int rc = cuda_check(cudaDeviceGetStreamPriorityRange(&least, &greatest), "cudaDeviceGetStreamPriorityRange"))
+      return rc;
+    if (int rc = cuda_check(cudaStreamCreateWithPriority(&s->side, cudaStreamNonBlocking, greatest),
+                            "cudaStreamCreateWithPriority"))
+      return rc;
     for (cudaEvent_t &e : s->ev)
       if (int rc = cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate")) return rc;
   }
@@ -615,6 +629,10 @@ int bh_surrogate_trace_image_host(BH_Surrogate *s, const BH_KerrScene *scene, co
       return rc;
     for (cudaEvent_t &e : s->copy_ev)
       if (int rc = cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate")) return rc;
+    for (cudaEvent_t &e : s->copy_done)
+      if (int rc = cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate")) return rc;
+    if (int rc = cuda_check(cudaEventCreateWithFlags(&s->gathered, cudaEventDisableTiming), "cudaEventCreate"))
+      return rc;
   }
   void *d[10];
   for (int i = 0; i < 10; ++i) d[i] = host[i] ? s->host_out + off[i] : nullptr;
@@ -647,9 +665,13 @@ int bh_surrogate_trace_image_host(BH_Surrogate *s, const BH_KerrScene *scene, co
   }
   // Rows go to the host chunk by chunk while the next chunk is inferred: the
   // accepted pixels of [p0, p1) are final once its refinement has run. The
-  // rejected ones are written later by the fallback tracers; they follow in
-  // compact form (gathered on the device, scattered here), up to `cap` of
-  // them; past that the whole frame is copied again.
+  // rejected ones are written later by the fallback tracers; the gather
+  // kernel writes them in compact form straight into mapped host memory (a
+  // copy would queue behind the rows on the copy engine), and each chunk's
+  // share is scattered here as soon as that chunk's rows have landed. Past
+  // `cap` rejected pixels the whole frame is copied again.
+  int64_t cp0[kRenderChunks] = {}, cp1[kRenderChunks] = {};
+  int n_done = 0;
   auto copy_rows = [&](int k, int64_t p0, int64_t p1) -> int {
     if (int rc = cuda_check(cudaEventRecord(s->copy_ev[k], s->side), "cudaEventRecord")) return rc;
     if (int rc = cuda_check(cudaStreamWaitEvent(s->copy_stream, s->copy_ev[k], 0), "cudaStreamWaitEvent")) return rc;
@@ -663,10 +685,11 @@ int bh_surrogate_trace_image_host(BH_Surrogate *s, const BH_KerrScene *scene, co
           return rc;
       }
     }
-    return 0;
+    cp0[k] = p0;
+    cp1[k] = p1;
+    n_done = k + 1;
+    return cuda_check(cudaEventRecord(s->copy_done[k], s->copy_stream), "cudaEventRecord");
   };
-  const int chunks = policy && policy->chunks > 0 ? policy->chunks : kRenderChunks;
-  if (int rc = render(s, scene, &dev, policy, s->host_stream, chunks, copy_rows)) return rc;
   // compact buffers: the count, the list, then each field's planes of `cap` entries
   const int64_t cap = std::min<int64_t>(int64_t(n), std::max<int64_t>(4096, int64_t(n) / 25));
   size_t gbytes = 256 + ((size_t(cap) * 4 + 255) & ~size_t(255)), goff[10];
@@ -675,66 +698,73 @@ int bh_surrogate_trace_image_host(BH_Surrogate *s, const BH_KerrScene *scene, co
     if (host[i]) gbytes += (size_t(cap) * planes[i] * esize[i] + 255) & ~size_t(255);
   }
   if (gbytes > s->gather_bytes) {
-    if (s->gather) {
-      auto it = std::find(s->allocs.begin(), s->allocs.end(), s->gather);
-      if (it != s->allocs.end()) s->allocs.erase(it);
-      cudaFree(s->gather);
-      s->gather = nullptr;
-    }
     if (s->gather_host) cudaFreeHost(s->gather_host);
-    s->gather_host = nullptr;
+    s->gather_host = s->gather_dev = nullptr;
     s->gather_bytes = 0;
-    if (int rc = alloc(s, &s->gather, gbytes, "cudaMalloc(gathered pixels)")) return rc;
-    if (int rc = cuda_check(cudaMallocHost(&s->gather_host, gbytes), "cudaMallocHost(gathered pixels)")) return rc;
+    if (int rc = cuda_check(cudaHostAlloc(&s->gather_host, gbytes, cudaHostAllocMapped), "cudaHostAlloc(gathered pixels)"))
+      return rc;
+    if (int rc = cuda_check(cudaHostGetDevicePointer(&s->gather_dev, s->gather_host, 0), "cudaHostGetDevicePointer")) {
+      cudaFreeHost(s->gather_host);
+      s->gather_host = nullptr;
+      return rc;
+    }
     s->gather_bytes = gbytes;
   }
+  // on a failure after rows were enqueued: no copy may still be writing into
+  // the caller's buffers when the call returns
+  auto drained = [&](int rc) {
+    cudaStreamSynchronize(s->copy_stream);
+    cudaStreamSynchronize(s->host_stream);
+    return rc;
+  };
+  const int chunks = policy && policy->chunks > 0 ? policy->chunks : kRenderChunks;
+  if (int rc = render(s, scene, &dev, policy, s->host_stream, chunks, copy_rows)) return drained(rc);
   BhkGather g{};
   for (int i = 0; i < 10; ++i) {
     g.src[i] = d[i];
-    g.dst[i] = host[i] ? s->gather + goff[i] : nullptr;
+    g.dst[i] = host[i] ? s->gather_dev + goff[i] : nullptr;
     g.size[i] = esize[i];
     g.planes[i] = planes[i];
   }
+  g.count_out = reinterpret_cast<unsigned int *>(s->gather_dev);
+  g.list_out = reinterpret_cast<int *>(s->gather_dev + 256);
   if (bhk_gather_pixels(&g, s->r_list, s->r_counts, int64_t(n), int(cap), s->host_stream))
-    return fail_msg("bh_surrogate_trace_image_host: gather launch failed");
-  if (int rc = cuda_check(cudaMemcpyAsync(s->gather_host, s->r_counts, sizeof(unsigned int), cudaMemcpyDeviceToHost,
-                                          s->host_stream),
-                          "cudaMemcpyAsync(D2H count)"))
-    return rc;
-  if (int rc = cuda_check(cudaStreamSynchronize(s->host_stream), "bh_surrogate_trace_image_host")) return rc;
-  const int64_t m = *reinterpret_cast<const unsigned int *>(s->gather_host);
+    return drained(fail_msg("bh_surrogate_trace_image_host: gather launch failed"));
+  if (int rc = cuda_check(cudaEventRecord(s->gathered, s->host_stream), "cudaEventRecord")) return drained(rc);
+  if (int rc = cuda_check(cudaEventSynchronize(s->gathered), "bh_surrogate_trace_image_host")) return drained(rc);
+  const int64_t m = *reinterpret_cast<volatile const unsigned int *>(s->gather_host);
   if (m <= cap) {
-    if (m > 0) {
-      if (int rc = cuda_check(cudaMemcpyAsync(s->gather_host + 256, s->r_list, size_t(m) * 4, cudaMemcpyDeviceToHost,
-                                              s->host_stream),
-                              "cudaMemcpyAsync(D2H list)"))
-        return rc;
-      for (int i = 0; i < 10; ++i)
-        if (host[i])
-          for (int c = 0; c < planes[i]; ++c) {
-            const size_t at = goff[i] + size_t(c) * cap * esize[i];
-            if (int rc = cuda_check(cudaMemcpyAsync(s->gather_host + at, s->gather + at, size_t(m) * esize[i],
-                                                    cudaMemcpyDeviceToHost, s->host_stream),
-                                    "cudaMemcpyAsync(D2H gathered)"))
-              return rc;
-          }
-    }
-    if (int rc = cuda_check(cudaStreamSynchronize(s->host_stream), "bh_surrogate_trace_image_host")) return rc;
-    if (int rc = cuda_check(cudaStreamSynchronize(s->copy_stream), "bh_surrogate_trace_image_host")) return rc;
+    // bucket the compact entries by chunk, then scatter each bucket once its rows are on the host
     const int *list = reinterpret_cast<const int *>(s->gather_host + 256);
-    for (int i = 0; i < 10; ++i) {
-      if (!host[i]) continue;
-      for (int c = 0; c < planes[i]; ++c) {
-        const char *from = s->gather_host + goff[i] + size_t(c) * cap * esize[i];
-        char *to = static_cast<char *>(host[i]) + size_t(c) * n * esize[i];
-        if (esize[i] == 4)
-          for (int64_t w = 0; w < m; ++w)
-            reinterpret_cast<int32_t *>(to)[list[w]] = reinterpret_cast<const int32_t *>(from)[w];
-        else
-          for (int64_t w = 0; w < m; ++w)
-            reinterpret_cast<double *>(to)[list[w]] = reinterpret_cast<const double *>(from)[w];
+    const int64_t csize = n_done > 0 ? cp1[0] - cp0[0] : 1;
+    std::vector<int64_t> start(static_cast<size_t>(n_done) + 1, 0);
+    std::vector<int32_t> order(static_cast<size_t>(m));
+    for (int64_t w = 0; w < m; ++w) ++start[size_t(std::min<int64_t>(list[w] / csize, n_done - 1)) + 1];
+    for (int k = 0; k < n_done; ++k) start[size_t(k) + 1] += start[size_t(k)];
+    {
+      std::vector<int64_t> fill(start.begin(), start.end() - 1);
+      for (int64_t w = 0; w < m; ++w)
+        order[size_t(fill[size_t(std::min<int64_t>(list[w] / csize, n_done - 1))]++)] = int32_t(w);
+    }
+    for (int k = 0; k < n_done; ++k) {
+      if (int rc = cuda_check(cudaEventSynchronize(s->copy_done[k]), "bh_surrogate_trace_image_host"))
+        return drained(rc);
+      for (int i = 0; i < 10; ++i) {
+        if (!host[i]) continue;
+        for (int c = 0; c < planes[i]; ++c) {
+          const char *from = s->gather_host + goff[i] + size_t(c) * cap * esize[i];
+          char *to = static_cast<char *>(host[i]) + size_t(c) * n * esize[i];
+          for (int64_t e = start[size_t(k)]; e < start[size_t(k) + 1]; ++e) {
+            const int32_t w = order[size_t(e)];
+            if (esize[i] == 4)
+              reinterpret_cast<int32_t *>(to)[list[w]] = reinterpret_cast<const int32_t *>(from)[w];
+            else
+              reinterpret_cast<double *>(to)[list[w]] = reinterpret_cast<const double *>(from)[w];
+          }
+        }
       }
     }
+    if (int rc = cuda_check(cudaStreamSynchronize(s->copy_stream), "bh_surrogate_trace_image_host")) return rc;
   } else {
     // more rejected pixels than the compact buffers hold: the whole frame again
     if (int rc = cuda_check(cudaStreamSynchronize(s->copy_stream), "bh_surrogate_trace_image_host")) return rc;
