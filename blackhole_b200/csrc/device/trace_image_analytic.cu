@@ -195,10 +195,15 @@ __global__ void __launch_bounds__(BH_ANALYTIC_THREADS, BH_ANALYTIC_MIN_CTAS)
                           const int *__restrict__ list, const unsigned int *__restrict__ count,
                           int *__restrict__ list2, unsigned int *__restrict__ count2) {
   const unsigned int total = *count;  // the same for every thread: uniform trips through the barriers
-  const unsigned int stride = gridDim.x * blockDim.x;
-  for (unsigned int base = blockIdx.x * blockDim.x; base < total; base += stride) {
+  // A short list (the renderer's ~1 % of a frame) is spread over every CTA
+  // in whole warps of consecutive entries, not packed into the first few
+  // CTAs: per CTA at most blockDim.x, at least a warp.
+  const unsigned int per =
+      min(blockDim.x, ((total + gridDim.x - 1) / gridDim.x + 31u) & ~31u);
+  const unsigned int stride = gridDim.x * per;
+  for (unsigned int base = blockIdx.x * per; base < total; base += stride) {
     const unsigned int w = base + threadIdx.x;
-    const bool live = w < total;
+    const bool live = threadIdx.x < per && w < total;
     const int pix = live ? list[w] : 0;
     if (!trace_pixel(p, o, pix, live) && live) list2[atomicAdd(count2, 1u)] = pix;
   }
