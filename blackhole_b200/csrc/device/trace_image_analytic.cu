@@ -14,6 +14,13 @@
 // last step's overshoot past r_esc.
 #include <cuda_runtime.h>
 
+// The routines that take a ray's solution structs are inlined, so that the
+// structs live in registers rather than in each thread's stack frame (the
+// kernel is compiled with 168 registers per thread: 384-thread CTAs).
+#ifndef BHA_INLINE_SOLUTION
+#define BHA_INLINE_SOLUTION 1
+#endif
+
 #include "image_fp64.cuh"
 #include "kerr_analytic.cuh"
 #include "launch.h"
@@ -53,7 +60,7 @@ __device__ __forceinline__ double phi_radial(const BhkImageParams &p, const Ray 
 // the CTA calls it and reaches every barrier (live: the thread has a pixel).
 // The kernel's code is longer than the instruction cache holds, and warps at
 // different points of it kept evicting each other's instructions (47 % of
-// fetches hit); aligned by the barriers, the CTA's 16 warps run each phase's
+// fetches hit); aligned by the barriers, the CTA's warps run each phase's
 // code at about the same time. Measured on the 2048^2 a = 0.9, 60 deg frame
 // with all outputs: 9.56 ms unaligned in 128-thread CTAs, 6.85 ms with one
 // barrier per pixel, 4.62 ms with that in 512-thread CTAs, 4.34 ms phased
@@ -166,13 +173,17 @@ __device__ __forceinline__ bool trace_pixel(const BhkImageParams &p, const BhkIm
 }
 
 // Threads per CTA and resident CTAs per SM the closed form is compiled for:
-// 512 x 1 at 128 registers per thread fills the SM's register file with one
-// CTA, whose warps the phases of trace_pixel keep together.
+// one CTA per SM, whose warps the phases of trace_pixel keep together. 384
+// threads at 168 registers (the solution structs in registers, a ~690-byte
+// frame) ran the 2048^2 a = 0.9, 60 deg frame in 4.06 ms with all outputs
+// and 1.61 ms with the disk fields, against 4.33 and 1.69 ms for 512
+// threads at 128 registers (1 KB frames that overflow L1); 320 threads
+// (168 registers, more spills) and 256 threads (246 registers) were slower.
 #ifndef BH_ANALYTIC_MIN_CTAS
 #define BH_ANALYTIC_MIN_CTAS 1
 #endif
 #ifndef BH_ANALYTIC_THREADS
-#define BH_ANALYTIC_THREADS 512
+#define BH_ANALYTIC_THREADS 384
 #endif
 
 __global__ void __launch_bounds__(BH_ANALYTIC_THREADS, BH_ANALYTIC_MIN_CTAS) k_trace_image_analytic(const __grid_constant__ BhkImageParams p,
