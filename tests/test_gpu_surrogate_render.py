@@ -281,15 +281,21 @@ def _host_render(net, s, pinned, chunks=0):
     return {f: t.numpy().reshape(-1) for f, t in outs.items()}
 
 
-@pytest.mark.parametrize("trained,pinned,chunks", [(True, True, 0), (True, True, 3), (True, False, 0),
-                                                   (False, True, 0), (False, False, 0)])
-def test_host_buffers_match_device_render(cuda, trained, pinned, chunks):
+@pytest.mark.parametrize("trained,pinned,chunks,shape", [(True, True, 0, (320, 320, 1)), (True, True, 3, (320, 320, 1)),
+                                                         (True, False, 0, (320, 320, 1)), (False, True, 0, (320, 320, 1)),
+                                                         (False, False, 0, (320, 320, 1)), (True, True, 0, (333, 217, 3)),
+                                                         (True, True, 5, (61, 47, 2)), (False, True, 0, (61, 47, 3))])
+def test_host_buffers_match_device_render(cuda, trained, pinned, chunks, shape):
     """The host-buffer entry point returns the device render's outputs bit
     for bit. Pinned buffers take the overlapped path: each chunk's rows are
     copied while the next is inferred, and the rejected pixels follow in
-    compact form (the trained network rejects under 1 %); with an untrained
-    network every pixel is rejected, more than the compact buffers hold, and
-    the frame is copied again. Pageable buffers are copied after the render."""
+    compact form (with one crossing plane the trained network rejects under
+    1 %); with an untrained
+    network every pixel is rejected, more than the compact buffers hold
+    (except on frames of at most 4096 pixels, where the compact buffers hold
+    the whole frame), and the frame is copied again. Pageable buffers are
+    copied after the render. Ragged frames with two or three crossing planes
+    check the per-plane row offsets."""
     from blackhole_b200 import kerr
     from blackhole_b200 import surrogate as S
 
@@ -298,12 +304,21 @@ def test_host_buffers_match_device_render(cuda, trained, pinned, chunks):
     net = S.Surrogate(max_batch=128, seed=3)
     if trained:
         net.load(WEIGHTS)
-    s = c4_scene(320, precision=1)
+    # Ragged sizes and several crossing planes exercise the per-plane row
+    # copies. With more than one plane, rays that hit the disk once and escape
+    # go to the integrator, so the 333 x 217 frame rejects more pixels than
+    # the compact buffers hold (the frame is copied again), while frames of at
+    # most 4096 pixels fit the compact buffers whole (gathered and scattered).
+    W, H, mc = shape
+    s = c4_scene(W, height=H, max_crossings=mc, precision=1)
     ref = host(net.trace_image(s, kerr.alloc_image_outputs(s, fields=list(ALL_FIELDS))))
     torch.cuda.synchronize()
     st = net.last_stats()
     rejected = st["pixels"] - st["accepted"]
-    assert (0 < rejected < 4096) if trained else rejected == st["pixels"], st
+    if mc == 1:
+        assert (0 < rejected < 4096) if trained else rejected == st["pixels"], st
+    else:
+        assert rejected > 0, st
     for _ in range(2):  # the second call reuses the grown buffers
         got = _host_render(net, s, pinned, chunks)
         for f in ALL_FIELDS:
