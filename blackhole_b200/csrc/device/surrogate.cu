@@ -469,6 +469,11 @@ __global__ void k_loss(const float* __restrict__ out, const float* __restrict__ 
 #define BHS_EPI_PIPE 1
 #endif
 
+// K steps (16 columns each) of layer 0's last 64-column chunk that can hold a
+// nonzero term: features 128..133 lie in the first.
+constexpr int kFeatTailSteps = (BHS_FEATURES_USED - 128 + 15) / 16;
+static_assert(BHS_FEATURES_USED > 128 && BHS_FEATURES_USED <= 144, "feature tail within one K step");
+
 constexpr int kInfThreads = 576;  // 2 control warps + 2 slots x 8 epilogue warps
 constexpr int kEpiThreads = 256;  // epilogue threads per slot
 constexpr int kInfRing = 3;
@@ -595,9 +600,12 @@ __global__ void __launch_bounds__(kInfThreads, 1)
               umma::tc_fence_after();
               const uint64_t ad = umma::sw128_desc(act0 + (uint32_t)s * kActBytes + (uint32_t)c * kActChunk);
               const uint64_t bd = umma::sw128_desc(ring0 + (uint32_t)st * kWChunk);
+              // layer 0's last chunk holds features 128..133 and zero padding
+              // (zero weights too): its first K step covers every nonzero term
+              const int ksteps = (l == 0 && c == layer_chunks(0) - 1) ? kFeatTailSteps : kBK / 16;
 #pragma unroll
               for (int k = 0; k < kBK / 16; ++k)
-                umma::mma_bf16(d, ad + 2u * k, bd + 2u * k, idesc, (c > 0 || k > 0) ? 1u : 0u);
+                if (k < ksteps) umma::mma_bf16(d, ad + 2u * k, bd + 2u * k, idesc, (c > 0 || k > 0) ? 1u : 0u);
               umma::mma_commit(empty(st));
             }
             umma::mma_commit(acc_full(s));
@@ -636,11 +644,10 @@ __global__ void __launch_bounds__(kInfThreads, 1)
           }
         }
         if (hf == 1) {
-          // unit 16: columns 128..135 (scaled inputs, lambda, eta, two zeros); units 17..23: zero
+          // unit 16: columns 128..135 (scaled inputs, lambda, eta, two zeros); unit 17: zero
           st_unit(act + 2u * kActChunk, r, 0, pack_f16(z * x[0], z * x[1]), pack_f16(z * x[2], z * x[3]),
                   pack_f16(z * lam, z * eta), 0u);
-#pragma unroll
-          for (int u = 17; u < BHS_FEATURES / 8; ++u) st_unit(act + 2u * kActChunk, r, u & 7, 0u, 0u, 0u, 0u);
+          st_unit(act + 2u * kActChunk, r, 1, 0u, 0u, 0u, 0u);  // unit 17; units 18..23 are never read
         }
       }
       umma::fence_async_smem();
