@@ -653,6 +653,32 @@ int bh_surrogate_trace_image_host(BH_Surrogate *s, const BH_KerrScene *scene, co
       pinned = false;
     }
   }
+  // compact buffers: the count, the list, then each field's planes of `cap`
+  // entries, in mapped page-locked memory; where that cannot be had, the
+  // frame takes the path of pageable buffers
+  const int64_t cap = std::min<int64_t>(int64_t(n), std::max<int64_t>(4096, int64_t(n) / 25));
+  size_t gbytes = 256 + ((size_t(cap) * 4 + 255) & ~size_t(255)), goff[10];
+  for (int i = 0; i < 10; ++i) {
+    goff[i] = gbytes;
+    if (host[i]) gbytes += (size_t(cap) * planes[i] * esize[i] + 255) & ~size_t(255);
+  }
+  if (pinned && gbytes > s->gather_bytes) {
+    if (s->gather_host) cudaFreeHost(s->gather_host);
+    s->gather_host = s->gather_dev = nullptr;
+    s->gather_bytes = 0;
+    if (cudaHostAlloc(&s->gather_host, gbytes, cudaHostAllocMapped) != cudaSuccess) {
+      cudaGetLastError();
+      s->gather_host = nullptr;
+      pinned = false;
+    } else if (cudaHostGetDevicePointer(&s->gather_dev, s->gather_host, 0) != cudaSuccess) {
+      cudaGetLastError();
+      cudaFreeHost(s->gather_host);
+      s->gather_host = s->gather_dev = nullptr;
+      pinned = false;
+    } else {
+      s->gather_bytes = gbytes;
+    }
+  }
   if (!pinned) {
     if (int rc = render(s, scene, &dev, policy, s->host_stream, 0, nullptr)) return rc;
     for (int i = 0; i < 10; ++i)
@@ -690,26 +716,6 @@ int bh_surrogate_trace_image_host(BH_Surrogate *s, const BH_KerrScene *scene, co
     n_done = k + 1;
     return cuda_check(cudaEventRecord(s->copy_done[k], s->copy_stream), "cudaEventRecord");
   };
-  // compact buffers: the count, the list, then each field's planes of `cap` entries
-  const int64_t cap = std::min<int64_t>(int64_t(n), std::max<int64_t>(4096, int64_t(n) / 25));
-  size_t gbytes = 256 + ((size_t(cap) * 4 + 255) & ~size_t(255)), goff[10];
-  for (int i = 0; i < 10; ++i) {
-    goff[i] = gbytes;
-    if (host[i]) gbytes += (size_t(cap) * planes[i] * esize[i] + 255) & ~size_t(255);
-  }
-  if (gbytes > s->gather_bytes) {
-    if (s->gather_host) cudaFreeHost(s->gather_host);
-    s->gather_host = s->gather_dev = nullptr;
-    s->gather_bytes = 0;
-    if (int rc = cuda_check(cudaHostAlloc(&s->gather_host, gbytes, cudaHostAllocMapped), "cudaHostAlloc(gathered pixels)"))
-      return rc;
-    if (int rc = cuda_check(cudaHostGetDevicePointer(&s->gather_dev, s->gather_host, 0), "cudaHostGetDevicePointer")) {
-      cudaFreeHost(s->gather_host);
-      s->gather_host = nullptr;
-      return rc;
-    }
-    s->gather_bytes = gbytes;
-  }
   // on a failure after rows were enqueued: no copy may still be writing into
   // the caller's buffers when the call returns
   auto drained = [&](int rc) {

@@ -146,8 +146,10 @@ int bh_surrogate_trace_image(BH_Surrogate* s, const BH_KerrScene* scene, const B
  * and each chunk's rows are copied while the next one is inferred; the
  * pixels the policy rejected follow, gathered on the device into compact
  * arrays and scattered on the host (past max(4096, pixels / 25) of them the
- * frame is copied again). Pageable buffers get one copy per field after the
- * render. The outputs are the same either way.
+ * frame is copied again; the gathered pixels go through a mapped page-locked
+ * buffer the network keeps). Pageable buffers, or a failed allocation of that
+ * buffer, get one copy per field after the render. The outputs are the same
+ * either way.
  * Returns -1 with a message when an allocation fails or when a bounded wait
  * of the network's kernels ran out (the outputs are then not valid); the
  * next call starts afresh. */
