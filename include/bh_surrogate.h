@@ -111,7 +111,8 @@ typedef struct BH_SurrogatePolicy {
                                  the Newton iteration of the solve) */
     double critical_band;  /* first-order image-plane distance to the critical curve, M,
                               below which a pixel goes to the integrator (0.05) */
-    int32_t refine_fp64;   /* 0: Mino-time quadrature in FP32 (r_hit to ~4e-6); 1: all FP64 (~1e-8) */
+    int32_t refine_fp64;   /* 0: Mino-time quadrature in FP32 (r_hit to ~4e-6, up to ~5e-5 for rays
+                              just outside the critical band); 1: all FP64 (~1e-8) */
     int32_t chunks;        /* pixel chunks whose refinement (second stream) overlaps the next
                               chunk's inference; 0 = default (1..8) */
 } BH_SurrogatePolicy;
