@@ -216,12 +216,28 @@ class Surrogate:
         return outs
 
     def trace_image_host(self, scene, fields=None, min_confidence: float = 0.99, verify: int = 1,
-                         critical_band: float = 0.05, refine_fp64: bool = False, chunks: int = 0) -> dict:
+                         critical_band: float = 0.05, refine_fp64: bool = False, chunks: int = 0,
+                         pinned: bool = True) -> dict:
         """The same render into host (numpy) buffers through
-        bh_surrogate_trace_image_host; raises on -1 with the library's message."""
-        from .kerr import host_image_outputs
+        bh_surrogate_trace_image_host; raises on -1 with the library's message.
 
-        arrs, o = host_image_outputs(scene, fields)
+        ``pinned``: the arrays are views of page-locked memory, so the library
+        copies each chunk's rows while later chunks render; with False they
+        are ordinary numpy arrays, copied after the render. The values are
+        the same either way."""
+        from .kerr import _out_struct, host_image_outputs
+
+        if pinned:
+            n = scene.width * scene.height
+            mc = scene.max_crossings
+            fields = fields or _abi.OUT_FIELDS
+            ts = {k: torch.zeros((mc, n) if k in _abi.PLANE_FIELDS else (n,),
+                                 dtype=torch.int32 if k in _abi.INT_FIELDS else torch.float64).pin_memory()
+                  for k in fields}
+            o = _out_struct(ts)
+            arrs = {k: v.numpy() for k, v in ts.items()}  # views: each keeps its page-locked tensor alive
+        else:
+            arrs, o = host_image_outputs(scene, fields)
         pol = _abi.SurrogatePolicy(min_confidence, verify, critical_band, int(refine_fp64), int(chunks))
         check(self._lib.bh_surrogate_trace_image_host(self._h, C.byref(scene), C.byref(o), C.byref(pol)))
         return arrs
