@@ -88,10 +88,11 @@ SURROGATE_WEIGHTS = ROOT / "blackhole_b200" / "data" / "surrogate_c4.npz"
 SKY_SIZE, SKY_STARS, SKY_SEED = 512, 10_000, 20261203
 # Algorithmic MACs per ray of the network, 2 FLOPs each: 134 input features
 # (128 Fourier, 4 raw inputs, lambda, eta) x 256, 3 x 256 x 256, 256 x 16
-# heads. The kernel executes the input layer on 192 zero-padded columns
-# (three 64-column TMA boxes): SURROGATE_MMA_FLOPS_PER_RAY.
+# heads. The kernel executes the input layer on 144 columns (two 64-column
+# K chunks and the one 16-column K step of the third that holds features
+# 128..133): SURROGATE_MMA_FLOPS_PER_RAY.
 SURROGATE_FLOPS_PER_RAY = 2.0 * (134 * 256 + 3 * 256 * 256 + 256 * 16)
-SURROGATE_MMA_FLOPS_PER_RAY = 2.0 * (192 * 256 + 3 * 256 * 256 + 256 * 16)
+SURROGATE_MMA_FLOPS_PER_RAY = 2.0 * (144 * 256 + 3 * 256 * 256 + 256 * 16)
 OUT_FIELDS_USED = ("cls", "steps", "n_cross", "r_hit", "phi_hit", "g", "flux", "intensity", "theta_inf", "phi_inf")
 
 
