@@ -70,3 +70,21 @@ def test_transfer_flops_constant(oracle, lib):
                             (desc.log_x_min, desc.log_x_max), p.nu_hz, p.length_cm, p.ds_max, p.min_transmit, pix)
     f = (c["add"] + c["mul"] + c["div"] + c["sqrt"]) / c["steps"]
     assert f == pytest.approx(bench.FLOPS_PER_STEP["rt"], rel=0.05)
+
+
+def test_surrogate_flop_constants(lib):
+    """The network FLOPs the surrogate line divides by follow the library's
+    layer shapes: 134 used input features of 192 (the rest is zero padding),
+    4 hidden layers of 256, a 16-wide head. The kernel executes the input
+    layer on 144 columns (two 64-column K chunks and the first 16-column K
+    step of the third, which holds features 128..133)."""
+    import bench
+
+    K = [192, 256, 256, 256, 256]
+    N = [256, 256, 256, 256, 16]
+    assert lib.bh_surrogate_param_count() == sum(k * n + n for k, n in zip(K, N))
+    used = [134] + K[1:]
+    assert bench.SURROGATE_FLOPS_PER_RAY == 2.0 * sum(k * n for k, n in zip(used, N))
+    executed_k0 = 128 + 16 * math.ceil((134 - 128) / 16)
+    assert executed_k0 == 144
+    assert bench.SURROGATE_MMA_FLOPS_PER_RAY == 2.0 * sum(k * n for k, n in zip([executed_k0] + K[1:], N))
